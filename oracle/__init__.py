@@ -1,0 +1,223 @@
+"""CPU oracle for the D3Q27 A-A hot path (test infrastructure only).
+
+Two checkers with the same call signatures:
+
+* ``Port``      -- this project's C restatement (``oracle/lbm_oracle.c``),
+  built into ``oracle/_build/liboracle.so``.
+* ``Reference`` -- TNL-LBM's own per-site headers compiled from the reference
+  tree through ``oracle/ref_harness.cpp`` into ``oracle/_ref/*.so``.  Present
+  only where those libraries were built (they travel with the repository
+  snapshot but cannot be rebuilt without the reference sources).
+
+Only the test-suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may use this package.  Nothing in the product imports it.
+
+Array conventions (numpy, C order):
+  populations  [27, Z+2, Y+2, X+2]  x fastest, one ghost layer
+  map          [Z, Y, X]            int16 GEO values of D3Q27_BC_All
+  macro        [4, Z, Y, X]         rho, vx, vy, vz
+  inflow       [Z, Y]               per-direction velocity profile or None
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REFDIR = os.path.join(HERE, "_ref")
+
+COLL = {"CUM": 0, "SRT": 1, "BGK": 2, "MRT": 3}
+EQ = {"EQ": 0, "INV_CUM": 1}
+CUM_2017 = 1
+CUM_ANTIALIAS = 2
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the restatement (and the reference harness when its sources exist)."""
+    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _dptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def _prec(dtype) -> int:
+    dtype = np.dtype(dtype)
+    if dtype == np.float64:
+        return 0
+    if dtype == np.float32:
+        return 1
+    raise TypeError(f"oracle supports float64/float32, not {dtype}")
+
+
+def _profiles(inflow):
+    if inflow is None:
+        return None, None, None
+    return tuple(None if p is None else np.ascontiguousarray(p, dtype=np.float64) for p in inflow)
+
+
+class _Base:
+    def allocate(self, X, Y, Z, dtype=np.float64):
+        return np.zeros((27, Z + 2, Y + 2, X + 2), dtype=dtype)
+
+
+class Port(_Base):
+    """This project's C restatement of the reference algorithm."""
+
+    def __init__(self):
+        path = os.path.join(BUILD, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = ctypes.CDLL(path)
+        for sfx in ("_f64", "_f32"):
+            fn = getattr(self.lib, "orc_aa_run" + sfx)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _vp, _vp,
+                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _vp,
+                           ctypes.c_long, ctypes.c_int, ctypes.c_int]
+            fn = getattr(self.lib, "orc_init_equilibrium" + sfx)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _vp, _dp, _dp, _dp, _dp,
+                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+            fn = getattr(self.lib, "orc_collide" + sfx)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _vp, _vp, ctypes.c_double,
+                           ctypes.c_double, ctypes.c_double, ctypes.c_double]
+            fn = getattr(self.lib, "orc_equilibrium" + sfx)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int, ctypes.c_long, _dp, _dp, _dp, _dp, _vp]
+
+    @staticmethod
+    def _sfx(dtype):
+        return "_f64" if _prec(dtype) == 0 else "_f32"
+
+    def aa_run(self, f, geo_map, coll="CUM", eq="INV_CUM", cum_flags=0, nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
+               macro=None, start_iter=0, nsteps=1, nthreads=0):
+        Z, Y, X = geo_map.shape
+        assert f.shape == (27, Z + 2, Y + 2, X + 2) and f.flags.c_contiguous
+        m = np.ascontiguousarray(geo_map, dtype=np.int16)
+        vx, vy, vz = _profiles(inflow)
+        if macro is not None:
+            assert macro.shape == (4, Z, Y, X) and macro.dtype == f.dtype
+        rc = getattr(self.lib, "orc_aa_run" + self._sfx(f.dtype))(
+            COLL[coll], EQ[eq], cum_flags, X, Y, Z, _ptr(f), _ptr(m), nu, *force, _dptr(vx), _dptr(vy), _dptr(vz),
+            _ptr(macro), start_iter, nsteps, nthreads)
+        if rc != 0:
+            raise RuntimeError(f"orc_aa_run failed with {rc}")
+        return f
+
+    def init_equilibrium(self, f, X, Y, Z, eq="INV_CUM", fields=None, uniform=(1.0, 0.0, 0.0, 0.0)):
+        rho = vx = vy = vz = None
+        if fields is not None:
+            rho, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in fields)
+        rc = getattr(self.lib, "orc_init_equilibrium" + self._sfx(f.dtype))(
+            EQ[eq], X, Y, Z, _ptr(f), _dptr(rho), _dptr(vx), _dptr(vy), _dptr(vz), *uniform)
+        if rc != 0:
+            raise RuntimeError("orc_init_equilibrium failed")
+        return f
+
+    def collide(self, f, coll="CUM", eq="INV_CUM", cum_flags=0, nu=0.01, force=(0.0, 0.0, 0.0)):
+        """Per-site collision of f[n, 27] in place; returns macro [n, 4] (pre-collision rho, u)."""
+        assert f.ndim == 2 and f.shape[1] == 27 and f.flags.c_contiguous
+        macro = np.zeros((f.shape[0], 4), dtype=f.dtype)
+        getattr(self.lib, "orc_collide" + self._sfx(f.dtype))(COLL[coll], EQ[eq], cum_flags, f.shape[0], _ptr(f),
+                                                               _ptr(macro), nu, *force)
+        return macro
+
+    def equilibrium(self, rho, vx, vy, vz, eq="INV_CUM", dtype=np.float64):
+        rho, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (rho, vx, vy, vz))
+        out = np.zeros((rho.size, 27), dtype=dtype)
+        getattr(self.lib, "orc_equilibrium" + self._sfx(dtype))(EQ[eq], rho.size, _dptr(rho), _dptr(vx), _dptr(vy),
+                                                                 _dptr(vz), _ptr(out))
+        return out
+
+
+_REF_VARIANTS = {0: "libref_cum_default", CUM_ANTIALIAS: "libref_cum_aa",
+                 CUM_2017 | CUM_ANTIALIAS: "libref_cum_2017aa"}
+
+
+def reference_available(cum_flags: int = 0) -> bool:
+    name = _REF_VARIANTS.get(cum_flags)
+    return name is not None and os.path.exists(os.path.join(REFDIR, name + ".so"))
+
+
+class Reference(_Base):
+    """TNL-LBM's own per-site code (one library per cumulant flag set)."""
+
+    def __init__(self, cum_flags: int = 0, fast: bool = False):
+        name = _REF_VARIANTS[cum_flags] + ("_fast" if fast else "")
+        path = os.path.join(REFDIR, name + ".so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.cum_flags = cum_flags
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_aa_run.restype = ctypes.c_int
+        L.ref_aa_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _vp,
+                                 _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp,
+                                 _vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_init_equilibrium.restype = ctypes.c_int
+        L.ref_init_equilibrium.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _vp, _dp,
+                                           _dp, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double]
+        L.ref_collide.restype = ctypes.c_int
+        L.ref_collide.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, _vp, _vp, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_equilibrium.restype = ctypes.c_int
+        L.ref_equilibrium.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, _dp, _dp, _dp, _dp, _vp]
+        L.ref_cum_flags.restype = ctypes.c_int
+        assert L.ref_cum_flags() == cum_flags
+
+    def aa_run(self, f, geo_map, coll="CUM", eq="INV_CUM", cum_flags=None, nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
+               macro=None, start_iter=0, nsteps=1, nthreads=0, return_time=False):
+        if cum_flags is not None and cum_flags != self.cum_flags:
+            raise ValueError("this reference build has cumulant flags %d" % self.cum_flags)
+        Z, Y, X = geo_map.shape
+        assert f.shape == (27, Z + 2, Y + 2, X + 2) and f.flags.c_contiguous
+        m = np.ascontiguousarray(geo_map, dtype=np.int16)
+        vx, vy, vz = _profiles(inflow)
+        el = ctypes.c_double(0.0)
+        rc = self.lib.ref_aa_run(_prec(f.dtype), COLL[coll], EQ[eq], X, Y, Z, _ptr(f), _ptr(m), nu, *force, _dptr(vx),
+                                 _dptr(vy), _dptr(vz), _ptr(macro), start_iter, nsteps, nthreads, ctypes.byref(el))
+        if rc != 0:
+            raise RuntimeError(f"ref_aa_run failed with {rc}")
+        return (f, el.value) if return_time else f
+
+    def init_equilibrium(self, f, X, Y, Z, eq="INV_CUM", fields=None, uniform=(1.0, 0.0, 0.0, 0.0)):
+        rho = vx = vy = vz = None
+        if fields is not None:
+            rho, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in fields)
+        rc = self.lib.ref_init_equilibrium(_prec(f.dtype), EQ[eq], X, Y, Z, _ptr(f), _dptr(rho), _dptr(vx), _dptr(vy),
+                                           _dptr(vz), *uniform)
+        if rc != 0:
+            raise RuntimeError("ref_init_equilibrium failed")
+        return f
+
+    def collide(self, f, coll="CUM", eq="INV_CUM", cum_flags=None, nu=0.01, force=(0.0, 0.0, 0.0)):
+        macro = np.zeros((f.shape[0], 4), dtype=f.dtype)
+        self.lib.ref_collide(_prec(f.dtype), COLL[coll], EQ[eq], f.shape[0], _ptr(f), _ptr(macro), nu, *force)
+        return macro
+
+    def equilibrium(self, rho, vx, vy, vz, eq="INV_CUM", dtype=np.float64):
+        rho, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (rho, vx, vy, vz))
+        out = np.zeros((rho.size, 27), dtype=dtype)
+        self.lib.ref_equilibrium(_prec(dtype), EQ[eq], rho.size, _dptr(rho), _dptr(vx), _dptr(vy), _dptr(vz), _ptr(out))
+        return out

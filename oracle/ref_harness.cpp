@@ -1,0 +1,547 @@
+// Reference harness: TNL-LBM's own per-site operator headers, compiled
+// unmodified from the reference tree (include/lbm3d/d3q27/*.h) against the
+// small shim in oracle/shim, driven by the per-site loop of the reference's
+// kernel (include/lbm3d/kernels.h:5-112) and its host OpenMP loop
+// (include/lbm3d/state.hpp:1388-1397).
+//
+// TEST INFRASTRUCTURE ONLY.  The resulting oracle/_ref/*.so is used by the
+// test-suite as a checker, by tests/golden/make_golden.py to produce fixtures,
+// and by bench.py's CPU-baseline leg.  The product library never links it.
+//
+// Streaming pattern: A-A (streaming_AA.h).  The reference's A-A kernel assumes
+// one ghost layer of lattice sites in every direction (kernels.h:30-37) that
+// is initialised together with the interior (lbm_block.hpp:248-278), so the
+// harness allocates that layer.  Storage order is the reference's own
+// (q, x, z, y) with y fastest (defs.h:90-91, lbm_data.h:50-54); the exported
+// functions exchange populations in the canonical order
+// [27][Z+2][Y+2][X+2] (x fastest, ghost layer included) and transpose at the
+// boundary of each call.
+//
+// Variant selection: the cumulant flags USE_GEIER_CUM_2017 and
+// USE_GEIER_CUM_ANTIALIAS are preprocessor switches in the reference
+// (defs.h:312-315), so this file is compiled once per flag set (see Makefile).
+
+#include <chrono>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+	#include <omp.h>
+#endif
+
+#include "lbm3d/defs.h"	 // resolves to oracle/shim/lbm3d/defs.h
+
+#include "lbm3d/d3q27/bc.h"
+#include "lbm3d/d3q27/col_bgk.h"
+#include "lbm3d/d3q27/col_cum.h"
+#include "lbm3d/d3q27/col_mrt.h"
+#include "lbm3d/d3q27/col_srt.h"
+#include "lbm3d/d3q27/eq.h"
+#include "lbm3d/d3q27/eq_inv_cum.h"
+#include "lbm3d/d3q27/macro.h"
+#include "lbm3d/d3q27/streaming_AA.h"
+
+namespace {
+
+template <typename DREAL>
+struct HarnessTraits
+{
+	using real = double;
+	using dreal = DREAL;
+	using idx = long int;
+	using map_t = short int;
+};
+
+int g_unsupported_hit = 0;
+
+// The reference's A-A streaming lacks the two members that D3Q27_BC_All calls
+// for adjoint and interpolated-outflow sites (bc.h:79, bc.h:196).  The harness
+// rejects maps containing those site types before stepping, so these bodies
+// are unreachable; they only let bc.h instantiate.
+template <typename TRAITS>
+struct HarnessStreamingAA : D3Q27_STREAMING<TRAITS>
+{
+	using idx = typename TRAITS::idx;
+
+	template <typename D, typename K>
+	static void streamingAdjoint(D&, K&, idx, idx, idx, idx, idx, idx, idx, idx, idx)
+	{
+		g_unsupported_hit = 1;
+	}
+
+	template <typename D, typename K>
+	static void streamingInterpRight(D&, K&, idx, idx, idx, idx, idx, idx, idx, idx, idx)
+	{
+		g_unsupported_hit = 1;
+	}
+};
+
+// Kernel data: the members D3Q27_BC_All, D3Q27_STREAMING and
+// D3Q27_MACRO_Default touch (lbm_data.h:8-61 LBM_Data, :65-73 NSE_Data,
+// :95-133 NSE_Data_InflowProfile), with the ghost-layer indexer.
+template <typename TRAITS>
+struct HarnessData
+{
+	using idx = typename TRAITS::idx;
+	using dreal = typename TRAITS::dreal;
+	using map_t = typename TRAITS::map_t;
+
+	bool even_iter = true;
+	idx nx = 0, ny = 0, nz = 0;	 // interior sizes
+	idx XYZ = 0;				 // per-direction stride incl. ghosts
+	dreal lbmViscosity = 0;
+	dreal fx = 0, fy = 0, fz = 0;
+	dreal* dfs[DFMAX] = {nullptr};
+	dreal* dmacro = nullptr;
+	const map_t* dmap = nullptr;
+	const dreal* inflow_vx = nullptr;
+	const dreal* inflow_vy = nullptr;
+	const dreal* inflow_vz = nullptr;
+
+	idx X() const { return nx; }
+	idx Y() const { return ny; }
+	idx Z() const { return nz; }
+
+	// reference storage order (q, x, z, y), y fastest; coordinates may be -1..N
+	idx storage(idx x, idx y, idx z) const
+	{
+		return ((x + 1) * (nz + 2) + (z + 1)) * (ny + 2) + (y + 1);
+	}
+
+	map_t map(idx x, idx y, idx z) const
+	{
+		return dmap[(z * ny + y) * nx + x];
+	}
+
+	dreal& df(uint8_t type, int q, idx x, idx y, idx z)
+	{
+		return dfs[type][q * XYZ + storage(x, y, z)];
+	}
+
+	dreal& macro(int id, idx x, idx y, idx z)
+	{
+		return dmacro[((id * nz + z) * ny + y) * nx + x];
+	}
+
+	template <typename LBM_KS>
+	void inflow(LBM_KS& KS, idx x, idx y, idx z)
+	{
+		(void) x;
+		KS.vx = inflow_vx ? inflow_vx[ny * z + y] : 0;
+		KS.vy = inflow_vy ? inflow_vy[ny * z + y] : 0;
+		KS.vz = inflow_vz ? inflow_vz[ny * z + y] : 0;
+	}
+};
+
+template <typename DREAL, typename COLL, typename EQ>
+using HarnessConfig = LBM_CONFIG<
+	HarnessTraits<DREAL>,
+	D3Q27_KernelStruct,
+	HarnessData<HarnessTraits<DREAL>>,
+	COLL,
+	EQ,
+	HarnessStreamingAA<HarnessTraits<DREAL>>,
+	D3Q27_BC_All,
+	D3Q27_MACRO_Default<HarnessTraits<DREAL>>>;
+
+// neighbour indices as kernelInitIndices (kernels.h:5-57), A-A branch, single
+// block (no distribution)
+template <typename NSE>
+inline void init_indices(
+	typename NSE::DATA& SD,
+	typename NSE::TRAITS::map_t map,
+	long x,
+	long y,
+	long z,
+	long& xp,
+	long& xm,
+	long& yp,
+	long& ym,
+	long& zp,
+	long& zm
+)
+{
+	if (NSE::BC::isPeriodic(map)) {
+		xp = (x == SD.X() - 1) ? 0 : (x + 1);
+		xm = (x == 0) ? (SD.X() - 1) : (x - 1);
+		yp = (y == SD.Y() - 1) ? 0 : (y + 1);
+		ym = (y == 0) ? (SD.Y() - 1) : (y - 1);
+		zp = (z == SD.Z() - 1) ? 0 : (z + 1);
+		zm = (z == 0) ? (SD.Z() - 1) : (z - 1);
+	}
+	else {
+		xp = x + 1;
+		xm = x - 1;
+		yp = y + 1;
+		ym = y - 1;
+		zp = z + 1;
+		zm = z - 1;
+	}
+}
+
+// one lattice-site update, the body of cudaLBMKernel / LBMKernel (kernels.h:92-111)
+template <typename NSE>
+inline void site_update(typename NSE::DATA& SD, long x, long y, long z, bool output_macro)
+{
+	using dreal = typename NSE::TRAITS::dreal;
+	const auto gi_map = SD.map(x, y, z);
+	long xp, xm, yp, ym, zp, zm;
+	init_indices<NSE>(SD, gi_map, x, y, z, xp, xm, yp, ym, zp, zm);
+
+	typename NSE::template KernelStruct<dreal> KS;
+	NSE::MACRO::copyQuantities(SD, KS, x, y, z);
+	NSE::MACRO::template computeForcing<typename NSE::BC>(SD, KS, xm, x, xp, ym, y, yp, zm, z, zp);
+	NSE::BC::preCollision(SD, KS, gi_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (NSE::BC::doCollision(gi_map))
+		NSE::COLL::collision(KS);
+	NSE::BC::postCollision(SD, KS, gi_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (output_macro)
+		NSE::MACRO::outputMacro(SD, KS, x, y, z);
+}
+
+// site types whose A-A update reads a slot that another site writes in the same
+// pass (GEO_INFLOW_BB_LEFT bc.h:155-163, GEO_OUTFLOW_RIGHT bc.h:73-74); with
+// these present the harness runs single-threaded in the reference loop order
+bool map_is_order_dependent(const short* map, long n)
+{
+	for (long i = 0; i < n; i++)
+		if (map[i] == 4 || map[i] == 7)
+			return true;
+	return false;
+}
+
+bool map_is_supported(const short* map, long n)
+{
+	for (long i = 0; i < n; i++)
+		if (map[i] < 0 || map[i] == 8 || map[i] > 16)
+			return false;
+	return true;
+}
+
+template <typename DREAL>
+void canonical_to_ref(const DREAL* src, DREAL* dst, long X, long Y, long Z)
+{
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+	for (int q = 0; q < 27; q++)
+		for (long z = 0; z < Z + 2; z++)
+			for (long y = 0; y < Y + 2; y++)
+				for (long x = 0; x < X + 2; x++)
+					dst[q * XYZ + (x * (Z + 2) + z) * (Y + 2) + y] = src[q * XYZ + (z * (Y + 2) + y) * (X + 2) + x];
+}
+
+template <typename DREAL>
+void ref_to_canonical(const DREAL* src, DREAL* dst, long X, long Y, long Z)
+{
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+	for (int q = 0; q < 27; q++)
+		for (long z = 0; z < Z + 2; z++)
+			for (long y = 0; y < Y + 2; y++)
+				for (long x = 0; x < X + 2; x++)
+					dst[q * XYZ + (z * (Y + 2) + y) * (X + 2) + x] = src[q * XYZ + (x * (Z + 2) + z) * (Y + 2) + y];
+}
+
+template <typename NSE>
+int run_aa(
+	long X,
+	long Y,
+	long Z,
+	typename NSE::TRAITS::dreal* f_canonical,
+	const short* map,
+	double nu,
+	double fx,
+	double fy,
+	double fz,
+	const double* in_vx,
+	const double* in_vy,
+	const double* in_vz,
+	typename NSE::TRAITS::dreal* macro,
+	long start_iter,
+	int nsteps,
+	int nthreads,
+	double* elapsed_s
+)
+{
+	using dreal = typename NSE::TRAITS::dreal;
+	const long n = X * Y * Z;
+	if (! map_is_supported(map, n))
+		return -2;
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+	std::vector<dreal> df(27 * XYZ);
+	canonical_to_ref(f_canonical, df.data(), X, Y, Z);
+
+	std::vector<dreal> pvx, pvy, pvz;
+	auto convert_profile = [&](const double* src, std::vector<dreal>& dst) -> const dreal*
+	{
+		if (! src)
+			return nullptr;
+		dst.resize(Y * Z);
+		for (long i = 0; i < Y * Z; i++)
+			dst[i] = (dreal) src[i];
+		return dst.data();
+	};
+
+	typename NSE::DATA SD;
+	SD.nx = X;
+	SD.ny = Y;
+	SD.nz = Z;
+	SD.XYZ = XYZ;
+	SD.lbmViscosity = (dreal) nu;
+	SD.fx = (dreal) fx;
+	SD.fy = (dreal) fy;
+	SD.fz = (dreal) fz;
+	SD.dfs[df_cur] = df.data();
+	SD.dmacro = macro;
+	SD.dmap = map;
+	SD.inflow_vx = convert_profile(in_vx, pvx);
+	SD.inflow_vy = convert_profile(in_vy, pvy);
+	SD.inflow_vz = convert_profile(in_vz, pvz);
+
+	const bool sequential = map_is_order_dependent(map, n);
+#ifdef _OPENMP
+	const int threads = sequential ? 1 : (nthreads > 0 ? nthreads : omp_get_max_threads());
+#else
+	(void) nthreads;
+	(void) sequential;
+#endif
+	g_unsupported_hit = 0;
+	const auto t0 = std::chrono::steady_clock::now();
+	for (int s = 0; s < nsteps; s++) {
+		// LBM::updateKernelData (lbm.hpp:311)
+		SD.even_iter = ((start_iter + s) % 2) == 0;
+		const bool output_macro = macro != nullptr;
+		// host loop of State::SimUpdate (state.hpp:1388-1397): x, z outer, y inner
+#pragma omp parallel for schedule(static) collapse(2) num_threads(threads)
+		for (long x = 0; x < X; x++)
+			for (long z = 0; z < Z; z++)
+				for (long y = 0; y < Y; y++)
+					site_update<NSE>(SD, x, y, z, output_macro);
+	}
+	const auto t1 = std::chrono::steady_clock::now();
+	if (elapsed_s)
+		*elapsed_s = std::chrono::duration<double>(t1 - t0).count();
+	ref_to_canonical(df.data(), f_canonical, X, Y, Z);
+	return g_unsupported_hit ? -3 : 0;
+}
+
+template <typename DREAL, typename COLL, typename EQ>
+int run_aa_typed(
+	long X,
+	long Y,
+	long Z,
+	void* f,
+	const short* map,
+	double nu,
+	double fx,
+	double fy,
+	double fz,
+	const double* vx,
+	const double* vy,
+	const double* vz,
+	void* macro,
+	long start_iter,
+	int nsteps,
+	int nthreads,
+	double* elapsed
+)
+{
+	using NSE = HarnessConfig<DREAL, COLL, EQ>;
+	return run_aa<NSE>(
+		X, Y, Z, (DREAL*) f, map, nu, fx, fy, fz, vx, vy, vz, (DREAL*) macro, start_iter, nsteps, nthreads, elapsed
+	);
+}
+
+template <typename DREAL, typename EQ>
+int dispatch_coll(int coll, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy, double fz,
+				  const double* vx, const double* vy, const double* vz, void* macro, long it, int ns, int nt, double* el)
+{
+	using T = HarnessTraits<DREAL>;
+	switch (coll) {
+		case 0:
+			return run_aa_typed<DREAL, D3Q27_CUM<T, EQ>, EQ>(X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, it, ns, nt, el);
+		case 1:
+			return run_aa_typed<DREAL, D3Q27_SRT<T, EQ>, EQ>(X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, it, ns, nt, el);
+		case 2:
+			return run_aa_typed<DREAL, D3Q27_BGK<T, EQ>, EQ>(X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, it, ns, nt, el);
+		case 3:
+			return run_aa_typed<DREAL, D3Q27_MRT<T, EQ>, EQ>(X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, it, ns, nt, el);
+		default:
+			return -1;
+	}
+}
+
+// equilibrium of one site through the collision's inherited setEquilibriumLat
+// (common.h:127-158), which takes rho and u in `real` (double)
+template <typename DREAL, typename EQ>
+void eq_into(DREAL* out27, double rho, double vx, double vy, double vz)
+{
+	struct View
+	{
+		DREAL* p;
+		DREAL& operator()(int q, long, long, long)
+		{
+			return p[q];
+		}
+	} v{out27};
+	D3Q27_COMMON<HarnessTraits<DREAL>, EQ>::setEquilibriumLat(v, 0, 0, 0, rho, vx, vy, vz);
+}
+
+template <typename DREAL, typename EQ>
+int init_eq_typed(long X, long Y, long Z, DREAL* f, const double* rho, const double* vx, const double* vy, const double* vz,
+				  double rho0, double vx0, double vy0, double vz0)
+{
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+	DREAL site[27];
+	for (long z = -1; z <= Z; z++)
+		for (long y = -1; y <= Y; y++)
+			for (long x = -1; x <= X; x++) {
+				const bool interior = x >= 0 && x < X && y >= 0 && y < Y && z >= 0 && z < Z;
+				const long i = (z * Y + y) * X + x;
+				if (interior && rho)
+					eq_into<DREAL, EQ>(site, rho[i], vx[i], vy[i], vz[i]);
+				else
+					eq_into<DREAL, EQ>(site, rho0, vx0, vy0, vz0);
+				const long s = ((z + 1) * (Y + 2) + (y + 1)) * (X + 2) + (x + 1);
+				for (int q = 0; q < 27; q++)
+					f[q * XYZ + s] = site[q];
+			}
+	return 0;
+}
+
+template <typename DREAL, typename COLL>
+int collide_typed(long n, DREAL* f, DREAL* macro_out, double nu, double fx, double fy, double fz)
+{
+	for (long s = 0; s < n; s++) {
+		D3Q27_KernelStruct<DREAL> KS;
+		for (int q = 0; q < 27; q++)
+			KS.f[q] = f[s * 27 + q];
+		KS.lbmViscosity = (DREAL) nu;
+		KS.fx = (DREAL) fx;
+		KS.fy = (DREAL) fy;
+		KS.fz = (DREAL) fz;
+		COLL::computeDensityAndVelocity(KS);
+		if (macro_out) {
+			macro_out[s * 4 + 0] = KS.rho;
+			macro_out[s * 4 + 1] = KS.vx;
+			macro_out[s * 4 + 2] = KS.vy;
+			macro_out[s * 4 + 3] = KS.vz;
+		}
+		COLL::collision(KS);
+		for (int q = 0; q < 27; q++)
+			f[s * 27 + q] = KS.f[q];
+	}
+	return 0;
+}
+
+template <typename DREAL, typename EQ>
+int collide_dispatch(int coll, long n, void* f, void* m, double nu, double fx, double fy, double fz)
+{
+	using T = HarnessTraits<DREAL>;
+	switch (coll) {
+		case 0:
+			return collide_typed<DREAL, D3Q27_CUM<T, EQ>>(n, (DREAL*) f, (DREAL*) m, nu, fx, fy, fz);
+		case 1:
+			return collide_typed<DREAL, D3Q27_SRT<T, EQ>>(n, (DREAL*) f, (DREAL*) m, nu, fx, fy, fz);
+		case 2:
+			return collide_typed<DREAL, D3Q27_BGK<T, EQ>>(n, (DREAL*) f, (DREAL*) m, nu, fx, fy, fz);
+		case 3:
+			return collide_typed<DREAL, D3Q27_MRT<T, EQ>>(n, (DREAL*) f, (DREAL*) m, nu, fx, fy, fz);
+		default:
+			return -1;
+	}
+}
+
+}  // namespace
+
+extern "C" {
+
+// Flags this build was compiled with: bit0 USE_GEIER_CUM_2017, bit1 USE_GEIER_CUM_ANTIALIAS.
+int ref_cum_flags(void)
+{
+	int flags = 0;
+#ifdef USE_GEIER_CUM_2017
+	flags |= 1;
+#endif
+#ifdef USE_GEIER_CUM_ANTIALIAS
+	flags |= 2;
+#endif
+	return flags;
+}
+
+// prec: 0 = double, 1 = float.  coll: 0 CUM, 1 SRT, 2 BGK, 3 MRT.
+// eq: 0 = D3Q27_EQ (eq.h), 1 = D3Q27_EQ_INV_CUM (eq_inv_cum.h).
+// f: [27][Z+2][Y+2][X+2] (x fastest), updated in place.  map: [Z][Y][X] GEO values.
+// inflow profiles: [Z][Y] or NULL.  macro: [4][Z][Y][X] (rho, vx, vy, vz) or NULL.
+int ref_aa_run(int prec, int coll, int eq, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy,
+			   double fz, const double* vx, const double* vy, const double* vz, void* macro, long start_iter, int nsteps,
+			   int nthreads, double* elapsed_s)
+{
+	if (prec == 0) {
+		if (eq == 0)
+			return dispatch_coll<double, D3Q27_EQ<HarnessTraits<double>>>(coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro,
+																		  start_iter, nsteps, nthreads, elapsed_s);
+		return dispatch_coll<double, D3Q27_EQ_INV_CUM<HarnessTraits<double>>>(coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz,
+																			  macro, start_iter, nsteps, nthreads, elapsed_s);
+	}
+	if (eq == 0)
+		return dispatch_coll<float, D3Q27_EQ<HarnessTraits<float>>>(coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro,
+																	start_iter, nsteps, nthreads, elapsed_s);
+	return dispatch_coll<float, D3Q27_EQ_INV_CUM<HarnessTraits<float>>>(coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro,
+																		start_iter, nsteps, nthreads, elapsed_s);
+}
+
+// Equilibrium populations on every site incl. the ghost layer, as
+// LBM_BLOCK::setEquilibrium (lbm_block.hpp:248-278).  rho/vx/vy/vz are [Z][Y][X]
+// fields for the interior (or NULL for the uniform state rho0, v0).
+int ref_init_equilibrium(int prec, int eq, long X, long Y, long Z, void* f, const double* rho, const double* vx, const double* vy,
+						 const double* vz, double rho0, double vx0, double vy0, double vz0)
+{
+	if (prec == 0) {
+		if (eq == 0)
+			return init_eq_typed<double, D3Q27_EQ<HarnessTraits<double>>>(X, Y, Z, (double*) f, rho, vx, vy, vz, rho0, vx0, vy0, vz0);
+		return init_eq_typed<double, D3Q27_EQ_INV_CUM<HarnessTraits<double>>>(X, Y, Z, (double*) f, rho, vx, vy, vz, rho0, vx0, vy0,
+																			  vz0);
+	}
+	if (eq == 0)
+		return init_eq_typed<float, D3Q27_EQ<HarnessTraits<float>>>(X, Y, Z, (float*) f, rho, vx, vy, vz, rho0, vx0, vy0, vz0);
+	return init_eq_typed<float, D3Q27_EQ_INV_CUM<HarnessTraits<float>>>(X, Y, Z, (float*) f, rho, vx, vy, vz, rho0, vx0, vy0, vz0);
+}
+
+// Per-site collision: computeDensityAndVelocity (common.h:17-50) then
+// COLL::collision on n independent sites f[n][27]; macro_out[n][4] or NULL.
+int ref_collide(int prec, int coll, int eq, long n, void* f, void* macro_out, double nu, double fx, double fy, double fz)
+{
+	if (prec == 0) {
+		if (eq == 0)
+			return collide_dispatch<double, D3Q27_EQ<HarnessTraits<double>>>(coll, n, f, macro_out, nu, fx, fy, fz);
+		return collide_dispatch<double, D3Q27_EQ_INV_CUM<HarnessTraits<double>>>(coll, n, f, macro_out, nu, fx, fy, fz);
+	}
+	if (eq == 0)
+		return collide_dispatch<float, D3Q27_EQ<HarnessTraits<float>>>(coll, n, f, macro_out, nu, fx, fy, fz);
+	return collide_dispatch<float, D3Q27_EQ_INV_CUM<HarnessTraits<float>>>(coll, n, f, macro_out, nu, fx, fy, fz);
+}
+
+// Equilibrium of n sites, out[n][27].
+int ref_equilibrium(int prec, int eq, long n, const double* rho, const double* vx, const double* vy, const double* vz, void* out)
+{
+	for (long s = 0; s < n; s++) {
+		if (prec == 0) {
+			double* o = (double*) out + s * 27;
+			if (eq == 0)
+				eq_into<double, D3Q27_EQ<HarnessTraits<double>>>(o, rho[s], vx[s], vy[s], vz[s]);
+			else
+				eq_into<double, D3Q27_EQ_INV_CUM<HarnessTraits<double>>>(o, rho[s], vx[s], vy[s], vz[s]);
+		}
+		else {
+			float* o = (float*) out + s * 27;
+			if (eq == 0)
+				eq_into<float, D3Q27_EQ<HarnessTraits<float>>>(o, rho[s], vx[s], vy[s], vz[s]);
+			else
+				eq_into<float, D3Q27_EQ_INV_CUM<HarnessTraits<float>>>(o, rho[s], vx[s], vy[s], vz[s]);
+		}
+	}
+	return 0;
+}
+
+}  // extern "C"
