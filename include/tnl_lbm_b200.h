@@ -1,0 +1,191 @@
+/*
+ * tnl_lbm_b200.h -- C-ABI of the B200-native D3Q27 A-A hot path.
+ *
+ * This is the drop-in boundary for TNL-LBM's per-step update: the fused
+ * collision + A-A streaming kernel with the COLL / BC / MACRO plugins of
+ * LBM_CONFIG (include/lbm3d/defs.h:288-310, include/lbm3d/kernels.h:59-112)
+ * and the host-side pieces of the time loop that drive it.  Plain C types
+ * only: sizes, host pointers, device pointers as void*.  Every entry point
+ * returns an int status (LBM_OK = 0); lbm_last_error() describes the last
+ * failure of the calling thread.  A handle owns one lattice on one GPU with
+ * its own CUDA stream; calls on one handle are not thread-safe.
+ *
+ * Population slot order (q = 0..26) is the reference's direction enum
+ * (include/lbm3d/defs.h:318-350); map values are the GEO enum of
+ * D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43).  Arrays exchanged with the
+ * host are dense, C order, x fastest:
+ *   populations  [27][Z][Y][X]       (LBM_LAYOUT_INTERIOR)
+ *                [27][Z+2][Y+2][X+2] (LBM_LAYOUT_GHOST: incl. the ghost layer)
+ *   map          [Z][Y][X] uint8
+ *   macro        [4][Z][Y][X] double (rho, vx, vy, vz)
+ *   inflow       [Z][Y] double per velocity component
+ */
+#ifndef TNL_LBM_B200_H
+#define TNL_LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbm_lattice* lbm_handle;
+
+/* status codes */
+#define LBM_OK 0
+#define LBM_ERR_INVALID 1     /* bad argument or handle */
+#define LBM_ERR_UNSUPPORTED 2 /* combination not provided (e.g. a site type) */
+#define LBM_ERR_CUDA 3        /* CUDA runtime error */
+#define LBM_ERR_NONFINITE 4   /* non-finite density detected by a reduction */
+#define LBM_ERR_SIZE 5        /* size beyond a documented maximum */
+
+/* population storage in HBM */
+#define LBM_STORE_F64 0   /* double f_q */
+#define LBM_STORE_F32 1   /* float f_q */
+#define LBM_STORE_F32S 2  /* float f_q - w_q (shifted) */
+#define LBM_STORE_F16S 3  /* half (f_q - w_q) * 2^k_q, 2^k_q >= 1/w_q; FP32 arithmetic */
+#define LBM_STORE_BF16S 4 /* bfloat16 f_q - w_q; FP32 arithmetic */
+
+/* collision slot (COLL of LBM_CONFIG) */
+#define LBM_COLL_CUM 0 /* D3Q27_CUM, include/lbm3d/d3q27/col_cum.h */
+#define LBM_COLL_SRT 1 /* D3Q27_SRT, col_srt.h */
+#define LBM_COLL_BGK 2 /* D3Q27_BGK, col_bgk.h */
+#define LBM_COLL_MRT 3 /* D3Q27_MRT (MRT-LES), col_mrt.h */
+
+/* cumulant variant bits (USE_GEIER_CUM_2017, USE_GEIER_CUM_ANTIALIAS; defs.h:312-315).
+ * Valid sets: 0, ANTIALIAS, 2017|ANTIALIAS. */
+#define LBM_CUM_GEIER_2017 1
+#define LBM_CUM_ANTIALIAS 2
+
+/* equilibrium (EQ of LBM_CONFIG) */
+#define LBM_EQ_SECOND_ORDER 0 /* D3Q27_EQ, eq.h */
+#define LBM_EQ_INV_CUM 1      /* D3Q27_EQ_INV_CUM, eq_inv_cum.h */
+
+#define LBM_LAYOUT_INTERIOR 0
+#define LBM_LAYOUT_GHOST 1
+#define LBM_DTYPE_F64 0
+#define LBM_DTYPE_F32 1
+
+/* lbm_step flags: what the last of the requested steps also produces */
+#define LBM_STEP_MACRO 1  /* store rho, u (D3Q27_MACRO_Default::outputMacro, macro.h:70-76) */
+#define LBM_STEP_SUMS 2   /* FP64 sums of rho, rho*u, rho*|u|^2 and a non-finite count */
+
+typedef struct lbm_desc {
+	int32_t X, Y, Z;      /* lattice sites per axis (without the ghost layer) */
+	int32_t storage;      /* LBM_STORE_* */
+	int32_t collision;    /* LBM_COLL_* */
+	int32_t cum_flags;    /* LBM_CUM_* bits, cumulant only */
+	int32_t equilibrium;  /* LBM_EQ_*: SRT collision and equilibrium BCs */
+	int32_t periodic;     /* 1: every site GEO_PERIODIC and no map is used */
+	double viscosity;     /* lattice viscosity nu (LBM_Data::lbmViscosity) */
+	double fx, fy, fz;    /* homogeneous body force (NSE_Data::fx..fz, lbm_data.h:65-73) */
+	int32_t device;       /* CUDA device ordinal */
+	int32_t use_graphs;   /* 1: replay the time loop from captured CUDA graphs */
+} lbm_desc;
+
+/* Allocate a lattice (populations incl. a one-site ghost layer, map, macro).
+ * Replaces LBM_BLOCK::allocateDeviceData (include/lbm3d/lbm_block.hpp:549-617)
+ * together with the LBM_CONFIG composition (defs.h:288-310). */
+LBM_API int lbm_create(const lbm_desc* desc, lbm_handle* out);
+
+/* Release everything the handle owns. */
+LBM_API int lbm_destroy(lbm_handle h);
+
+/* Message of the last failed call on this thread (never NULL). */
+LBM_API const char* lbm_last_error(void);
+
+/* Per-site GEO types, host [Z][Y][X] uint8; required unless desc.periodic.
+ * Replaces LBM_BLOCK map setup + copyMapToDevice (lbm_block.hpp, state.hpp:1151-1232).
+ * Supported: GEO_FLUID, WALL, INFLOW, INFLOW_LEFT, INFLOW_EQ_LEFT, OUTFLOW_EQ,
+ * PERIODIC, NOTHING, SYM_TOP..SYM_FRONT.  Returns LBM_ERR_UNSUPPORTED for
+ * INFLOW_BB_LEFT, OUTFLOW_RIGHT, OUTFLOW_RIGHT_INTERP and the adjoint types. */
+LBM_API int lbm_set_map(lbm_handle h, const uint8_t* map);
+
+/* Inlet velocity profiles, host [Z][Y] doubles; NULL means zero.
+ * Replaces NSE_Data_InflowProfile (include/lbm3d/lbm_data.h:95-133). */
+LBM_API int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const double* vz);
+
+/* Change the lattice viscosity (State::updateKernelData, state.hpp:1627-1634). */
+LBM_API int lbm_set_viscosity(lbm_handle h, double nu);
+
+/* Equilibrium populations on every site incl. the ghost layer.  rho, vx, vy,
+ * vz: host [Z][Y][X] fields for the interior, or all NULL for the uniform
+ * state (rho0, v0), which also fills the ghost layer.
+ * Replaces LBM_BLOCK::setEquilibrium (lbm_block.hpp:248-278) and the
+ * setEquilibriumLat initialisers (common.h:127-158, sim_4.cu:126-171). */
+LBM_API int lbm_init_equilibrium(lbm_handle h, const double* rho, const double* vx, const double* vy, const double* vz,
+                         double rho0, double vx0, double vy0, double vz0);
+
+/* Taylor-Green vortex of sim_NSE/sim_4.cu:145-163 in lattice units:
+ * u = u0 sin(kx) cos(ky) cos(kz), v = -u0 (kx/ky) cos(kx) sin(ky) cos(kz), w = 0,
+ * rho = rho0 + 3 (u0^2/16) (cos 2kx + cos 2ky)(cos 2kz + 2) with k = 2 pi / N per
+ * axis at cell centres (i + 1/2 - N/2); the ghost layer gets (rho0, 0). */
+LBM_API int lbm_init_taylor_green(lbm_handle h, double u0, double rho0);
+
+/* Copy populations in / out (dtype LBM_DTYPE_*, layout LBM_LAYOUT_*).
+ * Values are f_q in slot order at the current A-A parity (after an odd number
+ * of steps the slots hold the streamed, swapped state of streaming_AA.h). */
+LBM_API int lbm_set_populations(lbm_handle h, const void* host, int layout, int dtype);
+LBM_API int lbm_get_populations(lbm_handle h, void* host, int layout, int dtype);
+
+/* Advance nsteps A-A steps (State::SimUpdate + LBM::updateKernelData,
+ * state.hpp:1235-1314, lbm.hpp:307-323).  The even/odd parity follows the
+ * handle's iteration counter.  flags (LBM_STEP_*) apply to the last step. */
+LBM_API int lbm_step(lbm_handle h, int64_t nsteps, int flags);
+
+/* Iteration counter (LBM::iterations); setting it changes the A-A parity. */
+LBM_API int64_t lbm_iteration(lbm_handle h);
+LBM_API int lbm_set_iteration(lbm_handle h, int64_t iteration);
+
+/* Macro field of the last step run with LBM_STEP_MACRO, host [4][Z][Y][X]. */
+LBM_API int lbm_get_macro(lbm_handle h, double* host);
+
+/* Sums of the last step run with LBM_STEP_SUMS: out[6] = {sum rho, sum rho vx,
+ * sum rho vy, sum rho vz, sum rho |u|^2, non-finite count}.  Returns
+ * LBM_ERR_NONFINITE when the count is non-zero (state.hpp:1469-1492). */
+LBM_API int lbm_get_sums(lbm_handle h, double* out);
+
+/* sum rho |grad u|^2 over the macro field of the last LBM_STEP_MACRO step with
+ * periodic central differences (sim_4.cu:21-54, :279-298). */
+LBM_API int lbm_enstrophy_sum(lbm_handle h, double* out);
+
+/* Wait for all work of the handle. */
+LBM_API int lbm_synchronize(lbm_handle h);
+
+/* Thread-block shape of the step kernels; (0,0) restores the default. */
+LBM_API int lbm_set_block(lbm_handle h, int bx, int by);
+LBM_API int lbm_get_block(lbm_handle h, int* bx, int* by);
+
+/* Time candidate block shapes on the current state (which is restored) and
+ * keep the fastest; ntrials steps per candidate.  Replaces the heuristic of
+ * get_optimal_block_size (include/lbm3d/block_size_optimizer.h:18-111). */
+LBM_API int lbm_autotune(lbm_handle h, int ntrials);
+
+/* Device view for zero-copy interop (pytnl_lbm): the population base pointer
+ * and strides in elements: index(q,x,y,z) = q*sq + (z+1)*sz + (y+1)*sy + x0 + x. */
+typedef struct lbm_device_view {
+	void* populations;
+	int64_t sq;
+	int32_t sy, sz, x0;
+	int32_t elem_size;
+	void* macro;        /* compute type [4][Z][Y][X] */
+	int32_t macro_elem_size;
+	void* stream;       /* cudaStream_t of the handle */
+} lbm_device_view;
+LBM_API int lbm_device_view_get(lbm_handle h, lbm_device_view* out);
+
+/* Library build information: sm architecture and version string. */
+LBM_API const char* lbm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TNL_LBM_B200_H */

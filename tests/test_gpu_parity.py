@@ -1,0 +1,269 @@
+"""GPU parity of the sm_100a A-A kernels against the oracle, through the C-ABI.
+
+Every case feeds the same seeded populations (ghost layer included) to the
+GPU lattice (pytnl_lbm -> libtnl_lbm_b200.so) and to the oracle port
+(oracle/lbm_oracle.c, itself pinned bit for bit to the reference's own
+per-site code by tests/test_oracle_golden.py), runs the same number of A-A
+steps and compares populations, macro fields and sums.
+
+Tolerances (relative L-infinity over all population slots):
+  FP64 storage  1e-12   (different FMA contraction and reciprocal use only)
+  FP32 storage  1e-5    (the north-star bound for populations in FP32)
+  kinetic energy        1e-12 (FP64), 1e-6 (FP32)
+"""
+import numpy as np
+import pytest
+
+from helpers import (COLL_IDS, EQ_IDS, GEO, duct_map, random_map, rel_linf, seeded_state, sym_box_map,
+                     tgv_fields)
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float64: 1e-12, np.float32: 1e-5}
+KE_TOL = {np.float64: 1e-12, np.float32: 1e-6}
+
+
+@pytest.fixture(scope="module")
+def pl():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import pytnl_lbm
+    return pytnl_lbm
+
+
+def storage_of(pl, dtype):
+    return pl.STORE_F64 if dtype == np.float64 else pl.STORE_F32
+
+
+def run_both(pl, port, f0, geo_map, *, coll="CUM", flags=0, eq="INV_CUM", nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
+             steps=2, dtype=np.float64, periodic=False, start_iter=0, use_graphs=True, storage=None):
+    Z, Y, X = geo_map.shape
+    lat = pl.LBM(X, Y, Z, viscosity=nu, collision=COLL_IDS[coll], cum_flags=flags, equilibrium=EQ_IDS[eq],
+                 storage=storage if storage is not None else storage_of(pl, dtype), periodic=periodic, force=force,
+                 use_graphs=use_graphs)
+    if not periodic:
+        lat.set_map(geo_map)
+    if inflow is not None:
+        lat.set_inflow(*inflow)
+    lat.set_populations(f0.astype(dtype))
+    lat.iteration = start_iter
+    lat.step(steps, macro=True, sums=True)
+    fg = lat.get_populations(dtype=np.float64)
+    mg = lat.macro()
+    sg = lat.sums()
+    fo = np.ascontiguousarray(f0.astype(dtype))
+    mo = np.zeros((4, Z, Y, X), dtype)
+    port.aa_run(fo, geo_map.astype(np.int16), coll=coll, eq=eq, cum_flags=flags, nu=nu, force=force, inflow=inflow,
+                macro=mo, start_iter=start_iter, nsteps=steps)
+    lat.close()
+    return fg, fo, mg, mo, sg
+
+
+def ke_of(macro):
+    m = macro.astype(np.float64)
+    return float((m[0] * (m[1] ** 2 + m[2] ** 2 + m[3] ** 2)).sum())
+
+
+CASES_PERIODIC = [("CUM", 0, "INV_CUM"), ("CUM", 2, "INV_CUM"), ("CUM", 3, "INV_CUM"), ("SRT", 0, "EQ"),
+                  ("SRT", 0, "INV_CUM"), ("BGK", 0, "EQ"), ("MRT", 0, "EQ")]
+
+
+@pytest.mark.parametrize("coll,flags,eq", CASES_PERIODIC)
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("steps", [2, 11, 100])
+def test_periodic_taylor_green_parity(pl, port, coll, flags, eq, dtype, steps):
+    X, Y, Z = 40, 24, 16  # anisotropic, X not a multiple of the block width
+    f0 = port.allocate(X, Y, Z)
+    port.init_equilibrium(f0, X, Y, Z, eq=eq, fields=tgv_fields(X, Y, Z, u0=0.05))
+    m = np.full((Z, Y, X), GEO["PERIODIC"], np.uint8)
+    force = (1e-6, -2e-6, 0.0) if coll != "CUM" else (0.0, 0.0, 0.0)
+    fg, fo, mg, mo, sg = run_both(pl, port, f0, m, coll=coll, flags=flags, eq=eq, nu=0.004, force=force, steps=steps,
+                                  dtype=dtype, periodic=True)
+    assert rel_linf(fg, fo) <= TOL[dtype] * (1 if steps < 100 else 4)
+    assert rel_linf(mg[0], mo[0]) <= TOL[dtype]
+    assert abs(sg[4] - ke_of(mo)) <= KE_TOL[dtype] * ke_of(mo) * (1 if steps < 100 else 4)
+    assert abs(sg[0] - mo[0].astype(np.float64).sum()) <= 1e-13 * X * Y * Z
+    assert sg[5] == 0
+
+
+MAPS = ["duct_left", "duct_inflow", "duct_eqleft", "sym", "random", "periodic_map"]
+
+
+def build_map(kind, rng, X, Y, Z):
+    if kind == "duct_left":
+        return duct_map(X, Y, Z, GEO["INFLOW_LEFT"], GEO["OUTFLOW_EQ"])
+    if kind == "duct_inflow":
+        return duct_map(X, Y, Z, GEO["INFLOW"], GEO["OUTFLOW_EQ"])
+    if kind == "duct_eqleft":
+        return duct_map(X, Y, Z, GEO["INFLOW_EQ_LEFT"], GEO["OUTFLOW_EQ"])
+    if kind == "sym":
+        return sym_box_map(X, Y, Z)
+    if kind == "random":
+        return random_map(rng, X, Y, Z)
+    return np.full((Z, Y, X), GEO["PERIODIC"], np.uint8)
+
+
+@pytest.mark.parametrize("kind", MAPS)
+@pytest.mark.parametrize("coll,flags,eq", [("CUM", 0, "INV_CUM"), ("CUM", 3, "INV_CUM"), ("SRT", 0, "EQ"),
+                                           ("BGK", 0, "EQ"), ("MRT", 0, "EQ")])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_boundary_conditions_parity(pl, port, kind, coll, flags, eq, dtype):
+    rng = np.random.default_rng(hash((kind, coll, flags)) % 2 ** 32)
+    X, Y, Z = 37, 12, 10
+    m = build_map(kind, rng, X, Y, Z)
+    f0 = seeded_state(port, rng, X, Y, Z, eq=eq)
+    prof = (0.02 * rng.random((Z, Y)), 0.004 * rng.random((Z, Y)), -0.003 * rng.random((Z, Y)))
+    fg, fo, mg, mo, sg = run_both(pl, port, f0, m, coll=coll, flags=flags, eq=eq, nu=0.02, force=(1e-5, 0.0, 2e-6),
+                                  inflow=prof, steps=9, dtype=dtype)
+    assert rel_linf(fg, fo) <= TOL[dtype]
+    np.testing.assert_allclose(mg, mo.astype(np.float64), rtol=TOL[dtype], atol=TOL[dtype] * 1e-2)
+
+
+@pytest.mark.parametrize("name", ["tgv_cum2017", "duct_cum", "duct_eq_cumaa", "sym_srt", "mix_bgk", "periodic_mrt"])
+def test_golden_vectors_on_gpu(pl, golden, name):
+    """The reference's own outputs (tests/golden) reproduced by the kernels in FP64."""
+    p = "lat_" + name
+    flags, coll, eq, nu, fx, fy, fz, steps = golden[p + "_params"]
+    f0 = golden[p + "_in"]
+    m = golden[p + "_map"].astype(np.uint8)
+    Z, Y, X = m.shape
+    prof = golden[p + "_inflow"]
+    lat = pl.LBM(X, Y, Z, viscosity=nu, collision=int(coll), cum_flags=int(flags), equilibrium=int(eq),
+                 storage=pl.STORE_F64, force=(fx, fy, fz))
+    lat.set_map(m)
+    lat.set_inflow(prof[0], prof[1], None)
+    lat.set_populations(f0)
+    lat.step(int(steps), macro=True)
+    assert rel_linf(lat.get_populations(), golden[p + "_out"]) <= 1e-12
+    np.testing.assert_allclose(lat.macro(), golden[p + "_macro"], rtol=1e-12, atol=1e-14)
+
+
+def test_golden_tgv16_kinetic_energy_on_gpu(pl, golden):
+    N = 16
+    lat = pl.LBM(N, N, N, viscosity=float(golden["tgv16_nu"]), collision=pl.COLL_CUM, cum_flags=3,
+                 equilibrium=pl.EQ_INV_CUM, storage=pl.STORE_F64, periodic=True)
+    lat.init_taylor_green(0.05, 1.0)
+    ke = []
+    for _ in range(10):
+        lat.step(2, sums=True)
+        ke.append(pl.kinetic_energy(lat))
+    np.testing.assert_allclose(ke, golden["tgv16_ke"], rtol=1e-12)
+
+
+def test_taylor_green_init_matches_oracle(pl, port):
+    X, Y, Z = 24, 20, 16
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, storage=pl.STORE_F64, periodic=True)
+    lat.init_taylor_green(0.05, 1.0)
+    f0 = port.allocate(X, Y, Z)
+    port.init_equilibrium(f0, X, Y, Z, eq="INV_CUM", fields=tgv_fields(X, Y, Z))
+    assert rel_linf(lat.get_populations(), f0) <= 1e-14
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_graph_replay_matches_direct_launches(pl, port, dtype):
+    X, Y, Z = 32, 16, 12
+    f0 = port.allocate(X, Y, Z)
+    port.init_equilibrium(f0, X, Y, Z, eq="INV_CUM", fields=tgv_fields(X, Y, Z))
+    out = []
+    for graphs in (True, False):
+        lat = pl.LBM(X, Y, Z, viscosity=0.003, cum_flags=3, storage=storage_of(pl, dtype), periodic=True,
+                     use_graphs=graphs)
+        lat.set_populations(f0.astype(dtype))
+        lat.step(1)        # odd start for the graph path
+        lat.step(37)       # two graph replays plus single steps
+        out.append(lat.get_populations())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_odd_start_iteration(pl, port):
+    rng = np.random.default_rng(5)
+    X, Y, Z = 20, 10, 8
+    m = duct_map(X, Y, Z)
+    f0 = seeded_state(port, rng, X, Y, Z)
+    fg, fo, mg, mo, sg = run_both(pl, port, f0, m, steps=5, start_iter=7, dtype=np.float64,
+                                  inflow=(0.01 * np.ones((Z, Y)), None, None))
+    assert rel_linf(fg, fo) <= 1e-12
+
+
+@pytest.mark.parametrize("storage,tol", [("F64", 0.0), ("F32", 0.0), ("F32S", 1e-7), ("F16S", 2e-3), ("BF16S", 2e-2)])
+def test_storage_roundtrip(pl, port, storage, tol):
+    rng = np.random.default_rng(9)
+    X, Y, Z = 33, 9, 7
+    f0 = seeded_state(port, rng, X, Y, Z)
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, storage=getattr(pl, "STORE_" + storage), periodic=True)
+    dtype = np.float64 if storage == "F64" else np.float32
+    lat.set_populations(f0.astype(dtype))
+    back = lat.get_populations(dtype=np.float64)
+    ref = f0.astype(dtype).astype(np.float64)
+    # deviations from the weights carry the quantisation, relative to |f - w|
+    err = np.abs(back - ref).max()
+    assert err <= tol * np.abs(f0).max() + (0 if tol == 0 else 1e-12)
+    for layout in (pl.LAYOUT_INTERIOR, pl.LAYOUT_GHOST):
+        got = lat.get_populations(layout=layout, dtype=np.float32)
+        assert got.shape == lat._pop_shape(layout)
+
+
+@pytest.mark.parametrize("storage,tol", [("F32S", 1e-5), ("F16S", 2e-3), ("BF16S", 2e-2)])
+def test_shifted_storage_follows_fp64(pl, storage, tol):
+    """Shifted low-precision storage with FP32 arithmetic against an FP64 run
+    of the same Taylor-Green vortex (kinetic energy after 200 steps)."""
+    N = 32
+    ke = {}
+    for st in ("F64", storage):
+        lat = pl.LBM(N, N, N, viscosity=0.05 * N / (2 * np.pi) / 400, cum_flags=3,
+                     storage=getattr(pl, "STORE_" + st), periodic=True)
+        lat.init_taylor_green(0.05, 1.0)
+        lat.step(200, sums=True)
+        ke[st] = pl.kinetic_energy(lat)
+    assert abs(ke[storage] / ke["F64"] - 1) <= tol
+
+
+def test_enstrophy_matches_macro_field(pl):
+    N = 24
+    lat = pl.LBM(N, N, N, viscosity=0.002, cum_flags=3, storage=pl.STORE_F64, periodic=True)
+    lat.init_taylor_green(0.05, 1.0)
+    lat.step(6, macro=True)
+    m = lat.macro()
+    g2 = 0
+    for c in (1, 2, 3):
+        for ax in (0, 1, 2):
+            d = 0.5 * (np.roll(m[c], -1, axis=ax) - np.roll(m[c], 1, axis=ax))
+            g2 = g2 + d * d
+    np.testing.assert_allclose(lat.enstrophy_sum(), (m[0] * g2).sum(), rtol=1e-12)
+
+
+def test_unsupported_site_types_are_rejected(pl):
+    lat = pl.LBM(8, 6, 5, viscosity=0.01)
+    for geo in (GEO["INFLOW_BB_LEFT"], GEO["OUTFLOW_RIGHT"], GEO["OUTFLOW_RIGHT_INTERP"], 17, 200):
+        m = np.zeros((5, 6, 8), np.uint8)
+        m[2, 3, 4] = geo
+        with pytest.raises(pl.LbmError) as e:
+            lat.set_map(m)
+        assert e.value.code == 2
+    with pytest.raises(pl.LbmError):
+        lat.step(1)  # no map has been accepted
+
+
+def test_autotune_restores_state(pl, port):
+    X, Y, Z = 64, 32, 16
+    lat = pl.LBM(X, Y, Z, viscosity=0.003, cum_flags=3, periodic=True)
+    lat.init_taylor_green(0.05)
+    before = lat.get_populations()
+    it = lat.iteration
+    bx, by = lat.autotune(2)
+    assert bx % 32 == 0 and bx * by <= 256
+    assert lat.iteration == it
+    assert np.array_equal(lat.get_populations(), before)
+
+
+def test_nonfinite_density_is_reported(pl):
+    lat = pl.LBM(16, 8, 8, viscosity=0.01, storage=pl.STORE_F64, periodic=True)
+    lat.init_equilibrium()
+    f = lat.get_populations()
+    f[0, 4, 4, 4] = np.nan
+    lat.set_populations(f)
+    lat.step(2, sums=True)
+    with pytest.raises(pl.LbmError) as e:
+        lat.sums()
+    assert e.value.code == 4

@@ -1,0 +1,342 @@
+// A-A stepping kernels for sm_100a (even and odd step of the fused
+// stream + boundary + collide update), initialisation, layout conversion and
+// the FP64 reductions.
+//
+// Data layout in HBM (one allocation per lattice):
+//   populations  slot-major SoA: index(q, x, y, z) = q*sq + (z+1)*sz + (y+1)*sy + x0 + x
+//                x fastest.  One ghost layer of sites surrounds the lattice
+//                (x = -1 .. X, y = -1 .. Y, z = -1 .. Z), which the reference's
+//                A-A kernel assumes (include/lbm3d/kernels.h:30-37).  x0 pads
+//                the row so that interior x = 0 starts on a 128-byte boundary;
+//                sy is a multiple of 128 bytes, so every row of every
+//                direction is a coalesced, 128-byte-aligned stream.
+//   map          uint8 [Z][Y][X] GEO values (general kernels only)
+//   macro        compute type [4][Z][Y][X] (rho, vx, vy, vz)
+//
+// A-A pattern (include/lbm3d/d3q27/streaming_AA.h:12-116):
+//   even step  read slot q of the site, write direction q into slot opp(q)
+//              of the same site;
+//   odd step   read direction q from slot opp(q) of site x - c_q, write
+//              direction q into slot q of site x + c_q.
+// In both steps a thread writes exactly the 27 locations it read, and no
+// other thread touches them, so the update runs in place without races.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
+
+#include "collision.cuh"
+
+namespace lbm {
+
+template <int... Is, typename F>
+__device__ __forceinline__ void static_for_impl(std::integer_sequence<int, Is...>, F&& f)
+{
+	(f(std::integral_constant<int, Is>{}), ...);
+}
+// compile-time loop: f receives std::integral_constant<int, i> for i = 0..N-1
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+	static_for_impl(std::make_integer_sequence<int, N>{}, f);
+}
+
+// number of FP64 reduction quantities per block: sum rho, rho*vx, rho*vy,
+// rho*vz, rho*|u|^2 and the count of non-finite densities
+constexpr int NRED = 6;
+
+template <typename T, typename R>
+struct StepArgs
+{
+	T* f;
+	long long sq;
+	int sy, sz, x0;
+	int X, Y, Z;
+	const uint8_t* map;	 // general kernels only
+	const R* in_vx;
+	const R* in_vy;
+	const R* in_vz;
+	R* macro;		   // [4][Z][Y][X] or null
+	double* partials;  // [blocks][NRED] or null
+	CollParams<R> p;
+};
+
+// Offsets (in elements) of the neighbour sites; periodic sites wrap, all
+// other sites reach into the ghost layer (kernels.h:21-37).
+struct Offsets
+{
+	long long x[3], y[3], z[3];
+};
+
+__device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, int z, int X, int Y, int Z, int sy, int sz)
+{
+	Offsets o;
+	o.x[0] = (wrap && x == 0) ? (X - 1) : -1;
+	o.x[1] = 0;
+	o.x[2] = (wrap && x == X - 1) ? -(X - 1) : 1;
+	o.y[0] = (long long) ((wrap && y == 0) ? (Y - 1) : -1) * sy;
+	o.y[1] = 0;
+	o.y[2] = (long long) ((wrap && y == Y - 1) ? -(Y - 1) : 1) * sy;
+	o.z[0] = (long long) ((wrap && z == 0) ? (Z - 1) : -1) * sz;
+	o.z[1] = 0;
+	o.z[2] = (long long) ((wrap && z == Z - 1) ? -(Z - 1) : 1) * sz;
+	return o;
+}
+
+// A-A read of the 27 populations (streaming_AA.h:79-116)
+template <typename S, bool ODD>
+__device__ __forceinline__ void aa_read(const typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
+										typename S::R* v)
+{
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (ODD)
+				v[q] = S::template load<opp(q)>(f + opp(q) * sq + base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]);
+			else
+				v[q] = S::template load<q>(f + q * sq + base);
+		}
+	);
+}
+
+// A-A write of the 27 populations (streaming_AA.h:12-76)
+template <typename S, bool ODD>
+__device__ __forceinline__ void aa_write(typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
+										 const typename S::R* v)
+{
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (ODD)
+				S::template store<q>(f + q * sq + base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)], v[q]);
+			else
+				S::template store<opp(q)>(f + opp(q) * sq + base, v[q]);
+		}
+	);
+}
+
+// mirror copy of a symmetry plane: directions whose AXIS component equals
+// SIDE take the value of their mirror image (bc.h:222-293)
+template <int AXIS, int SIDE, typename R>
+__device__ __forceinline__ void symmetry(R* f)
+{
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			constexpr int c = AXIS == 0 ? cx(q) : (AXIS == 1 ? cy(q) : cz(q));
+			if constexpr (c == SIDE) {
+				constexpr int m = dir(AXIS == 0 ? -cx(q) : cx(q), AXIS == 1 ? -cy(q) : cy(q), AXIS == 2 ? -cz(q) : cz(q));
+				f[q] = f[m];
+			}
+		}
+	);
+}
+
+// density of a left inlet from the populations that stream in from the
+// interior (bc.h:97-110)
+template <typename R>
+__device__ __forceinline__ R inlet_density(const R* f, R vx)
+{
+	return R(1) / (R(1) - vx)
+		 * ((f[ZZZ] + (((f[ZPP] + f[ZMM]) + (f[ZPM] + f[ZMP])) + ((f[ZPZ] + f[ZMZ]) + (f[ZZP] + f[ZZM]))))
+			+ R(2) * (f[MZZ] + (((f[MPP] + f[MMM]) + (f[MPM] + f[MMP])) + ((f[MPZ] + f[MMZ]) + (f[MZP] + f[MZM])))));
+}
+
+// moment-based velocity inlet of Eichler et al. (bc.h:91-142)
+template <typename R>
+__device__ __forceinline__ void inlet_moments(Site<R>& s)
+{
+	R* f = s.f;
+	s.rho = inlet_density(f, s.vx);
+	const R rho = s.rho, vx = s.vx, vy = s.vy, vz = s.vz;
+	const R third = R(1.0 / 3.0), ninth = R(1.0 / 9.0);
+	const R m100 = rho * vx, m010 = rho * vy, m001 = rho * vz;
+	const R m011 = rho * (vy * vz);
+	const R m020 = third * rho + rho * (vy * vy);
+	const R m002 = third * rho + rho * (vz * vz);
+	const R m021 = third * rho * vz + rho * ((vy * vy) * vz);
+	const R m012 = third * rho * vy + rho * (vy * (vz * vz));
+	const R m022 = ninth * rho + third * rho * (vy * vy + vz * vz) + rho * (vy * vy) * (vz * vz);
+	f[PZZ] = m100 + (m022 - (m020 + m002)) + f[MZZ] + (((f[ZPP] + f[ZMM]) + (f[ZPM] + f[ZMP])) + ((f[ZZP] + f[ZZM]) + (f[ZPZ] + f[ZMZ])))
+		   + R(2) * (((f[MPP] + f[MMM]) + (f[MPM] + f[MMP])) + ((f[MPZ] + f[MMZ]) + (f[MZP] + f[MZM])));
+	f[PPZ] = R(0.5) * ((m020 - m022) + (m010 - m012)) - (f[MPZ] + f[ZPZ]);
+	f[PMZ] = R(0.5) * ((m020 - m022) + (m012 - m010)) - (f[MMZ] + f[ZMZ]);
+	f[PZP] = R(0.5) * ((m002 - m022) + (m001 - m021)) - (f[MZP] + f[ZZP]);
+	f[PZM] = R(0.5) * ((m002 - m022) + (m021 - m001)) - (f[MZM] + f[ZZM]);
+	f[PPP] = R(0.25) * ((m022 + m011) + (m021 + m012)) - (f[MPP] + f[ZPP]);
+	f[PPM] = R(0.25) * ((m022 - m011) + (m012 - m021)) - (f[MPM] + f[ZPM]);
+	f[PMP] = R(0.25) * ((m022 - m011) + (m021 - m012)) - (f[MMP] + f[ZMP]);
+	f[PMM] = R(0.25) * ((m022 + m011) - (m021 + m012)) - (f[MMM] + f[ZMM]);
+}
+
+template <typename R>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* partials)
+{
+	// warp level
+#pragma unroll
+	for (int k = 0; k < NRED; k++)
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1)
+			v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+	__shared__ double red[32][NRED];
+	const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+	const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+	const int lane = tid & 31, warp = tid >> 5, nwarps = (nthreads + 31) >> 5;
+	if (lane == 0)
+#pragma unroll
+		for (int k = 0; k < NRED; k++)
+			red[warp][k] = v[k];
+	__syncthreads();
+	if (tid < NRED) {
+		double acc = 0;
+		for (int w = 0; w < nwarps; w++)
+			acc += red[w][tid];
+		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
+		partials[block * NRED + tid] = acc;
+	}
+}
+
+// One A-A step over the whole lattice.  GENERAL = false: every site is
+// periodic (no map read).  GENERAL = true: per-site GEO type from the map with
+// the boundary conditions of D3Q27_BC_All (bc.h:60-422) that are free of
+// cross-site ordering in the A-A pattern.
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, int MINB>
+__global__ void __launch_bounds__(256, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
+{
+	using R = typename S::R;
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int y = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	const bool active = x < a.X && y < a.Y;
+
+	double red[NRED] = {0, 0, 0, 0, 0, 0};
+	if (active) {
+		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+		const long long site = ((long long) z * a.Y + y) * a.X + x;
+		uint8_t geo = GEO_PERIODIC;
+		if constexpr (GENERAL)
+			geo = a.map[site];
+		Site<R> s;
+		bool store = true;
+		if (GENERAL && geo == GEO_NOTHING) {
+			s.rho = R(1);
+			s.vx = s.vy = s.vz = R(0);
+			store = false;
+		}
+		else {
+			const Offsets o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+			bool coll = true;
+			if constexpr (GENERAL) {
+				const long long prof = (long long) z * a.Y + y;
+				switch (geo) {
+					case GEO_INFLOW:
+						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+						s.rho = R(1);
+						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+						coll = false;
+						break;
+					case GEO_INFLOW_LEFT:
+						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+						inlet_moments(s);
+						s.ir = rcp(s.rho);
+						break;
+					case GEO_INFLOW_EQ_LEFT:
+						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+						s.rho = inlet_density(s.f, s.vx);
+						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+						coll = false;
+						break;
+					case GEO_OUTFLOW_EQ:
+						density_velocity(s, a.p);
+						s.rho = R(1);
+						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+						coll = false;
+						break;
+					case GEO_WALL:
+						// full-way bounce-back (bc.h:201-221)
+						s.rho = R(1);
+						s.vx = s.vy = s.vz = R(0);
+#pragma unroll
+						for (int q = 1; q < 27; q += 2) {
+							const R t = s.f[q];
+							s.f[q] = s.f[q + 1];
+							s.f[q + 1] = t;
+						}
+						coll = false;
+						break;
+					case GEO_SYM_TOP:
+						symmetry<2, -1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					case GEO_SYM_BOTTOM:
+						symmetry<2, 1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					case GEO_SYM_LEFT:
+						symmetry<0, 1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					case GEO_SYM_RIGHT:
+						symmetry<0, -1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					case GEO_SYM_BACK:
+						symmetry<1, 1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					case GEO_SYM_FRONT:
+						symmetry<1, -1>(s.f);
+						density_velocity(s, a.p);
+						coll = false;
+						break;
+					default:  // GEO_FLUID, GEO_PERIODIC
+						density_velocity(s, a.p);
+						break;
+				}
+			}
+			else {
+				density_velocity(s, a.p);
+			}
+			if (coll)
+				collide<R, COLL, CUMF>(s, a.p);
+			aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+		}
+		(void) store;
+		if (a.macro) {
+			const long long n = (long long) a.X * a.Y * a.Z;
+			a.macro[site] = s.rho;
+			a.macro[n + site] = s.vx;
+			a.macro[2 * n + site] = s.vy;
+			a.macro[3 * n + site] = s.vz;
+		}
+		if (a.partials) {
+			const double rho = (double) s.rho, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
+			red[0] = rho;
+			red[1] = rho * vx;
+			red[2] = rho * vy;
+			red[3] = rho * vz;
+			red[4] = rho * (vx * vx + vy * vy + vz * vz);
+			red[5] = isfinite(rho) ? 0.0 : 1.0;
+		}
+	}
+	if (a.partials)
+		block_reduce_store<R>(red, a.partials);
+}
+
+}  // namespace lbm

@@ -1,0 +1,5 @@
+// Kernel instantiations for the f16s population storage (StoreF16S).
+#define LBM_STORE_MINB 2
+#include "aa_store_impl.cuh"
+
+LBM_DEFINE_STORAGE_OPS(storage_ops_f16s, StoreF16S, "f16s")

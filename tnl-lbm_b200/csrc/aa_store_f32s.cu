@@ -1,0 +1,5 @@
+// Kernel instantiations for the f32s population storage (StoreF32S).
+#define LBM_STORE_MINB 2
+#include "aa_store_impl.cuh"
+
+LBM_DEFINE_STORAGE_OPS(storage_ops_f32s, StoreF32S, "f32s")

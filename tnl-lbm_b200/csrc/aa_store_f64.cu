@@ -1,0 +1,5 @@
+// Kernel instantiations for the f64 population storage (StoreF64).
+#define LBM_STORE_MINB 1
+#include "aa_store_impl.cuh"
+
+LBM_DEFINE_STORAGE_OPS(storage_ops_f64, StoreF64, "f64")

@@ -1,0 +1,241 @@
+// Kernel instantiations for one population storage format.  Included by
+// aa_store_<format>.cu with LBM_STORE (the StoreXXX type), LBM_STORE_NAME and
+// LBM_STORE_MINB (min resident blocks in __launch_bounds__) defined.
+#pragma once
+
+#include "aa_kernels.cuh"
+#include "launch.h"
+
+namespace lbm {
+
+template <typename R>
+inline CollParams<R> make_coll_params(const CollParamsD& d)
+{
+	CollParams<R> p{};
+	const double w1 = d.w1;
+	const double g = 1.0 / w1 - 0.5;
+	p.nu = (R) d.nu;
+	p.fx = (R) d.fx;
+	p.fy = (R) d.fy;
+	p.fz = (R) d.fz;
+	p.hfx = (R) (0.5 * d.fx);
+	p.hfy = (R) (0.5 * d.fy);
+	p.hfz = (R) (0.5 * d.fz);
+	p.w1 = (R) w1;
+	p.one_m_w1 = (R) (1.0 - w1);
+	p.k33 = (R) (3.0 * (1.0 - 0.5 * w1));
+	p.hw1 = (R) (0.5 * w1);
+	p.w1_3h = (R) (1.5 * w1);
+	p.w1_3 = (R) (3.0 * w1);
+	p.w3 = (R) d.w3;
+	p.w4 = (R) d.w4;
+	p.w5 = (R) d.w5;
+	p.c43 = (R) (2.0 / 3.0 * g * d.A);
+	p.c45 = (R) (-4.0 / 3.0 * g * d.A);
+	p.cB = (R) (-1.0 / 3.0 * g * d.B);
+	p.inv_tau = (R) (1.0 / d.tau);
+	p.srt_force = (R) (1.0 - 0.5 / d.tau);
+	p.bgk_force = (R) (1.0 - 0.5 * w1);
+	p.tau = (R) d.tau;
+	p.tau2 = (R) (d.tau * d.tau);
+	p.eq = d.eq;
+	return p;
+}
+
+template <typename S>
+struct StorageUnit
+{
+	using T = typename S::T;
+	using R = typename S::R;
+
+	template <int COLL, int CUMF, bool ODD, bool GENERAL>
+	static cudaError_t launch_one(const StepLaunch& L, const StepArgs<T, R>& a)
+	{
+		aa_step_kernel<S, COLL, CUMF, ODD, GENERAL, LBM_STORE_MINB><<<L.grid, L.block, 0, L.stream>>>(a);
+		return cudaGetLastError();
+	}
+
+	template <int COLL, int CUMF>
+	static cudaError_t launch_parity(const StepLaunch& L, const StepArgs<T, R>& a)
+	{
+		const bool general = L.map != nullptr;
+		if (L.odd)
+			return general ? launch_one<COLL, CUMF, true, true>(L, a) : launch_one<COLL, CUMF, true, false>(L, a);
+		return general ? launch_one<COLL, CUMF, false, true>(L, a) : launch_one<COLL, CUMF, false, false>(L, a);
+	}
+
+	static cudaError_t step(const StepLaunch& L)
+	{
+		StepArgs<T, R> a;
+		a.f = (T*) L.g.f;
+		a.sq = L.g.sq;
+		a.sy = L.g.sy;
+		a.sz = L.g.sz;
+		a.x0 = L.g.x0;
+		a.X = L.g.X;
+		a.Y = L.g.Y;
+		a.Z = L.g.Z;
+		a.map = L.map;
+		a.in_vx = (const R*) L.inflow[0];
+		a.in_vy = (const R*) L.inflow[1];
+		a.in_vz = (const R*) L.inflow[2];
+		a.macro = (R*) L.macro;
+		a.partials = L.partials;
+		a.p = make_coll_params<R>(L.p);
+		switch (L.coll) {
+			case COLL_CUM:
+				switch (L.cum_flags) {
+					case 0:
+						return launch_parity<COLL_CUM, 0>(L, a);
+					case CUM_ANTIALIAS:
+						return launch_parity<COLL_CUM, CUM_ANTIALIAS>(L, a);
+					case CUM_2017 | CUM_ANTIALIAS:
+						return launch_parity<COLL_CUM, CUM_2017 | CUM_ANTIALIAS>(L, a);
+					default:
+						return cudaErrorInvalidValue;
+				}
+			case COLL_SRT:
+				return launch_parity<COLL_SRT, 0>(L, a);
+			case COLL_BGK:
+				return launch_parity<COLL_BGK, 0>(L, a);
+			case COLL_MRT:
+				return launch_parity<COLL_MRT, 0>(L, a);
+			default:
+				return cudaErrorInvalidValue;
+		}
+	}
+
+	static cudaError_t init_eq(const Geometry& g, const InitSpec& spec, cudaStream_t st);
+	static cudaError_t pack(const Geometry& g, void* dense, int dtype, int ghost, cudaStream_t st);
+	static cudaError_t unpack(const Geometry& g, const void* dense, int dtype, int ghost, cudaStream_t st);
+};
+
+// equilibrium everywhere incl. the ghost layer (lbm_block.hpp:248-278); one
+// thread per site of the (X+2)(Y+2)(Z+2) box.  The Taylor-Green field follows
+// sim_NSE/sim_4.cu:145-163 at cell centres (i + 1/2 - N/2) with k = 2 pi / N.
+template <typename S>
+__global__ void init_eq_kernel(Geometry g, InitSpec spec)
+{
+	using R = typename S::R;
+	using T = typename S::T;
+	const long long nx = g.X + 2, ny = g.Y + 2, nz = g.Z + 2;
+	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+	if (i >= nx * ny * nz)
+		return;
+	const int x = (int) (i % nx) - 1;
+	const int y = (int) ((i / nx) % ny) - 1;
+	const int z = (int) (i / (nx * ny)) - 1;
+	const bool interior = x >= 0 && x < g.X && y >= 0 && y < g.Y && z >= 0 && z < g.Z;
+	double r = spec.rho0, u = spec.vx0, v = spec.vy0, w = spec.vz0;
+	if (interior && spec.mode == 1) {
+		const long long s = ((long long) z * g.Y + y) * g.X + x;
+		r = spec.rho[s];
+		u = spec.vx[s];
+		v = spec.vy[s];
+		w = spec.vz[s];
+	}
+	else if (interior && spec.mode == 2) {
+		const double pi = 3.14159265358979323846;
+		const double kx = 2 * pi / g.X, ky = 2 * pi / g.Y, kz = 2 * pi / g.Z;
+		const double px = kx * (x + 0.5 - 0.5 * g.X), py = ky * (y + 0.5 - 0.5 * g.Y), pz = kz * (z + 0.5 - 0.5 * g.Z);
+		const double u0 = spec.u0;
+		u = u0 * sin(px) * cos(py) * cos(pz);
+		v = -u0 * (kx / ky) * cos(px) * sin(py) * cos(pz);
+		w = 0;
+		r = spec.rho0 + 3 * (u0 * u0 / 16) * (cos(2 * px) + cos(2 * py)) * (cos(2 * pz) + 2);
+	}
+	else if (spec.mode == 2) {
+		u = v = w = 0;
+	}
+	R f[27];
+	set_equilibrium<R>(f, spec.eq, (R) r, (R) u, (R) v, (R) w);
+	T* base = (T*) g.f + (long long) (z + 1) * g.sz + (long long) (y + 1) * g.sy + g.x0 + x;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			S::template store<q>(base + q * g.sq, f[q]);
+		}
+	);
+}
+
+// dense [27][nz][ny][nx] <-> storage
+template <typename S, typename D, bool TO_DENSE>
+__global__ void convert_kernel(Geometry g, D* dense, int ghost)
+{
+	using T = typename S::T;
+	const int gh = ghost ? 1 : 0;
+	const long long nx = g.X + 2 * gh, ny = g.Y + 2 * gh, nz = g.Z + 2 * gh;
+	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+	if (i >= nx * ny * nz)
+		return;
+	const int x = (int) (i % nx) - gh;
+	const int y = (int) ((i / nx) % ny) - gh;
+	const int z = (int) (i / (nx * ny)) - gh;
+	T* base = (T*) g.f + (long long) (z + 1) * g.sz + (long long) (y + 1) * g.sy + g.x0 + x;
+	const long long n = nx * ny * nz;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (TO_DENSE)
+				dense[q * n + i] = (D) S::template load<q>(base + q * g.sq);
+			else
+				S::template store<q>(base + q * g.sq, (typename S::R) dense[q * n + i]);
+		}
+	);
+}
+
+template <typename S>
+cudaError_t StorageUnit<S>::init_eq(const Geometry& g, const InitSpec& spec, cudaStream_t st)
+{
+	const long long n = (long long) (g.X + 2) * (g.Y + 2) * (g.Z + 2);
+	const int bs = 128;
+	init_eq_kernel<S><<<(unsigned) ((n + bs - 1) / bs), bs, 0, st>>>(g, spec);
+	return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t StorageUnit<S>::pack(const Geometry& g, void* dense, int dtype, int ghost, cudaStream_t st)
+{
+	const int gh = ghost ? 1 : 0;
+	const long long n = (long long) (g.X + 2 * gh) * (g.Y + 2 * gh) * (g.Z + 2 * gh);
+	const int bs = 128;
+	const unsigned nb = (unsigned) ((n + bs - 1) / bs);
+	if (dtype == 0)
+		convert_kernel<S, double, true><<<nb, bs, 0, st>>>(g, (double*) dense, ghost);
+	else
+		convert_kernel<S, float, true><<<nb, bs, 0, st>>>(g, (float*) dense, ghost);
+	return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t StorageUnit<S>::unpack(const Geometry& g, const void* dense, int dtype, int ghost, cudaStream_t st)
+{
+	const int gh = ghost ? 1 : 0;
+	const long long n = (long long) (g.X + 2 * gh) * (g.Y + 2 * gh) * (g.Z + 2 * gh);
+	const int bs = 128;
+	const unsigned nb = (unsigned) ((n + bs - 1) / bs);
+	if (dtype == 0)
+		convert_kernel<S, double, false><<<nb, bs, 0, st>>>(g, (double*) dense, ghost);
+	else
+		convert_kernel<S, float, false><<<nb, bs, 0, st>>>(g, (float*) dense, ghost);
+	return cudaGetLastError();
+}
+
+}  // namespace lbm
+
+#define LBM_DEFINE_STORAGE_OPS(FN, S, NAME)                                                                          \
+	namespace lbm {                                                                                                  \
+	const StorageOps& FN()                                                                                           \
+	{                                                                                                                \
+		static const StorageOps ops = {&StorageUnit<S>::step,                                                        \
+									   &StorageUnit<S>::init_eq,                                                     \
+									   &StorageUnit<S>::pack,                                                        \
+									   &StorageUnit<S>::unpack,                                                      \
+									   (int) sizeof(typename S::R),                                                  \
+									   (int) sizeof(typename S::T),                                                  \
+									   NAME};                                                                        \
+		return ops;                                                                                                  \
+	}                                                                                                                \
+	}

@@ -1,0 +1,187 @@
+// D3Q27 lattice constants and population storage formats for the sm_100a
+// kernels.
+//
+// Direction numbering is the slot order of TNL-LBM's population arrays
+// (include/lbm3d/defs.h:318-350): zzz, pzz, mzz, zpz, zmz, zzp, zzm, ppz,
+// mmz, pmz, mpz, pzp, mzm, pzm, mzp, zpp, zmm, zpm, zmp, ppp, mmm, ppm, mmp,
+// pmp, mpm, pmm, mpp.  Opposite directions are adjacent pairs (1,2), (3,4), ...
+#pragma once
+
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace lbm {
+
+enum Dir : int
+{
+	ZZZ, PZZ, MZZ, ZPZ, ZMZ, ZZP, ZZM, PPZ, MMZ, PMZ, MPZ, PZP, MZM, PZM, MZP,
+	ZPP, ZMM, ZPM, ZMP, PPP, MMM, PPM, MMP, PMP, MPM, PMM, MPP
+};
+
+__host__ __device__ constexpr int cx(int q)
+{
+	constexpr int t[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+	return t[q];
+}
+__host__ __device__ constexpr int cy(int q)
+{
+	constexpr int t[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
+	return t[q];
+}
+__host__ __device__ constexpr int cz(int q)
+{
+	constexpr int t[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1};
+	return t[q];
+}
+__host__ __device__ constexpr int opp(int q)
+{
+	return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1);
+}
+// number of non-zero velocity components: 0 rest, 1 face, 2 edge, 3 corner
+__host__ __device__ constexpr int nnz(int q)
+{
+	return (cx(q) != 0) + (cy(q) != 0) + (cz(q) != 0);
+}
+// direction index from components (used with compile-time arguments)
+__host__ __device__ constexpr int dir(int x, int y, int z)
+{
+	int r = -1;
+	for (int q = 0; q < 27; q++)
+		if (cx(q) == x && cy(q) == y && cz(q) == z)
+			r = q;
+	return r;
+}
+// lattice weights w_q
+__host__ __device__ constexpr double weight(int q)
+{
+	return nnz(q) == 0 ? 8.0 / 27.0 : nnz(q) == 1 ? 2.0 / 27.0 : nnz(q) == 2 ? 1.0 / 54.0 : 1.0 / 216.0;
+}
+// exact power-of-two scale applied to the FP16 deviations: the smallest 2^k
+// with 2^k >= 1/w_q, so that (f_q - w_q) * 2^k stays in FP16's normal range
+__host__ __device__ constexpr float half_scale(int q)
+{
+	return nnz(q) == 0 ? 4.0f : nnz(q) == 1 ? 16.0f : nnz(q) == 2 ? 64.0f : 256.0f;
+}
+
+// GEO site types of D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43); the map
+// stores these values as uint8
+enum Geo : uint8_t
+{
+	GEO_FLUID = 0,
+	GEO_WALL = 1,
+	GEO_INFLOW = 2,
+	GEO_INFLOW_LEFT = 3,
+	GEO_INFLOW_BB_LEFT = 4,
+	GEO_INFLOW_EQ_LEFT = 5,
+	GEO_OUTFLOW_EQ = 6,
+	GEO_OUTFLOW_RIGHT = 7,
+	GEO_OUTFLOW_RIGHT_INTERP = 8,
+	GEO_PERIODIC = 9,
+	GEO_NOTHING = 10,
+	GEO_SYM_TOP = 11,
+	GEO_SYM_BOTTOM = 12,
+	GEO_SYM_LEFT = 13,
+	GEO_SYM_RIGHT = 14,
+	GEO_SYM_BACK = 15,
+	GEO_SYM_FRONT = 16,
+};
+
+// ---------------------------------------------------------------------------
+// population storage formats
+//   F64   double  f_q
+//   F32   float   f_q
+//   F32S  float   f_q - w_q
+//   F16S  half    (f_q - w_q) * half_scale(q)
+//   BF16S bf16    f_q - w_q
+// Every format is read into the compute type R and written back from it.
+// ---------------------------------------------------------------------------
+struct StoreF64
+{
+	using T = double;
+	using R = double;
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		return __ldcs(p);
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		__stcs(p, v);
+	}
+};
+
+struct StoreF32
+{
+	using T = float;
+	using R = float;
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		return __ldcs(p);
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		__stcs(p, v);
+	}
+};
+
+struct StoreF32S
+{
+	using T = float;
+	using R = float;
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		return __ldcs(p) + (float) weight(Q);
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		__stcs(p, v - (float) weight(Q));
+	}
+};
+
+struct StoreF16S
+{
+	using T = __half;
+	using R = float;
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		const unsigned short raw = __ldcs(reinterpret_cast<const unsigned short*>(p));
+		return __half2float(__ushort_as_half(raw)) * (1.0f / half_scale(Q)) + (float) weight(Q);
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		const __half h = __float2half_rn((v - (float) weight(Q)) * half_scale(Q));
+		__stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
+	}
+};
+
+struct StoreBF16S
+{
+	using T = __nv_bfloat16;
+	using R = float;
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		const unsigned short raw = __ldcs(reinterpret_cast<const unsigned short*>(p));
+		return __bfloat162float(__ushort_as_bfloat16(raw)) + (float) weight(Q);
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		const __nv_bfloat16 h = __float2bfloat16_rn(v - (float) weight(Q));
+		__stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(h));
+	}
+};
+
+// host-side conversions of the same formats (set/get of populations)
+template <typename S>
+struct HostConv;
+
+}  // namespace lbm

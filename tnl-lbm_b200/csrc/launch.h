@@ -1,0 +1,90 @@
+// Internal launch interface between the C-ABI (lbm_abi.cu) and the kernel
+// instantiations, one translation unit per population storage format
+// (aa_store_*.cu).  Arguments are type-erased here and converted to the
+// storage's compute type inside each unit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lbm {
+
+enum Storage : int
+{
+	ST_F64 = 0,
+	ST_F32 = 1,
+	ST_F32S = 2,
+	ST_F16S = 3,
+	ST_BF16S = 4,
+	ST_COUNT = 5
+};
+
+// collision-slot constants in double; each unit casts them to its compute type
+struct CollParamsD
+{
+	double nu, fx, fy, fz;
+	double w1, w3, w4, w5, A, B;
+	double tau;
+	int eq;
+};
+
+struct Geometry
+{
+	void* f;		  // population storage (element 0 of the allocation)
+	long long sq;	  // direction stride in elements
+	int sy, sz, x0;	  // row stride, plane stride, interior x offset (elements)
+	int X, Y, Z;
+};
+
+// initial state: mode 0 uniform (rho0, v0) everywhere; mode 1 device double
+// [Z][Y][X] fields for the interior, uniform state in the ghost layer; mode 2
+// Taylor-Green vortex of amplitude u0 around rho0 (ghost layer: rho0, 0)
+struct InitSpec
+{
+	int mode;
+	int eq;
+	const double *rho, *vx, *vy, *vz;
+	double rho0, vx0, vy0, vz0;
+	double u0;
+};
+
+struct StepLaunch
+{
+	Geometry g;
+	const uint8_t* map;		   // null: periodic kernel
+	const void* inflow[3];	   // compute-type [Z][Y] profiles or null
+	void* macro;			   // compute-type [4][Z][Y][X] or null
+	double* partials;		   // [blocks][NRED] or null
+	CollParamsD p;
+	int coll, cum_flags;
+	bool odd;
+	dim3 grid, block;
+	cudaStream_t stream;
+};
+
+struct StorageOps
+{
+	// one A-A step
+	cudaError_t (*step)(const StepLaunch&);
+	// equilibrium on every site incl. the ghost layer
+	cudaError_t (*init_eq)(const Geometry&, const InitSpec&, cudaStream_t);
+	// convert between storage and a dense buffer [27][nz][ny][nx] of double
+	// (dtype 0) or float (dtype 1); ghost = 1 includes the ghost layer
+	cudaError_t (*pack)(const Geometry&, void* dense, int dtype, int ghost, cudaStream_t);
+	cudaError_t (*unpack)(const Geometry&, const void* dense, int dtype, int ghost, cudaStream_t);
+	int compute_size;  // sizeof the compute type (8 or 4)
+	int elem_size;	   // sizeof the storage element
+	const char* name;
+};
+
+const StorageOps& storage_ops(int storage);
+
+// FP64 reductions shared by all storages (lbm_reduce.cu)
+constexpr int NRED_HOST = 6;
+cudaError_t finish_sums(const double* partials, long long nblocks, double* out, cudaStream_t);
+// enstrophy-type sum rho * |grad u|^2 with central differences over the macro
+// field (compute type given by compute_size), periodic wrap as sim_4.cu:21-54
+cudaError_t enstrophy_partials(const void* macro, int compute_size, int X, int Y, int Z, double* partials, long long* nblocks,
+							   cudaStream_t);
+
+}  // namespace lbm

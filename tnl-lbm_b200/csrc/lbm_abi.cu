@@ -1,0 +1,794 @@
+// C-ABI of the B200 hot path (declared in include/tnl_lbm_b200.h).
+//
+// Owns the device state of one lattice (populations with ghost layer, map,
+// inflow profiles, macro field, reduction scratch), computes the per-viscosity
+// collision constants once on the host, and drives the even/odd A-A kernels
+// from a host loop or from captured CUDA graphs.  Mirrors the host side of the
+// reference's time step: LBM::updateKernelData (include/lbm3d/lbm.hpp:307-323)
+// and State::SimUpdate (include/lbm3d/state.hpp:1235-1314).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tnl_lbm_b200.h"
+#include "d3q27.cuh"
+#include "launch.h"
+
+namespace lbm {
+const StorageOps& storage_ops_f64();
+const StorageOps& storage_ops_f32();
+const StorageOps& storage_ops_f32s();
+const StorageOps& storage_ops_f16s();
+const StorageOps& storage_ops_bf16s();
+
+const StorageOps& storage_ops(int storage)
+{
+	switch (storage) {
+		case ST_F64:
+			return storage_ops_f64();
+		case ST_F32:
+			return storage_ops_f32();
+		case ST_F32S:
+			return storage_ops_f32s();
+		case ST_F16S:
+			return storage_ops_f16s();
+		default:
+			return storage_ops_bf16s();
+	}
+}
+}  // namespace lbm
+
+namespace {
+
+thread_local std::string g_error = "no error";
+
+int fail(int code, const char* fmt, ...)
+{
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	g_error = buf;
+	return code;
+}
+
+#define LBM_CUDA(call)                                                                                   \
+	do {                                                                                                 \
+		cudaError_t err_ = (call);                                                                       \
+		if (err_ != cudaSuccess)                                                                         \
+			return fail(LBM_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, \
+						__LINE__);                                                                       \
+	} while (0)
+
+// Geier 2017 relaxation rates for omega2 = 1 (col_cum.h:195-228), evaluated
+// once per viscosity in double precision
+void cumulant_rates(double nu, lbm::CollParamsD& p)
+{
+	const double w1 = 1.0 / (3.0 * nu + 0.5);
+	const double w2 = 1.0;
+	p.w1 = w1;
+	p.w3 = 8 * (w1 - 2) * (w2 * (3 * w1 - 1) - 5 * w1) / (8 * (5 - 2 * w1) * w1 + w2 * (8 + w1 * (9 * w1 - 26)));
+	p.w4 = 8 * (w1 - 2) * (w1 + w2 * (3 * w1 - 7)) / (w2 * (56 - 42 * w1 + 9 * w1 * w1) - 8 * w1);
+	p.w5 = 24 * (w1 - 2) * (4 * w1 * w1 + w1 * w2 * (18 - 13 * w1) + w2 * w2 * (2 + w1 * (6 * w1 - 11)))
+		 / (16 * w1 * w1 * (w1 - 6) - 2 * w1 * w2 * (216 + 5 * w1 * (9 * w1 - 46))
+			+ w2 * w2 * (w1 * (3 * w1 - 10) * (15 * w1 - 28) - 48));
+	p.A = (4 * w1 * w1 + 2 * w1 * w2 * (w1 - 6) + w2 * w2 * (w1 * (10 - 3 * w1) - 4)) / (w1 - w2) / (w2 * (2 + 3 * w1) - 8 * w1);
+	p.B = (4 * w1 * w2 * (9 * w1 - 16) - 4 * w1 * w1 - 2 * w2 * w2 * (2 + 9 * w1 * (w1 - 2))) / 3.0 / (w1 - w2)
+		/ (w2 * (2 + 3 * w1) - 8 * w1);
+	p.tau = 3.0 * nu + 0.5;
+}
+
+bool site_type_supported(uint8_t g)
+{
+	switch (g) {
+		case lbm::GEO_FLUID:
+		case lbm::GEO_WALL:
+		case lbm::GEO_INFLOW:
+		case lbm::GEO_INFLOW_LEFT:
+		case lbm::GEO_INFLOW_EQ_LEFT:
+		case lbm::GEO_OUTFLOW_EQ:
+		case lbm::GEO_PERIODIC:
+		case lbm::GEO_NOTHING:
+		case lbm::GEO_SYM_TOP:
+		case lbm::GEO_SYM_BOTTOM:
+		case lbm::GEO_SYM_LEFT:
+		case lbm::GEO_SYM_RIGHT:
+		case lbm::GEO_SYM_BACK:
+		case lbm::GEO_SYM_FRONT:
+			return true;
+		default:
+			return false;
+	}
+}
+
+}  // namespace
+
+struct lbm_lattice
+{
+	lbm_desc d{};
+	const lbm::StorageOps* ops = nullptr;
+	lbm::Geometry g{};
+	size_t pop_bytes = 0;
+	cudaStream_t stream = nullptr;
+	uint8_t* map = nullptr;
+	bool map_set = false;
+	void* inflow[3] = {nullptr, nullptr, nullptr};
+	void* inflow_host = nullptr;  // pinned staging of the converted profiles
+	void* macro = nullptr;
+	bool macro_valid = false;
+	double* partials = nullptr;
+	long long partials_cap = 0;	 // in blocks
+	double* sums_dev = nullptr;
+	double* sums_host = nullptr;  // pinned [NRED]
+	bool sums_valid = false;
+	long long iteration = 0;
+	int bx = 0, by = 0;	 // 0: default
+	lbm::CollParamsD p{};
+	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
+	cudaGraphExec_t graph = nullptr;
+	static constexpr int GRAPH_STEPS = 16;
+
+	long long sites() const
+	{
+		return (long long) d.X * d.Y * d.Z;
+	}
+	dim3 block() const
+	{
+		if (bx > 0)
+			return dim3(bx, by, 1);
+		const int bxd = d.X >= 128 ? 128 : ((d.X + 31) / 32) * 32;
+		return dim3(bxd, 128 / bxd, 1);
+	}
+	dim3 grid() const
+	{
+		const dim3 b = block();
+		return dim3((d.X + b.x - 1) / b.x, (d.Y + b.y - 1) / b.y, d.Z);
+	}
+	long long grid_blocks() const
+	{
+		const dim3 gr = grid();
+		return (long long) gr.x * gr.y * gr.z;
+	}
+	void drop_graph()
+	{
+		if (graph) {
+			cudaGraphExecDestroy(graph);
+			graph = nullptr;
+		}
+	}
+};
+
+namespace {
+
+int check(lbm_handle h)
+{
+	if (!h)
+		return fail(LBM_ERR_INVALID, "null handle");
+	if (cudaSetDevice(h->d.device) != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "cudaSetDevice(%d) failed", h->d.device);
+	return LBM_OK;
+}
+
+int ensure_partials(lbm_handle h, long long blocks)
+{
+	if (blocks <= h->partials_cap)
+		return LBM_OK;
+	if (h->partials)
+		cudaFree(h->partials);
+	h->partials = nullptr;
+	h->partials_cap = 0;
+	LBM_CUDA(cudaMalloc(&h->partials, (size_t) blocks * lbm::NRED_HOST * sizeof(double)));
+	h->partials_cap = blocks;
+	return LBM_OK;
+}
+
+int ensure_macro(lbm_handle h)
+{
+	if (h->macro)
+		return LBM_OK;
+	LBM_CUDA(cudaMalloc(&h->macro, (size_t) 4 * h->sites() * h->ops->compute_size));
+	return LBM_OK;
+}
+
+int launch_step(lbm_handle h, bool macro, bool sums)
+{
+	lbm::StepLaunch L{};
+	L.g = h->g;
+	L.map = h->d.periodic ? nullptr : h->map;
+	for (int k = 0; k < 3; k++)
+		L.inflow[k] = h->inflow[k];
+	L.macro = macro ? h->macro : nullptr;
+	L.partials = sums ? h->partials : nullptr;
+	L.p = h->p;
+	L.coll = h->d.collision;
+	L.cum_flags = h->d.cum_flags;
+	L.odd = (h->iteration % 2) != 0;
+	L.grid = h->grid();
+	L.block = h->block();
+	L.stream = h->stream;
+	const cudaError_t err = h->ops->step(L);
+	if (err != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(err));
+	h->iteration++;
+	return LBM_OK;
+}
+
+int build_graph(lbm_handle h)
+{
+	h->drop_graph();
+	const long long saved = h->iteration;
+	h->iteration = 0;  // graph starts at an even step
+	cudaGraph_t graph = nullptr;
+	LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+	int rc = LBM_OK;
+	for (int s = 0; s < lbm_lattice::GRAPH_STEPS && rc == LBM_OK; s++)
+		rc = launch_step(h, false, false);
+	const cudaError_t end = cudaStreamEndCapture(h->stream, &graph);
+	h->iteration = saved;
+	if (rc != LBM_OK) {
+		if (graph)
+			cudaGraphDestroy(graph);
+		return rc;
+	}
+	if (end != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(end));
+	const cudaError_t inst = cudaGraphInstantiate(&h->graph, graph, 0);
+	cudaGraphDestroy(graph);
+	if (inst != cudaSuccess) {
+		h->graph = nullptr;
+		return fail(LBM_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(inst));
+	}
+	return LBM_OK;
+}
+
+int run_plain_steps(lbm_handle h, long long n)
+{
+	while (n > 0 && (h->iteration % 2) != 0) {
+		int rc = launch_step(h, false, false);
+		if (rc)
+			return rc;
+		n--;
+	}
+	if (h->d.use_graphs && n >= lbm_lattice::GRAPH_STEPS) {
+		if (!h->graph) {
+			int rc = build_graph(h);
+			if (rc)
+				return rc;
+		}
+		while (n >= lbm_lattice::GRAPH_STEPS) {
+			LBM_CUDA(cudaGraphLaunch(h->graph, h->stream));
+			h->iteration += lbm_lattice::GRAPH_STEPS;
+			n -= lbm_lattice::GRAPH_STEPS;
+		}
+	}
+	while (n > 0) {
+		int rc = launch_step(h, false, false);
+		if (rc)
+			return rc;
+		n--;
+	}
+	return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lbm_last_error(void)
+{
+	return g_error.c_str();
+}
+
+const char* lbm_version(void)
+{
+	return "tnl-lbm-b200 0.1 (sm_100a, D3Q27 A-A)";
+}
+
+int lbm_create(const lbm_desc* desc, lbm_handle* out)
+{
+	if (!desc || !out)
+		return fail(LBM_ERR_INVALID, "null argument");
+	*out = nullptr;
+	const lbm_desc& d = *desc;
+	if (d.X < 1 || d.Y < 1 || d.Z < 1)
+		return fail(LBM_ERR_INVALID, "lattice sizes must be positive (got %d x %d x %d)", d.X, d.Y, d.Z);
+	if (d.X > 65535 * 4 || d.Y > 65535 || d.Z > 65535)
+		return fail(LBM_ERR_SIZE, "lattice sizes beyond the launch limits");
+	if (d.storage < 0 || d.storage >= lbm::ST_COUNT)
+		return fail(LBM_ERR_INVALID, "unknown storage %d", d.storage);
+	if (d.collision < LBM_COLL_CUM || d.collision > LBM_COLL_MRT)
+		return fail(LBM_ERR_INVALID, "unknown collision %d", d.collision);
+	if (d.collision == LBM_COLL_CUM && d.cum_flags != 0 && d.cum_flags != LBM_CUM_ANTIALIAS
+		&& d.cum_flags != (LBM_CUM_GEIER_2017 | LBM_CUM_ANTIALIAS))
+		return fail(LBM_ERR_UNSUPPORTED, "cumulant flags %d: the 2017 variant requires the anti-aliasing terms", d.cum_flags);
+	if (d.equilibrium != LBM_EQ_SECOND_ORDER && d.equilibrium != LBM_EQ_INV_CUM)
+		return fail(LBM_ERR_INVALID, "unknown equilibrium %d", d.equilibrium);
+	if (!(d.viscosity > 0.0) || !std::isfinite(d.viscosity))
+		return fail(LBM_ERR_INVALID, "viscosity must be positive and finite (state.hpp:1240-1245)");
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		return fail(LBM_ERR_CUDA, "no CUDA device available");
+	if (d.device < 0 || d.device >= ndev)
+		return fail(LBM_ERR_INVALID, "device %d out of range", d.device);
+	LBM_CUDA(cudaSetDevice(d.device));
+
+	lbm_lattice* h = new lbm_lattice();
+	h->d = d;
+	h->ops = &lbm::storage_ops(d.storage);
+	const int es = h->ops->elem_size;
+	const int align = 128 / es;	 // elements per 128 bytes
+	h->g.x0 = align;
+	h->g.sy = ((align + d.X + 1 + align - 1) / align) * align;
+	h->g.sz = h->g.sy * (d.Y + 2);
+	h->g.sq = (long long) h->g.sz * (d.Z + 2);
+	h->g.X = d.X;
+	h->g.Y = d.Y;
+	h->g.Z = d.Z;
+	h->pop_bytes = (size_t) 27 * h->g.sq * es;
+	cumulant_rates(d.viscosity, h->p);
+	h->p.nu = d.viscosity;
+	h->p.fx = d.fx;
+	h->p.fy = d.fy;
+	h->p.fz = d.fz;
+	h->p.eq = d.equilibrium;
+
+	auto cleanup = [&](int rc) {
+		lbm_destroy(h);
+		return rc;
+	};
+	if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "stream creation failed"));
+	cudaError_t e = cudaMalloc(&h->g.f, h->pop_bytes);
+	if (e != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "population allocation of %zu bytes failed: %s", h->pop_bytes, cudaGetErrorString(e)));
+	if (cudaMemsetAsync(h->g.f, 0, h->pop_bytes, h->stream) != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "population memset failed"));
+	if (!d.periodic && cudaMalloc(&h->map, (size_t) h->sites()) != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "map allocation failed"));
+	if (cudaMalloc(&h->sums_dev, lbm::NRED_HOST * sizeof(double)) != cudaSuccess
+		|| cudaMallocHost(&h->sums_host, lbm::NRED_HOST * sizeof(double)) != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "reduction buffers allocation failed"));
+	int rc = ensure_partials(h, h->grid_blocks());
+	if (rc)
+		return cleanup(rc);
+	*out = h;
+	return LBM_OK;
+}
+
+int lbm_destroy(lbm_handle h)
+{
+	if (!h)
+		return LBM_OK;
+	cudaSetDevice(h->d.device);
+	if (h->stream)
+		cudaStreamSynchronize(h->stream);
+	h->drop_graph();
+	cudaFree(h->g.f);
+	cudaFree(h->map);
+	for (auto* p : h->inflow)
+		cudaFree(p);
+	cudaFree(h->macro);
+	if (h->inflow_host)
+		cudaFreeHost(h->inflow_host);
+	cudaFree(h->partials);
+	cudaFree(h->sums_dev);
+	if (h->sums_host)
+		cudaFreeHost(h->sums_host);
+	if (h->stream)
+		cudaStreamDestroy(h->stream);
+	delete h;
+	return LBM_OK;
+}
+
+int lbm_set_map(lbm_handle h, const uint8_t* map)
+{
+	if (int rc = check(h))
+		return rc;
+	if (h->d.periodic)
+		return fail(LBM_ERR_INVALID, "periodic lattice has no map");
+	if (!map)
+		return fail(LBM_ERR_INVALID, "null map");
+	const long long n = h->sites();
+	for (long long i = 0; i < n; i++)
+		if (!site_type_supported(map[i]))
+			return fail(LBM_ERR_UNSUPPORTED,
+						"site type %d at index %lld is not provided by the A-A kernels (reads a slot another site writes "
+						"in the same pass, or belongs to the adjoint set)",
+						(int) map[i], i);
+	LBM_CUDA(cudaMemcpyAsync(h->map, map, (size_t) n, cudaMemcpyHostToDevice, h->stream));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	h->map_set = true;
+	return LBM_OK;
+}
+
+int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const double* vz)
+{
+	if (int rc = check(h))
+		return rc;
+	const double* src[3] = {vx, vy, vz};
+	const size_t n = (size_t) h->d.Y * h->d.Z;
+	const int cs = h->ops->compute_size;
+	if (!h->inflow_host)
+		LBM_CUDA(cudaMallocHost(&h->inflow_host, 3 * n * cs));
+	bool realloc = false;
+	for (int k = 0; k < 3; k++) {
+		if (!src[k]) {
+			if (h->inflow[k]) {
+				LBM_CUDA(cudaMemsetAsync(h->inflow[k], 0, n * cs, h->stream));
+			}
+			continue;
+		}
+		if (!h->inflow[k]) {
+			LBM_CUDA(cudaMalloc(&h->inflow[k], n * cs));
+			realloc = true;
+		}
+		unsigned char* stage = (unsigned char*) h->inflow_host + k * n * cs;
+		if (cs == 8)
+			std::memcpy(stage, src[k], n * 8);
+		else
+			for (size_t i = 0; i < n; i++)
+				((float*) stage)[i] = (float) src[k][i];
+		LBM_CUDA(cudaMemcpyAsync(h->inflow[k], stage, n * cs, cudaMemcpyHostToDevice, h->stream));
+	}
+	// the staging buffer is reused by the next call: wait for the copies
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	if (realloc)
+		h->drop_graph();  // kernel arguments changed; new values alone need no new graph
+	return LBM_OK;
+}
+
+int lbm_set_viscosity(lbm_handle h, double nu)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!(nu > 0.0) || !std::isfinite(nu))
+		return fail(LBM_ERR_INVALID, "viscosity must be positive and finite");
+	h->d.viscosity = nu;
+	cumulant_rates(nu, h->p);
+	h->p.nu = nu;
+	h->drop_graph();
+	return LBM_OK;
+}
+
+int lbm_init_equilibrium(lbm_handle h, const double* rho, const double* vx, const double* vy, const double* vz, double rho0,
+						 double vx0, double vy0, double vz0)
+{
+	if (int rc = check(h))
+		return rc;
+	const bool fields = rho || vx || vy || vz;
+	if (fields && !(rho && vx && vy && vz))
+		return fail(LBM_ERR_INVALID, "either all four fields or none");
+	lbm::InitSpec spec{};
+	spec.mode = fields ? 1 : 0;
+	spec.eq = h->d.equilibrium;
+	spec.rho0 = rho0;
+	spec.vx0 = vx0;
+	spec.vy0 = vy0;
+	spec.vz0 = vz0;
+	double* dev = nullptr;
+	const size_t n = (size_t) h->sites();
+	if (fields) {
+		LBM_CUDA(cudaMallocAsync((void**) &dev, 4 * n * sizeof(double), h->stream));
+		const double* src[4] = {rho, vx, vy, vz};
+		for (int k = 0; k < 4; k++)
+			LBM_CUDA(cudaMemcpyAsync(dev + k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+		spec.rho = dev;
+		spec.vx = dev + n;
+		spec.vy = dev + 2 * n;
+		spec.vz = dev + 3 * n;
+	}
+	const cudaError_t e = h->ops->init_eq(h->g, spec, h->stream);
+	if (dev)
+		cudaFreeAsync(dev, h->stream);
+	if (e != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "init kernel failed: %s", cudaGetErrorString(e));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	h->iteration = 0;
+	h->macro_valid = h->sums_valid = false;
+	return LBM_OK;
+}
+
+int lbm_init_taylor_green(lbm_handle h, double u0, double rho0)
+{
+	if (int rc = check(h))
+		return rc;
+	lbm::InitSpec spec{};
+	spec.mode = 2;
+	spec.eq = h->d.equilibrium;
+	spec.rho0 = rho0;
+	spec.u0 = u0;
+	const cudaError_t e = h->ops->init_eq(h->g, spec, h->stream);
+	if (e != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "init kernel failed: %s", cudaGetErrorString(e));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	h->iteration = 0;
+	h->macro_valid = h->sums_valid = false;
+	return LBM_OK;
+}
+
+static size_t dense_count(lbm_handle h, int layout)
+{
+	const int gh = layout == LBM_LAYOUT_GHOST ? 2 : 0;
+	return (size_t) 27 * (h->d.X + gh) * (size_t) (h->d.Y + gh) * (h->d.Z + gh);
+}
+
+int lbm_set_populations(lbm_handle h, const void* host, int layout, int dtype)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!host || (layout != 0 && layout != 1) || (dtype != 0 && dtype != 1))
+		return fail(LBM_ERR_INVALID, "bad arguments");
+	const size_t bytes = dense_count(h, layout) * (dtype == 0 ? 8 : 4);
+	void* dev = nullptr;
+	LBM_CUDA(cudaMallocAsync(&dev, bytes, h->stream));
+	LBM_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, h->stream));
+	const cudaError_t e = h->ops->unpack(h->g, dev, dtype, layout, h->stream);
+	cudaFreeAsync(dev, h->stream);
+	if (e != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "unpack failed: %s", cudaGetErrorString(e));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	return LBM_OK;
+}
+
+int lbm_get_populations(lbm_handle h, void* host, int layout, int dtype)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!host || (layout != 0 && layout != 1) || (dtype != 0 && dtype != 1))
+		return fail(LBM_ERR_INVALID, "bad arguments");
+	const size_t bytes = dense_count(h, layout) * (dtype == 0 ? 8 : 4);
+	void* dev = nullptr;
+	LBM_CUDA(cudaMallocAsync(&dev, bytes, h->stream));
+	const cudaError_t e = h->ops->pack(h->g, dev, dtype, layout, h->stream);
+	if (e != cudaSuccess) {
+		cudaFreeAsync(dev, h->stream);
+		return fail(LBM_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
+	}
+	LBM_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, h->stream));
+	cudaFreeAsync(dev, h->stream);
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	return LBM_OK;
+}
+
+int lbm_step(lbm_handle h, int64_t nsteps, int flags)
+{
+	if (int rc = check(h))
+		return rc;
+	if (nsteps < 0 || (nsteps == 0 && flags))
+		return fail(LBM_ERR_INVALID, "nsteps must be positive when flags are given");
+	if (!h->d.periodic && !h->map_set)
+		return fail(LBM_ERR_INVALID, "lbm_set_map must be called before stepping a non-periodic lattice");
+	if (nsteps == 0)
+		return LBM_OK;
+	const bool macro = (flags & LBM_STEP_MACRO) != 0;
+	const bool sums = (flags & LBM_STEP_SUMS) != 0;
+	int rc = run_plain_steps(h, nsteps - ((macro || sums) ? 1 : 0));
+	if (rc)
+		return rc;
+	if (macro || sums) {
+		if (macro && (rc = ensure_macro(h)))
+			return rc;
+		if (sums && (rc = ensure_partials(h, h->grid_blocks())))
+			return rc;
+		if ((rc = launch_step(h, macro, sums)))
+			return rc;
+		if (sums) {
+			const cudaError_t e = lbm::finish_sums(h->partials, h->grid_blocks(), h->sums_dev, h->stream);
+			if (e != cudaSuccess)
+				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
+			LBM_CUDA(cudaMemcpyAsync(h->sums_host, h->sums_dev, lbm::NRED_HOST * sizeof(double), cudaMemcpyDeviceToHost,
+									 h->stream));
+		}
+		h->macro_valid = macro;
+		h->sums_valid = sums;
+	}
+	else {
+		h->macro_valid = h->sums_valid = false;
+	}
+	return LBM_OK;
+}
+
+int64_t lbm_iteration(lbm_handle h)
+{
+	return h ? h->iteration : -1;
+}
+
+int lbm_set_iteration(lbm_handle h, int64_t iteration)
+{
+	if (int rc = check(h))
+		return rc;
+	if (iteration < 0)
+		return fail(LBM_ERR_INVALID, "iteration must be non-negative");
+	h->iteration = iteration;
+	return LBM_OK;
+}
+
+int lbm_get_macro(lbm_handle h, double* host)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!host)
+		return fail(LBM_ERR_INVALID, "null output");
+	if (!h->macro_valid)
+		return fail(LBM_ERR_INVALID, "no macro field: run lbm_step with LBM_STEP_MACRO first");
+	const size_t n = 4 * (size_t) h->sites();
+	if (h->ops->compute_size == 8) {
+		LBM_CUDA(cudaMemcpyAsync(host, h->macro, n * 8, cudaMemcpyDeviceToHost, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+	}
+	else {
+		std::vector<float> tmp(n);
+		LBM_CUDA(cudaMemcpyAsync(tmp.data(), h->macro, n * 4, cudaMemcpyDeviceToHost, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+		for (size_t i = 0; i < n; i++)
+			host[i] = tmp[i];
+	}
+	return LBM_OK;
+}
+
+int lbm_get_sums(lbm_handle h, double* out)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!out)
+		return fail(LBM_ERR_INVALID, "null output");
+	if (!h->sums_valid)
+		return fail(LBM_ERR_INVALID, "no sums: run lbm_step with LBM_STEP_SUMS first");
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	std::memcpy(out, h->sums_host, lbm::NRED_HOST * sizeof(double));
+	if (out[5] != 0.0)
+		return fail(LBM_ERR_NONFINITE, "%.0f sites with a non-finite density", out[5]);
+	return LBM_OK;
+}
+
+int lbm_enstrophy_sum(lbm_handle h, double* out)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!out)
+		return fail(LBM_ERR_INVALID, "null output");
+	if (!h->macro_valid)
+		return fail(LBM_ERR_INVALID, "no macro field: run lbm_step with LBM_STEP_MACRO first");
+	long long nb = 0;
+	const long long need = (long long) ((h->d.X + 127) / 128) * h->d.Y * h->d.Z;
+	if (int rc = ensure_partials(h, need))
+		return rc;
+	double* dres = nullptr;
+	LBM_CUDA(cudaMallocAsync((void**) &dres, lbm::NRED_HOST * sizeof(double), h->stream));
+	cudaError_t e = lbm::enstrophy_partials(h->macro, h->ops->compute_size, h->d.X, h->d.Y, h->d.Z, h->partials, &nb, h->stream);
+	if (e == cudaSuccess)
+		e = lbm::finish_sums(h->partials, nb, dres, h->stream);
+	double res[lbm::NRED_HOST];
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(res, dres, sizeof(res), cudaMemcpyDeviceToHost, h->stream);
+	cudaFreeAsync(dres, h->stream);
+	if (e != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "enstrophy reduction failed: %s", cudaGetErrorString(e));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	*out = res[0];
+	return LBM_OK;
+}
+
+int lbm_synchronize(lbm_handle h)
+{
+	if (int rc = check(h))
+		return rc;
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	return LBM_OK;
+}
+
+int lbm_set_block(lbm_handle h, int bx, int by)
+{
+	if (int rc = check(h))
+		return rc;
+	if (bx == 0 && by == 0) {
+		h->bx = h->by = 0;
+	}
+	else {
+		if (bx < 32 || bx % 32 != 0 || by < 1 || bx * by > 256)
+			return fail(LBM_ERR_INVALID, "block (%d, %d): bx must be a multiple of 32 and bx*by <= 256", bx, by);
+		h->bx = bx;
+		h->by = by;
+	}
+	h->drop_graph();
+	return ensure_partials(h, h->grid_blocks());
+}
+
+int lbm_get_block(lbm_handle h, int* bx, int* by)
+{
+	if (int rc = check(h))
+		return rc;
+	const dim3 b = h->block();
+	if (bx)
+		*bx = (int) b.x;
+	if (by)
+		*by = (int) b.y;
+	return LBM_OK;
+}
+
+int lbm_autotune(lbm_handle h, int ntrials)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!h->d.periodic && !h->map_set)
+		return fail(LBM_ERR_INVALID, "lbm_set_map must be called before autotuning");
+	if (ntrials < 2)
+		ntrials = 2;
+	ntrials += ntrials % 2;
+	void* backup = nullptr;
+	LBM_CUDA(cudaMalloc(&backup, h->pop_bytes));
+	LBM_CUDA(cudaMemcpyAsync(backup, h->g.f, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream));
+	const long long it0 = h->iteration;
+	static const int cands[][2] = {{32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}, {32, 2}, {64, 1}};
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	float best = 1e30f;
+	int bbx = 0, bby = 0;
+	const int obx = h->bx, oby = h->by;
+	for (auto& c : cands) {
+		if (c[0] > 32 && c[0] / 2 >= h->d.X)
+			continue;  // far wider than the lattice
+		h->bx = c[0];
+		h->by = c[1];
+		if (ensure_partials(h, h->grid_blocks()))
+			break;
+		// warm-up pair, then timed steps
+		launch_step(h, false, false);
+		launch_step(h, false, false);
+		cudaEventRecord(e0, h->stream);
+		for (int s = 0; s < ntrials; s++)
+			launch_step(h, false, false);
+		cudaEventRecord(e1, h->stream);
+		cudaEventSynchronize(e1);
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		if (ms < best) {
+			best = ms;
+			bbx = c[0];
+			bby = c[1];
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	h->iteration = it0;
+	cudaMemcpyAsync(h->g.f, backup, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
+	cudaStreamSynchronize(h->stream);
+	cudaFree(backup);
+	const cudaError_t err = cudaGetLastError();
+	if (err != cudaSuccess) {
+		h->bx = obx;
+		h->by = oby;
+		return fail(LBM_ERR_CUDA, "autotune failed: %s", cudaGetErrorString(err));
+	}
+	h->bx = bbx;
+	h->by = bby;
+	h->drop_graph();
+	return ensure_partials(h, h->grid_blocks());
+}
+
+int lbm_device_view_get(lbm_handle h, lbm_device_view* out)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!out)
+		return fail(LBM_ERR_INVALID, "null output");
+	out->populations = h->g.f;
+	out->sq = h->g.sq;
+	out->sy = h->g.sy;
+	out->sz = h->g.sz;
+	out->x0 = h->g.x0;
+	out->elem_size = h->ops->elem_size;
+	out->macro = h->macro;
+	out->macro_elem_size = h->ops->compute_size;
+	out->stream = (void*) h->stream;
+	return LBM_OK;
+}
+
+}  // extern "C"

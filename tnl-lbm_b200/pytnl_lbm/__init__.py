@@ -1,0 +1,203 @@
+"""pytnl_lbm -- Python binding of the B200 D3Q27 A-A hot path.
+
+Counterpart of TNL-LBM's nanobind module (pytnl_lbm/pytnl_lbm.cpp:15-73).  The
+binding is a thin ctypes layer over the C-ABI in include/tnl_lbm_b200.h; the
+compute runs in the sm_100a kernels of lib/libtnl_lbm_b200.so.  There is no
+CPU fallback: creating a lattice without the library or without a CUDA device
+raises.  numpy arrays are exchanged with the host entry points; torch tensors
+(the only place PyTorch is used) can wrap the device buffers without copies
+through ``LBM.device_view()``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import (  # noqa: F401  (re-exported constants)
+    COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
+    GEO, LAYOUT_GHOST, LAYOUT_INTERIOR, STEP_MACRO, STEP_SUMS, STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S,
+    STORE_F64, LbmError, library, library_path)
+
+__all__ = ["LBM", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
+
+# D3Q27_MACRO_Default quantity order (include/lbm3d/d3q27/macro.h:61-68)
+macro_names = ("rho", "vx", "vy", "vz")
+
+
+@dataclass
+class Config:
+    """Composition of the plugin slots (LBM_CONFIG, include/lbm3d/defs.h:288-310)."""
+    collision: int = COLL_CUM
+    cum_flags: int = 0
+    equilibrium: int = EQ_INV_CUM
+    storage: int = STORE_F32
+
+
+class LBM:
+    """One lattice on one GPU (LBM_BLOCK + LBM of the reference, single block).
+
+    Sizes are lattice sites per axis without the ghost layer.  ``periodic=True``
+    makes every site GEO_PERIODIC and no map is needed.
+    """
+
+    def __init__(self, X, Y, Z, *, viscosity, collision=COLL_CUM, cum_flags=0, equilibrium=EQ_INV_CUM,
+                 storage=STORE_F32, periodic=False, force=(0.0, 0.0, 0.0), device=0, use_graphs=True):
+        self.lib = library()
+        d = _abi.lbm_desc()
+        d.X, d.Y, d.Z = int(X), int(Y), int(Z)
+        d.storage, d.collision, d.cum_flags, d.equilibrium = storage, collision, cum_flags, equilibrium
+        d.periodic = 1 if periodic else 0
+        d.viscosity = float(viscosity)
+        d.fx, d.fy, d.fz = (float(v) for v in force)
+        d.device = int(device)
+        d.use_graphs = 1 if use_graphs else 0
+        self.desc = d
+        self.shape = (int(Z), int(Y), int(X))
+        self.X, self.Y, self.Z = int(X), int(Y), int(Z)
+        self.storage = storage
+        h = _abi.lbm_handle()
+        _abi.check(self.lib.lbm_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+
+    # -- lifetime -------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- setup ----------------------------------------------------------
+    def set_map(self, geo_map):
+        m = np.ascontiguousarray(geo_map, dtype=np.uint8)
+        assert m.shape == self.shape, f"map shape {m.shape} != {self.shape}"
+        _abi.check(self.lib.lbm_set_map(self.h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def set_inflow(self, vx=None, vy=None, vz=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (vx, vy, vz)]
+        for a in arrs:
+            if a is not None:
+                assert a.shape == (self.Z, self.Y)
+        _abi.check(self.lib.lbm_set_inflow(self.h, *[_abi.dptr(a) for a in arrs]))
+
+    def set_viscosity(self, nu):
+        _abi.check(self.lib.lbm_set_viscosity(self.h, float(nu)))
+
+    def init_equilibrium(self, rho=None, vx=None, vy=None, vz=None, uniform=(1.0, 0.0, 0.0, 0.0)):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, vx, vy, vz)]
+        _abi.check(self.lib.lbm_init_equilibrium(self.h, *[_abi.dptr(a) for a in arrs], *map(float, uniform)))
+
+    def init_taylor_green(self, u0, rho0=1.0):
+        _abi.check(self.lib.lbm_init_taylor_green(self.h, float(u0), float(rho0)))
+
+    def set_populations(self, f, layout=LAYOUT_GHOST):
+        f = np.ascontiguousarray(f)
+        dtype = 0 if f.dtype == np.float64 else 1
+        assert f.dtype in (np.float64, np.float32)
+        assert f.shape == self._pop_shape(layout), f"{f.shape} != {self._pop_shape(layout)}"
+        _abi.check(self.lib.lbm_set_populations(self.h, f.ctypes.data_as(ctypes.c_void_p), layout, dtype))
+
+    def get_populations(self, layout=LAYOUT_GHOST, dtype=np.float64):
+        out = np.empty(self._pop_shape(layout), dtype=dtype)
+        _abi.check(self.lib.lbm_get_populations(self.h, out.ctypes.data_as(ctypes.c_void_p), layout,
+                                                0 if out.dtype == np.float64 else 1))
+        return out
+
+    def _pop_shape(self, layout):
+        g = 2 if layout == LAYOUT_GHOST else 0
+        return (27, self.Z + g, self.Y + g, self.X + g)
+
+    # -- stepping -------------------------------------------------------
+    def step(self, nsteps=1, macro=False, sums=False):
+        flags = (STEP_MACRO if macro else 0) | (STEP_SUMS if sums else 0)
+        _abi.check(self.lib.lbm_step(self.h, int(nsteps), flags))
+
+    @property
+    def iteration(self):
+        return int(self.lib.lbm_iteration(self.h))
+
+    @iteration.setter
+    def iteration(self, it):
+        _abi.check(self.lib.lbm_set_iteration(self.h, int(it)))
+
+    def macro(self):
+        out = np.empty((4,) + self.shape, dtype=np.float64)
+        _abi.check(self.lib.lbm_get_macro(self.h, _abi.dptr(out)))
+        return out
+
+    def sums(self):
+        out = np.zeros(6, dtype=np.float64)
+        _abi.check(self.lib.lbm_get_sums(self.h, _abi.dptr(out)))
+        return out
+
+    def enstrophy_sum(self):
+        v = ctypes.c_double(0)
+        _abi.check(self.lib.lbm_enstrophy_sum(self.h, ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        _abi.check(self.lib.lbm_synchronize(self.h))
+
+    def set_block(self, bx, by):
+        _abi.check(self.lib.lbm_set_block(self.h, int(bx), int(by)))
+
+    def block(self):
+        bx, by = ctypes.c_int(0), ctypes.c_int(0)
+        _abi.check(self.lib.lbm_get_block(self.h, ctypes.byref(bx), ctypes.byref(by)))
+        return bx.value, by.value
+
+    def autotune(self, ntrials=4):
+        _abi.check(self.lib.lbm_autotune(self.h, int(ntrials)))
+        return self.block()
+
+    def device_view(self):
+        v = _abi.lbm_device_view()
+        _abi.check(self.lib.lbm_device_view_get(self.h, ctypes.byref(v)))
+        return v
+
+    def populations_tensor(self):
+        """torch view of the raw population storage [27, Z+2, Y+2, pitch] (no copy)."""
+        import torch
+        v = self.device_view()
+        dt = {8: torch.float64, 4: torch.float32, 2: torch.float16 if self.storage == STORE_F16S else torch.bfloat16}[
+            v.elem_size]
+        n = 27 * v.sq
+        return _wrap_device(v.populations, n, dt, self.desc.device).view(27, self.Z + 2, self.Y + 2, v.sy)
+
+
+def _wrap_device(ptr, n, dtype, device):
+    import torch
+
+    class _CudaArray:
+        def __init__(self):
+            self.__cuda_array_interface__ = {
+                "shape": (n,), "typestr": {torch.float64: "<f8", torch.float32: "<f4", torch.float16: "<f2",
+                                           torch.bfloat16: "<f2"}[dtype],
+                "data": (int(ptr), False), "version": 3}
+
+    t = torch.as_tensor(_CudaArray(), device=f"cuda:{device}")
+    return t.view(dtype) if dtype == torch.bfloat16 else t
+
+
+def kinetic_energy(lbm: LBM, rho0=1.0):
+    """Kinetic energy of the last summed step, E = sum rho |u|^2 / (2 rho0 V)
+    (sim_NSE/sim_4.cu:257-275), in lattice units."""
+    s = lbm.sums()
+    return s[4] / rho0 / 2.0 / (lbm.X * lbm.Y * lbm.Z)
+
+
+from ._state import State, execute  # noqa: E402,F401
