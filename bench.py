@@ -174,7 +174,7 @@ def max_over_ranks(dist, value, device):
     return float(t.item())
 
 
-def make_lattice(pl, spec, storage, device):
+def make_lattice(pl, spec, storage, device, kernel="tile"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
@@ -182,6 +182,7 @@ def make_lattice(pl, spec, storage, device):
         m, prof, nu, fields = duct_setup(X, Y, Z)
         lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                      equilibrium=pl.EQ_INV_CUM, storage=st, device=device)
+        lat.set_kernel(pl.KERNEL_TILE if kernel == "tile" else pl.KERNEL_DIRECT)
         lat.set_map(m)
         lat.set_inflow(prof, None, None)
         lat.init_equilibrium(*fields)
@@ -189,6 +190,7 @@ def make_lattice(pl, spec, storage, device):
     nu = 0.05 * (X / (2 * math.pi)) / 1600.0
     lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                  equilibrium=pl.EQ_INV_CUM, storage=st, periodic=True, device=device)
+    lat.set_kernel(pl.KERNEL_TILE if kernel == "tile" else pl.KERNEL_DIRECT)
     lat.init_taylor_green(0.05, 1.0)
     return lat, None
 
@@ -217,7 +219,7 @@ def run_ours(args):
     device = torch.device("cuda", local)
     spec = workload_spec(args.workload)
     sites = spec["X"] * spec["Y"] * spec["Z"]
-    lat, prof = make_lattice(pl, spec, args.storage, local)
+    lat, prof = make_lattice(pl, spec, args.storage, local, args.kernel)
     if args.autotune:
         lat.autotune(4)
     stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
@@ -267,13 +269,19 @@ def run_ours(args):
     if args.variants and args.storage == "f32":
         lat.close()
         for st in ("f16s", "bf16s"):
-            vl, _ = make_lattice(pl, spec, st, local)
+            vl, _ = make_lattice(pl, spec, st, local, args.kernel)
             vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
             vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
             variants[st] = {"mlups": sites * args.steps / vsecs / 1e6,
                             "speedup_vs_f32": secs / vsecs,
                             "achieved_gbs": 2 * 27 * 2 * sites / (vsecs / args.steps) / 1e9}
             vl.close()
+        other = "direct" if args.kernel == "tile" else "tile"
+        vl, _ = make_lattice(pl, spec, "f32", local, other)
+        vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
+        vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
+        variants[f"f32_{other}_kernel"] = {"mlups": sites * args.steps / vsecs / 1e6}
+        vl.close()
     else:
         lat.close()
 
@@ -290,7 +298,8 @@ def run_ours(args):
                            " Geier-2017+antialias" if spec["cum_flags"] == 3 else " default"),
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
-                       "block": list(block)},
+                       "step_kernel": args.kernel,
+                       "block": list(block) if args.kernel == "direct" else "persistent tile kernel, 128+32 threads"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -423,6 +432,7 @@ def main():
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--kernel", default="tile", choices=["tile", "direct"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -168,6 +168,20 @@ LBM_API int lbm_get_block(lbm_handle h, int* bx, int* by);
  * get_optimal_block_size (include/lbm3d/block_size_optimizer.h:18-111). */
 LBM_API int lbm_autotune(lbm_handle h, int ntrials);
 
+/* Step kernel: LBM_KERNEL_TILE (default) is the persistent kernel that
+ * streams population rows into shared memory with bulk copies;
+ * LBM_KERNEL_DIRECT is one thread per site with direct loads.  Both compute
+ * the same update. */
+#define LBM_KERNEL_DIRECT 0
+#define LBM_KERNEL_TILE 1
+LBM_API int lbm_set_kernel(lbm_handle h, int kernel);
+LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
+
+/* Device status word: bit LBM_STATUS_TIMEOUT is set when a bounded wait inside
+ * a kernel gave up (the kernel then stops early; the step's result is invalid). */
+#define LBM_STATUS_TIMEOUT 1
+LBM_API int lbm_status(lbm_handle h, int* status);
+
 /* Device view for zero-copy interop (pytnl_lbm): the population base pointer
  * and strides in elements: index(q,x,y,z) = q*sq + (z+1)*sz + (y+1)*sy + x0 + x. */
 typedef struct lbm_device_view {

@@ -64,10 +64,21 @@ def seeded_state(port, rng, X, Y, Z, eq="INV_CUM", dtype=np.float64, noise=0.01,
 
 
 def rel_linf(a, b):
-    """max |a - b| / |b| over all entries (populations are bounded away from 0)."""
+    """Relative L-infinity error ||a - b||_inf / ||b||_inf (norm-wise)."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def rel_linf_fields(a, b):
+    """Norm-wise relative L-infinity error of a macro field [rho, vx, vy, vz]:
+    the density against its own scale, the velocity vector against max |u|
+    over all three components (a component that is zero in the flow carries
+    only rounding noise and has no scale of its own)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    vel_scale = max(np.max(np.abs(b[1:4])), 1e-300)
+    return max(rel_linf(a[0], b[0]), float(np.max(np.abs(a[1:4] - b[1:4])) / vel_scale))
 
 
 def max_abs(a, b):

@@ -58,7 +58,7 @@ struct StepArgs
 	const R* in_vy;
 	const R* in_vz;
 	R* macro;		   // [4][Z][Y][X] or null
-	double* partials;  // [blocks][NRED] or null
+	double* partials;  // [NRED][blocks] or null
 	CollParams<R> p;
 };
 
@@ -173,6 +173,82 @@ __device__ __forceinline__ void inlet_moments(Site<R>& s)
 	f[PMM] = R(0.25) * ((m022 + m011) - (m021 + m012)) - (f[MMM] + f[ZMM]);
 }
 
+// Pre-collision part of D3Q27_BC_All for one site (bc.h:85-403) for the site
+// types that are free of cross-site ordering in the A-A pattern: fills rho and
+// u, rewrites the populations a boundary prescribes, and returns whether the
+// site collides (bc.h:406-412).
+template <typename R, typename T>
+__device__ __forceinline__ bool apply_boundary(Site<R>& s, uint8_t geo, const StepArgs<T, R>& a, int z, int y)
+{
+	const long long prof = (long long) z * a.Y + y;
+	switch (geo) {
+		case GEO_INFLOW:
+			s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+			s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+			s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+			s.rho = R(1);
+			set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+			return false;
+		case GEO_INFLOW_LEFT:
+			s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+			s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+			s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+			inlet_moments(s);
+			s.ir = rcp(s.rho);
+			return true;
+		case GEO_INFLOW_EQ_LEFT:
+			s.vx = a.in_vx ? a.in_vx[prof] : R(0);
+			s.vy = a.in_vy ? a.in_vy[prof] : R(0);
+			s.vz = a.in_vz ? a.in_vz[prof] : R(0);
+			s.rho = inlet_density(s.f, s.vx);
+			set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+			return false;
+		case GEO_OUTFLOW_EQ:
+			density_velocity(s, a.p);
+			s.rho = R(1);
+			set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
+			return false;
+		case GEO_WALL:
+			// full-way bounce-back (bc.h:201-221)
+			s.rho = R(1);
+			s.vx = s.vy = s.vz = R(0);
+#pragma unroll
+			for (int q = 1; q < 27; q += 2) {
+				const R t = s.f[q];
+				s.f[q] = s.f[q + 1];
+				s.f[q + 1] = t;
+			}
+			return false;
+		case GEO_SYM_TOP:
+			symmetry<2, -1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		case GEO_SYM_BOTTOM:
+			symmetry<2, 1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		case GEO_SYM_LEFT:
+			symmetry<0, 1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		case GEO_SYM_RIGHT:
+			symmetry<0, -1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		case GEO_SYM_BACK:
+			symmetry<1, 1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		case GEO_SYM_FRONT:
+			symmetry<1, -1>(s.f);
+			density_velocity(s, a.p);
+			return false;
+		default:  // GEO_FLUID, GEO_PERIODIC
+			density_velocity(s, a.p);
+			return true;
+	}
+}
+
 template <typename R>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* partials)
 {
@@ -195,8 +271,11 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* pa
 		double acc = 0;
 		for (int w = 0; w < nwarps; w++)
 			acc += red[w][tid];
+		// structure of arrays: partials[k][block], so that the finish kernels
+		// read each quantity with coalesced loads
+		const long long nblocks = (long long) gridDim.x * gridDim.y * gridDim.z;
 		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
-		partials[block * NRED + tid] = acc;
+		partials[tid * nblocks + block] = acc;
 	}
 }
 
@@ -231,88 +310,10 @@ __global__ void __launch_bounds__(256, MINB) aa_step_kernel(const StepArgs<typen
 			const Offsets o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
 			bool coll = true;
-			if constexpr (GENERAL) {
-				const long long prof = (long long) z * a.Y + y;
-				switch (geo) {
-					case GEO_INFLOW:
-						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
-						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
-						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
-						s.rho = R(1);
-						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
-						coll = false;
-						break;
-					case GEO_INFLOW_LEFT:
-						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
-						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
-						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
-						inlet_moments(s);
-						s.ir = rcp(s.rho);
-						break;
-					case GEO_INFLOW_EQ_LEFT:
-						s.vx = a.in_vx ? a.in_vx[prof] : R(0);
-						s.vy = a.in_vy ? a.in_vy[prof] : R(0);
-						s.vz = a.in_vz ? a.in_vz[prof] : R(0);
-						s.rho = inlet_density(s.f, s.vx);
-						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
-						coll = false;
-						break;
-					case GEO_OUTFLOW_EQ:
-						density_velocity(s, a.p);
-						s.rho = R(1);
-						set_equilibrium(s.f, a.p.eq, s.rho, s.vx, s.vy, s.vz);
-						coll = false;
-						break;
-					case GEO_WALL:
-						// full-way bounce-back (bc.h:201-221)
-						s.rho = R(1);
-						s.vx = s.vy = s.vz = R(0);
-#pragma unroll
-						for (int q = 1; q < 27; q += 2) {
-							const R t = s.f[q];
-							s.f[q] = s.f[q + 1];
-							s.f[q + 1] = t;
-						}
-						coll = false;
-						break;
-					case GEO_SYM_TOP:
-						symmetry<2, -1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					case GEO_SYM_BOTTOM:
-						symmetry<2, 1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					case GEO_SYM_LEFT:
-						symmetry<0, 1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					case GEO_SYM_RIGHT:
-						symmetry<0, -1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					case GEO_SYM_BACK:
-						symmetry<1, 1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					case GEO_SYM_FRONT:
-						symmetry<1, -1>(s.f);
-						density_velocity(s, a.p);
-						coll = false;
-						break;
-					default:  // GEO_FLUID, GEO_PERIODIC
-						density_velocity(s, a.p);
-						break;
-				}
-			}
-			else {
+			if constexpr (GENERAL)
+				coll = apply_boundary(s, geo, a, z, y);
+			else
 				density_velocity(s, a.p);
-			}
 			if (coll)
 				collide<R, COLL, CUMF>(s, a.p);
 			aa_write<S, ODD>(a.f, a.sq, base, o, s.f);

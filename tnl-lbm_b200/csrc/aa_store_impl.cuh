@@ -4,6 +4,7 @@
 #pragma once
 
 #include "aa_kernels.cuh"
+#include "aa_tile.cuh"
 #include "launch.h"
 
 namespace lbm {
@@ -48,9 +49,60 @@ struct StorageUnit
 	using T = typename S::T;
 	using R = typename S::R;
 
+	static constexpr int TILE_X = 128;
+	static constexpr int TILE_STAGES = 3;
+
+	template <int COLL, int CUMF, bool ODD, bool GENERAL>
+	static cudaError_t launch_tile(const StepLaunch& L, const StepArgs<T, R>& a)
+	{
+		auto kern = aa_tile_kernel<S, COLL, CUMF, ODD, GENERAL, TILE_X, TILE_STAGES>;
+		constexpr int smem = tile_smem_bytes<T, TILE_X, ODD, TILE_STAGES>();
+		constexpr int threads = TILE_X + 32;
+		// per-device launch facts of this instantiation, computed once
+		static int per_sm_cache[64] = {0};
+		static int sms_cache[64] = {0};
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (dev < 0 || dev >= 64)
+			return cudaErrorInvalidDevice;
+		if (per_sm_cache[dev] == 0) {
+			cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+			if (e != cudaSuccess)
+				return e;
+			int per_sm = 0, sms = 0;
+			e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+			if (e != cudaSuccess)
+				return e;
+			e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+			if (e != cudaSuccess)
+				return e;
+			if (per_sm < 1)
+				return cudaErrorInvalidConfiguration;
+			sms_cache[dev] = sms;
+			per_sm_cache[dev] = per_sm < TILE_MAX_BLOCKS_PER_SM ? per_sm : TILE_MAX_BLOCKS_PER_SM;
+		}
+		const int tiles_x = (a.X + TILE_X - 1) / TILE_X;
+		const long long ntiles = (long long) tiles_x * a.Y * a.Z;
+		long long grid = (long long) per_sm_cache[dev] * sms_cache[dev];
+		if (grid > ntiles)
+			grid = ntiles;
+		if (L.blocks_out)
+			*L.blocks_out = grid;
+		if (L.dry_run)
+			return cudaSuccess;
+		kern<<<(unsigned) grid, threads, smem, L.stream>>>(a, L.status, ntiles, tiles_x);
+		return cudaGetLastError();
+	}
+
 	template <int COLL, int CUMF, bool ODD, bool GENERAL>
 	static cudaError_t launch_one(const StepLaunch& L, const StepArgs<T, R>& a)
 	{
+		if (L.kernel == KERNEL_TILE)
+			return launch_tile<COLL, CUMF, ODD, GENERAL>(L, a);
+		if (L.blocks_out)
+			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
+		if (L.dry_run)
+			return cudaSuccess;
 		aa_step_kernel<S, COLL, CUMF, ODD, GENERAL, LBM_STORE_MINB><<<L.grid, L.block, 0, L.stream>>>(a);
 		return cudaGetLastError();
 	}

@@ -110,6 +110,11 @@ struct StoreF64
 	{
 		__stcs(p, v);
 	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return *p;
+	}
 };
 
 struct StoreF32
@@ -126,6 +131,11 @@ struct StoreF32
 	{
 		__stcs(p, v);
 	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return *p;
+	}
 };
 
 struct StoreF32S
@@ -141,6 +151,11 @@ struct StoreF32S
 	__device__ static __forceinline__ void store(T* p, R v)
 	{
 		__stcs(p, v - (float) weight(Q));
+	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return *p + (float) weight(Q);
 	}
 };
 
@@ -160,6 +175,11 @@ struct StoreF16S
 		const __half h = __float2half_rn((v - (float) weight(Q)) * half_scale(Q));
 		__stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
 	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return __half2float(*p) * (1.0f / half_scale(Q)) + (float) weight(Q);
+	}
 };
 
 struct StoreBF16S
@@ -178,10 +198,11 @@ struct StoreBF16S
 		const __nv_bfloat16 h = __float2bfloat16_rn(v - (float) weight(Q));
 		__stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(h));
 	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return __bfloat162float(*p) + (float) weight(Q);
+	}
 };
-
-// host-side conversions of the same formats (set/get of populations)
-template <typename S>
-struct HostConv;
 
 }  // namespace lbm

@@ -58,9 +58,23 @@ struct StepLaunch
 	CollParamsD p;
 	int coll, cum_flags;
 	bool odd;
-	dim3 grid, block;
+	int kernel;		   // KERNEL_DIRECT or KERNEL_TILE
+	dim3 grid, block;  // direct kernel launch shape
+	int* status;	   // device status word (STATUS_* bits)
 	cudaStream_t stream;
+	long long* blocks_out;	// number of blocks the launch used (partials)
+	bool dry_run;			// only resolve launch facts (attributes, grid), launch nothing
 };
+
+// step kernel variants: one thread per site with direct loads, or the
+// persistent bulk-copy pipeline of aa_tile.cuh
+enum : int
+{
+	KERNEL_DIRECT = 0,
+	KERNEL_TILE = 1
+};
+// upper bound of the tile kernel's grid (blocks per SM x SMs)
+constexpr int TILE_MAX_BLOCKS_PER_SM = 8;
 
 struct StorageOps
 {
@@ -81,7 +95,10 @@ const StorageOps& storage_ops(int storage);
 
 // FP64 reductions shared by all storages (lbm_reduce.cu)
 constexpr int NRED_HOST = 6;
-cudaError_t finish_sums(const double* partials, long long nblocks, double* out, cudaStream_t);
+// partials are stored as [NRED][nblocks]; stage is scratch of
+// finish_scratch_doubles() doubles
+long long finish_scratch_doubles();
+cudaError_t finish_sums(const double* partials, long long nblocks, double* stage, double* out, cudaStream_t);
 // enstrophy-type sum rho * |grad u|^2 with central differences over the macro
 // field (compute type given by compute_size), periodic wrap as sim_4.cu:21-54
 cudaError_t enstrophy_partials(const void* macro, int compute_size, int X, int Y, int Z, double* partials, long long* nblocks,

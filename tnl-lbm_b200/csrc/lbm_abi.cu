@@ -129,6 +129,10 @@ struct lbm_lattice
 	bool sums_valid = false;
 	long long iteration = 0;
 	int bx = 0, by = 0;	 // 0: default
+	int kernel = lbm::KERNEL_TILE;
+	int sms = 148;
+	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
+	long long last_blocks = 0;	// blocks of the last step launch
 	lbm::CollParamsD p{};
 	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
 	cudaGraphExec_t graph = nullptr;
@@ -154,6 +158,13 @@ struct lbm_lattice
 	{
 		const dim3 gr = grid();
 		return (long long) gr.x * gr.y * gr.z;
+	}
+	// partial-sum slots any step kernel variant may need
+	long long max_step_blocks() const
+	{
+		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
+		const long long direct = grid_blocks();
+		return tile > direct ? tile : direct;
 	}
 	void drop_graph()
 	{
@@ -183,7 +194,8 @@ int ensure_partials(lbm_handle h, long long blocks)
 		cudaFree(h->partials);
 	h->partials = nullptr;
 	h->partials_cap = 0;
-	LBM_CUDA(cudaMalloc(&h->partials, (size_t) blocks * lbm::NRED_HOST * sizeof(double)));
+	// per-block partials [NRED][blocks] followed by the finish-stage scratch
+	LBM_CUDA(cudaMalloc(&h->partials, ((size_t) blocks * lbm::NRED_HOST + lbm::finish_scratch_doubles()) * sizeof(double)));
 	h->partials_cap = blocks;
 	return LBM_OK;
 }
@@ -196,7 +208,7 @@ int ensure_macro(lbm_handle h)
 	return LBM_OK;
 }
 
-int launch_step(lbm_handle h, bool macro, bool sums)
+int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 {
 	lbm::StepLaunch L{};
 	L.g = h->g;
@@ -212,9 +224,17 @@ int launch_step(lbm_handle h, bool macro, bool sums)
 	L.grid = h->grid();
 	L.block = h->block();
 	L.stream = h->stream;
+	L.kernel = h->kernel;
+	L.status = h->status_dev;
+	long long blocks = 0;
+	L.blocks_out = &blocks;
+	L.dry_run = dry_run;
 	const cudaError_t err = h->ops->step(L);
 	if (err != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(err));
+	if (dry_run)
+		return LBM_OK;
+	h->last_blocks = blocks;
 	h->iteration++;
 	return LBM_OK;
 }
@@ -223,6 +243,15 @@ int build_graph(lbm_handle h)
 {
 	h->drop_graph();
 	const long long saved = h->iteration;
+	// resolve per-kernel launch attributes outside of the capture
+	for (int parity = 0; parity < 2; parity++) {
+		h->iteration = parity;
+		int rc = launch_step(h, false, false, true);
+		if (rc) {
+			h->iteration = saved;
+			return rc;
+		}
+	}
 	h->iteration = 0;  // graph starts at an even step
 	cudaGraph_t graph = nullptr;
 	LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -324,7 +353,11 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 	const int es = h->ops->elem_size;
 	const int align = 128 / es;	 // elements per 128 bytes
 	h->g.x0 = align;
-	h->g.sy = ((align + d.X + 1 + align - 1) / align) * align;
+	// row: x0 elements of front pad (ghost x = -1 at x0 - 1), X interior sites,
+	// and room for the tile kernel's odd-step window, which reaches up to
+	// 2 x (16 bytes) beyond the last site
+	const int a16 = 16 / es;
+	h->g.sy = ((align + d.X + 2 * a16 + align - 1) / align) * align;
 	h->g.sz = h->g.sy * (d.Y + 2);
 	h->g.sq = (long long) h->g.sz * (d.Z + 2);
 	h->g.X = d.X;
@@ -354,7 +387,10 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 	if (cudaMalloc(&h->sums_dev, lbm::NRED_HOST * sizeof(double)) != cudaSuccess
 		|| cudaMallocHost(&h->sums_host, lbm::NRED_HOST * sizeof(double)) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "reduction buffers allocation failed"));
-	int rc = ensure_partials(h, h->grid_blocks());
+	if (cudaMalloc(&h->status_dev, sizeof(int)) != cudaSuccess || cudaMemsetAsync(h->status_dev, 0, sizeof(int), h->stream) != cudaSuccess)
+		return cleanup(fail(LBM_ERR_CUDA, "status word allocation failed"));
+	cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, d.device);
+	int rc = ensure_partials(h, h->max_step_blocks());
 	if (rc)
 		return cleanup(rc);
 	*out = h;
@@ -378,6 +414,7 @@ int lbm_destroy(lbm_handle h)
 		cudaFreeHost(h->inflow_host);
 	cudaFree(h->partials);
 	cudaFree(h->sums_dev);
+	cudaFree(h->status_dev);
 	if (h->sums_host)
 		cudaFreeHost(h->sums_host);
 	if (h->stream)
@@ -574,12 +611,13 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 	if (macro || sums) {
 		if (macro && (rc = ensure_macro(h)))
 			return rc;
-		if (sums && (rc = ensure_partials(h, h->grid_blocks())))
+		if (sums && (rc = ensure_partials(h, h->max_step_blocks())))
 			return rc;
 		if ((rc = launch_step(h, macro, sums)))
 			return rc;
 		if (sums) {
-			const cudaError_t e = lbm::finish_sums(h->partials, h->grid_blocks(), h->sums_dev, h->stream);
+			const long long nb = h->last_blocks;
+			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->sums_dev, h->stream);
 			if (e != cudaSuccess)
 				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
 			LBM_CUDA(cudaMemcpyAsync(h->sums_host, h->sums_dev, lbm::NRED_HOST * sizeof(double), cudaMemcpyDeviceToHost,
@@ -663,7 +701,7 @@ int lbm_enstrophy_sum(lbm_handle h, double* out)
 	LBM_CUDA(cudaMallocAsync((void**) &dres, lbm::NRED_HOST * sizeof(double), h->stream));
 	cudaError_t e = lbm::enstrophy_partials(h->macro, h->ops->compute_size, h->d.X, h->d.Y, h->d.Z, h->partials, &nb, h->stream);
 	if (e == cudaSuccess)
-		e = lbm::finish_sums(h->partials, nb, dres, h->stream);
+		e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, dres, h->stream);
 	double res[lbm::NRED_HOST];
 	if (e == cudaSuccess)
 		e = cudaMemcpyAsync(res, dres, sizeof(res), cudaMemcpyDeviceToHost, h->stream);
@@ -697,7 +735,7 @@ int lbm_set_block(lbm_handle h, int bx, int by)
 		h->by = by;
 	}
 	h->drop_graph();
-	return ensure_partials(h, h->grid_blocks());
+	return ensure_partials(h, h->max_step_blocks());
 }
 
 int lbm_get_block(lbm_handle h, int* bx, int* by)
@@ -737,7 +775,8 @@ int lbm_autotune(lbm_handle h, int ntrials)
 			continue;  // far wider than the lattice
 		h->bx = c[0];
 		h->by = c[1];
-		if (ensure_partials(h, h->grid_blocks()))
+		h->kernel = lbm::KERNEL_DIRECT;
+		if (ensure_partials(h, h->max_step_blocks()))
 			break;
 		// warm-up pair, then timed steps
 		launch_step(h, false, false);
@@ -755,6 +794,24 @@ int lbm_autotune(lbm_handle h, int ntrials)
 			bby = c[1];
 		}
 	}
+	// the tile kernel (block shape does not apply to it)
+	int best_kernel = lbm::KERNEL_DIRECT;
+	{
+		h->kernel = lbm::KERNEL_TILE;
+		launch_step(h, false, false);
+		launch_step(h, false, false);
+		cudaEventRecord(e0, h->stream);
+		for (int s = 0; s < ntrials; s++)
+			launch_step(h, false, false);
+		cudaEventRecord(e1, h->stream);
+		cudaEventSynchronize(e1);
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		if (ms < best) {
+			best = ms;
+			best_kernel = lbm::KERNEL_TILE;
+		}
+	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	h->iteration = it0;
@@ -769,8 +826,41 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	}
 	h->bx = bbx;
 	h->by = bby;
+	h->kernel = best_kernel;
 	h->drop_graph();
-	return ensure_partials(h, h->grid_blocks());
+	return ensure_partials(h, h->max_step_blocks());
+}
+
+int lbm_set_kernel(lbm_handle h, int kernel)
+{
+	if (int rc = check(h))
+		return rc;
+	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE)
+		return fail(LBM_ERR_INVALID, "unknown kernel %d", kernel);
+	h->kernel = kernel;
+	h->drop_graph();
+	return LBM_OK;
+}
+
+int lbm_get_kernel(lbm_handle h, int* kernel)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!kernel)
+		return fail(LBM_ERR_INVALID, "null output");
+	*kernel = h->kernel;
+	return LBM_OK;
+}
+
+int lbm_status(lbm_handle h, int* status)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!status)
+		return fail(LBM_ERR_INVALID, "null output");
+	LBM_CUDA(cudaMemcpyAsync(status, h->status_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	return LBM_OK;
 }
 
 int lbm_device_view_get(lbm_handle h, lbm_device_view* out)

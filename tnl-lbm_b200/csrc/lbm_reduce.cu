@@ -11,35 +11,67 @@
 
 namespace lbm {
 
-// one block; each thread accumulates a strided subset of the partials in a
-// fixed order, then a fixed tree combines them, so the result does not depend
-// on scheduling
-__global__ void finish_sums_kernel(const double* __restrict__ partials, long long nblocks, double* __restrict__ out)
+// Two-stage deterministic finish of the per-block partial sums, stored as
+// partials[k][nblocks].  Stage 1: FINISH_BLOCKS blocks, each summing a fixed
+// contiguous chunk of every quantity in a fixed order; stage 2: one block
+// summing the stage-1 results.  The result does not depend on scheduling.
+constexpr int FINISH_THREADS = 256;
+constexpr int FINISH_BLOCKS = 296;
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
 {
-	__shared__ double acc[256][NRED];
-	double v[NRED] = {0, 0, 0, 0, 0, 0};
-	for (long long b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-		for (int k = 0; k < NRED; k++)
-			v[k] += partials[b * NRED + k];
-#pragma unroll
-	for (int k = 0; k < NRED; k++)
-		acc[threadIdx.x][k] = v[k];
+	sh[threadIdx.x] = v;
 	__syncthreads();
-	for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+	for (int s = FINISH_THREADS / 2; s > 0; s >>= 1) {
 		if ((int) threadIdx.x < s)
-#pragma unroll
-			for (int k = 0; k < NRED; k++)
-				acc[threadIdx.x][k] += acc[threadIdx.x + s][k];
+			sh[threadIdx.x] += sh[threadIdx.x + s];
 		__syncthreads();
 	}
-	if (threadIdx.x < NRED)
-		out[threadIdx.x] = acc[0][threadIdx.x];
+	const double r = sh[0];
+	__syncthreads();
+	return r;
 }
 
-cudaError_t finish_sums(const double* partials, long long nblocks, double* out, cudaStream_t st)
+__global__ void __launch_bounds__(FINISH_THREADS) finish_stage1(const double* __restrict__ partials, long long nblocks,
+																double* __restrict__ stage)
 {
-	finish_sums_kernel<<<1, 256, 0, st>>>(partials, nblocks, out);
+	__shared__ double sh[FINISH_THREADS];
+	const long long chunk = (nblocks + gridDim.x - 1) / gridDim.x;
+	const long long b0 = blockIdx.x * chunk;
+	const long long b1 = b0 + chunk < nblocks ? b0 + chunk : nblocks;
+	for (int k = 0; k < NRED; k++) {
+		double v = 0;
+		for (long long b = b0 + threadIdx.x; b < b1; b += FINISH_THREADS)
+			v += partials[k * nblocks + b];
+		const double r = block_sum(v, sh);
+		if (threadIdx.x == 0)
+			stage[k * gridDim.x + blockIdx.x] = r;
+	}
+}
+
+__global__ void __launch_bounds__(FINISH_THREADS) finish_stage2(const double* __restrict__ stage, int nstage,
+																double* __restrict__ out)
+{
+	__shared__ double sh[FINISH_THREADS];
+	for (int k = 0; k < NRED; k++) {
+		double v = 0;
+		for (int b = threadIdx.x; b < nstage; b += FINISH_THREADS)
+			v += stage[k * nstage + b];
+		const double r = block_sum(v, sh);
+		if (threadIdx.x == 0)
+			out[k] = r;
+	}
+}
+
+long long finish_scratch_doubles()
+{
+	return (long long) FINISH_BLOCKS * NRED;
+}
+
+cudaError_t finish_sums(const double* partials, long long nblocks, double* stage, double* out, cudaStream_t st)
+{
+	finish_stage1<<<FINISH_BLOCKS, FINISH_THREADS, 0, st>>>(partials, nblocks, stage);
+	finish_stage2<<<1, FINISH_THREADS, 0, st>>>(stage, FINISH_BLOCKS, out);
 	return cudaGetLastError();
 }
 

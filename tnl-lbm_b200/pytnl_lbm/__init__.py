@@ -19,8 +19,8 @@ import numpy as np
 from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
     COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
-    GEO, LAYOUT_GHOST, LAYOUT_INTERIOR, STEP_MACRO, STEP_SUMS, STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S,
-    STORE_F64, LbmError, library, library_path)
+    GEO, KERNEL_DIRECT, KERNEL_TILE, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
+    STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
 
 __all__ = ["LBM", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
 
@@ -159,6 +159,20 @@ class LBM:
         bx, by = ctypes.c_int(0), ctypes.c_int(0)
         _abi.check(self.lib.lbm_get_block(self.h, ctypes.byref(bx), ctypes.byref(by)))
         return bx.value, by.value
+
+    def set_kernel(self, kernel):
+        _abi.check(self.lib.lbm_set_kernel(self.h, int(kernel)))
+
+    @property
+    def kernel(self):
+        k = ctypes.c_int(0)
+        _abi.check(self.lib.lbm_get_kernel(self.h, ctypes.byref(k)))
+        return k.value
+
+    def status(self):
+        v = ctypes.c_int(0)
+        _abi.check(self.lib.lbm_status(self.h, ctypes.byref(v)))
+        return v.value
 
     def autotune(self, ntrials=4):
         _abi.check(self.lib.lbm_autotune(self.h, int(ntrials)))

@@ -15,6 +15,8 @@ CUM_GEIER_2017, CUM_ANTIALIAS = 1, 2
 EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
 LAYOUT_INTERIOR, LAYOUT_GHOST = 0, 1
 STEP_MACRO, STEP_SUMS = 1, 2
+KERNEL_DIRECT, KERNEL_TILE = 0, 1
+STATUS_TIMEOUT = 1
 
 # GEO site types of D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43)
 GEO = dict(FLUID=0, WALL=1, INFLOW=2, INFLOW_LEFT=3, INFLOW_BB_LEFT=4, INFLOW_EQ_LEFT=5, OUTFLOW_EQ=6,
@@ -69,6 +71,9 @@ SIGNATURES = {
     "lbm_get_block": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "lbm_autotune": (ctypes.c_int, [_H, ctypes.c_int]),
     "lbm_device_view_get": (ctypes.c_int, [_H, ctypes.POINTER(lbm_device_view)]),
+    "lbm_set_kernel": (ctypes.c_int, [_H, ctypes.c_int]),
+    "lbm_get_kernel": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
+    "lbm_status": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_version": (ctypes.c_char_p, []),
 }
 
