@@ -57,7 +57,7 @@ struct StorageUnit
 	{
 		auto kern = aa_tile_kernel<S, COLL, CUMF, ODD, GENERAL, TILE_X, TILE_STAGES>;
 		constexpr int smem = tile_smem_bytes<T, TILE_X, ODD, TILE_STAGES>();
-		constexpr int threads = TILE_X + 32;
+		constexpr int threads = TILE_X;
 		// per-device launch facts of this instantiation, computed once
 		static int per_sm_cache[64] = {0};
 		static int sms_cache[64] = {0};

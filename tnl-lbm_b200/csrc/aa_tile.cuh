@@ -1,13 +1,14 @@
 // Persistent, warp-specialised A-A step kernel for sm_100a.
 //
-// Each CTA owns one producer warp and TX consumer threads (one lattice site
-// per consumer thread).  The CTA walks over row tiles (TX consecutive sites of
-// one (y, z) row) in a grid-stride loop.  For every tile the producer issues
-// 27 bulk copies (cp.async.bulk, one per population direction) of the rows the
-// tile's A-A read needs into a STAGES-deep shared-memory ring, signalled by
-// mbarrier transaction counts; the consumers read their 27 values from shared
-// memory, apply boundary conditions and the collision, and store to HBM with
-// ordinary coalesced stores.  The number of bytes in flight per SM is set by
+// Each CTA has TX threads, one lattice site per thread, and walks over row
+// tiles (TX consecutive sites of one (y, z) row) in a grid-stride loop.  For
+// every tile, lanes 0..26 of warp 0 issue 27 bulk copies (cp.async.bulk, one
+// per population direction) of the rows the tile's A-A read needs into a
+// STAGES-deep shared-memory ring, signalled by mbarrier transaction counts; a
+// stage is refilled as soon as all warps have released it.  All threads read
+// their 27 values from shared memory, apply boundary conditions and the
+// collision, and store to HBM with ordinary coalesced stores.  No warp is set
+// aside as a producer, so every register of the CTA does site work.  The number of bytes in flight per SM is set by
 // the ring depth, not by the registers a thread can spare for loads.
 //
 // Odd step: direction q of the site at x comes from slot opp(q) of the site
@@ -103,8 +104,48 @@ constexpr int tile_smem_bytes()
 	return STAGES * TileShape<T, TX, ODD>::STAGE_BYTES + 2 * STAGES * 8;
 }
 
+// Issue the 27 bulk copies of one tile into stage s (called by warp 0; lane q
+// copies the window of slot q).
+template <typename S, bool ODD, bool GENERAL, int TX, int STAGES>
+__device__ __forceinline__ void issue_tile(const StepArgs<typename S::T, typename S::R>& a, typename S::T* ring,
+										   uint64_t* full, int s, long long t, int tiles_x, int lane)
+{
+	using T = typename S::T;
+	using Shape = TileShape<T, TX, ODD>;
+	constexpr int A = Shape::A;
+	constexpr int W = Shape::W;
+	const int xt = (int) (t % tiles_x);
+	const long long row = t / tiles_x;
+	const int y = (int) (row % a.Y);
+	const int z = (int) (row / a.Y);
+	const int xs = xt * TX;
+	const int n = min(TX, a.X - xs);
+	const int n_al = (n + A - 1) / A * A;
+	const uint32_t bytes = (uint32_t) ((ODD ? n_al + 2 * A : n_al) * (int) sizeof(T));
+	if (lane == 0)
+		mbar_arrive_expect_tx(&full[s], 27 * bytes);
+	__syncwarp();
+	if (lane < 27) {
+		const int q = lane;
+		long long src;
+		if (ODD) {
+			// slot q of the sites x + c_q: read there by site x as direction opp(q)
+			int yy = y + cy_rt(q), zz = z + cz_rt(q);
+			if (!GENERAL) {
+				yy = yy < 0 ? a.Y - 1 : (yy >= a.Y ? 0 : yy);
+				zz = zz < 0 ? a.Z - 1 : (zz >= a.Z ? 0 : zz);
+			}
+			src = (long long) q * a.sq + (long long) (zz + 1) * a.sz + (long long) (yy + 1) * a.sy + a.x0 + xs - A;
+		}
+		else {
+			src = (long long) q * a.sq + (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + xs;
+		}
+		bulk_g2s(ring + (long long) s * 27 * W + q * W, a.f + src, bytes, &full[s]);
+	}
+}
+
 template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, int TX, int STAGES>
-__global__ void __launch_bounds__(TX + 32, LBM_TILE_MINB)
+__global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 	aa_tile_kernel(const StepArgs<typename S::T, typename S::R> a, int* status, long long ntiles, int tiles_x)
 {
 	using R = typename S::R;
@@ -112,6 +153,7 @@ __global__ void __launch_bounds__(TX + 32, LBM_TILE_MINB)
 	using Shape = TileShape<T, TX, ODD>;
 	constexpr int A = Shape::A;
 	constexpr int W = Shape::W;
+	constexpr int WARPS = TX / 32;
 
 	extern __shared__ __align__(128) unsigned char smem_raw[];
 	T* ring = reinterpret_cast<T*>(smem_raw);
@@ -119,13 +161,13 @@ __global__ void __launch_bounds__(TX + 32, LBM_TILE_MINB)
 	uint64_t* empty = full + STAGES;
 
 	const int tid = threadIdx.x;
-	const bool producer = tid >= TX;
-	constexpr int CONSUMER_WARPS = TX / 32;
+	const int lane = tid & 31;
+	const bool warp0 = tid < 32;
 
 	if (tid == 0) {
 		for (int s = 0; s < STAGES; s++) {
 			mbar_init(&full[s], 1);
-			mbar_init(&empty[s], CONSUMER_WARPS);
+			mbar_init(&empty[s], WARPS);
 		}
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -134,159 +176,125 @@ __global__ void __launch_bounds__(TX + 32, LBM_TILE_MINB)
 	const long long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 	double red[NRED] = {0, 0, 0, 0, 0, 0};
 	bool timed_out = false;
+	long long issued = 0;
 
-	if (producer) {
-		// ---------------- producer warp: lanes 0..26 each copy one direction row
-		const int lane = tid - TX;
-		long long issued = 0;
-		for (long long i = 0; i < my_tiles; i++) {
-			const int s = (int) (i % STAGES);
-			if (i >= STAGES) {
-				const uint32_t parity = (uint32_t) ((i / STAGES - 1) & 1);
-				bool ok = true;
-				if (lane == 0)
-					ok = mbar_wait(&empty[s], parity);
-				ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-				if (!ok) {
-					timed_out = true;
-					break;
-				}
-			}
-			const long long t = blockIdx.x + i * gridDim.x;
-			const int xt = (int) (t % tiles_x);
-			const long long row = t / tiles_x;
-			const int y = (int) (row % a.Y);
-			const int z = (int) (row / a.Y);
-			const int xs = xt * TX;
-			const int n = min(TX, a.X - xs);
-			const int n_al = (n + A - 1) / A * A;
-			const uint32_t bytes = (uint32_t) ((ODD ? n_al + 2 * A : n_al) * (int) sizeof(T));
-			if (lane == 0)
-				mbar_arrive_expect_tx(&full[s], 27 * bytes);
-			__syncwarp();
-			if (lane < 27) {
-				const int q = lane;	 // the window of slot q
-				long long src;
-				if (ODD) {
-					// slot q at rows (y + c_q): read by the site x = x' + c_q as direction opp(q)
-					int yy = y + cy(q), zz = z + cz(q);
-					if (!GENERAL) {
-						yy = yy < 0 ? a.Y - 1 : (yy >= a.Y ? 0 : yy);
-						zz = zz < 0 ? a.Z - 1 : (zz >= a.Z ? 0 : zz);
-					}
-					src = (long long) q * a.sq + (long long) (zz + 1) * a.sz + (long long) (yy + 1) * a.sy + a.x0 + xs - A;
-				}
-				else {
-					src = (long long) q * a.sq + (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + xs;
-				}
-				bulk_g2s(ring + (long long) s * 27 * W + q * W, a.f + src, bytes, &full[s]);
-			}
-			issued = i + 1;
-		}
-		// drain: every issued stage must have landed before the CTA exits
-		if (tid == TX) {
-			const long long first = issued > STAGES ? issued - STAGES : 0;
-			for (long long i = first; i < issued; i++) {
-				const int s = (int) (i % STAGES);
-				mbar_wait(&full[s], (uint32_t) ((i / STAGES) & 1));
-			}
-		}
-		if (timed_out && tid == TX)
-			atomicOr(status, STATUS_TIMEOUT);
+	// prologue: warp 0 fills the ring
+	if (warp0) {
+		for (long long i = 0; i < STAGES && i < my_tiles; i++)
+			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, (int) i, blockIdx.x + i * gridDim.x, tiles_x, lane);
+		issued = my_tiles < STAGES ? my_tiles : STAGES;
 	}
-	else {
-		// ---------------- consumers: one site per thread
-		for (long long i = 0; i < my_tiles; i++) {
-			const int s = (int) (i % STAGES);
-			if (!mbar_wait(&full[s], (uint32_t) ((i / STAGES) & 1))) {
+
+	for (long long i = 0; i < my_tiles; i++) {
+		const int s = (int) (i % STAGES);
+		if (!mbar_wait(&full[s], (uint32_t) ((i / STAGES) & 1))) {
+			timed_out = true;
+			break;
+		}
+		const long long t = blockIdx.x + i * gridDim.x;
+		const int xt = (int) (t % tiles_x);
+		const long long row = t / tiles_x;
+		const int y = (int) (row % a.Y);
+		const int z = (int) (row / a.Y);
+		const int x = xt * TX + tid;
+		const bool active = x < a.X;
+		const T* st = ring + (long long) s * 27 * W;
+
+		Site<R> site;
+		// slot q's window holds direction opp(q) of the tile's sites (odd step)
+		// or direction q (even step)
+		if (active) {
+			static_for<27>(
+				[&](auto Qc)
+				{
+					constexpr int q = decltype(Qc)::value;
+					if constexpr (ODD)
+						site.f[q] = S::template load_smem<opp(q)>(st + opp(q) * W + A - cx(q) + tid);
+					else
+						site.f[q] = S::template load_smem<q>(st + q * W + tid);
+				}
+			);
+		}
+		__syncwarp();
+		if (lane == 0)
+			mbar_arrive(&empty[s]);
+		// warp 0 refills stage s with tile i + STAGES once every warp has read it
+		if (warp0 && i + STAGES < my_tiles) {
+			bool ok = true;
+			if (lane == 0)
+				ok = mbar_wait(&empty[s], (uint32_t) ((i / STAGES) & 1));
+			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+			if (!ok) {
 				timed_out = true;
 				break;
 			}
-			const long long t = blockIdx.x + i * gridDim.x;
-			const int xt = (int) (t % tiles_x);
-			const long long row = t / tiles_x;
-			const int y = (int) (row % a.Y);
-			const int z = (int) (row / a.Y);
-			const int x = xt * TX + tid;
-			const bool active = x < a.X;
-			const T* st = ring + (long long) s * 27 * W;
+			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, s, blockIdx.x + (i + STAGES) * gridDim.x, tiles_x, lane);
+			issued = i + STAGES + 1;
+		}
+		if (!active)
+			continue;
 
-			Site<R> site;
-			// read the 27 populations from the stage: slot q's window holds
-			// direction opp(q) of the sites (odd) or direction q (even)
-			if (active) {
-				static_for<27>(
-					[&](auto Qc)
-					{
-						constexpr int q = decltype(Qc)::value;
-						if constexpr (ODD)
-							site.f[q] = S::template load_smem<opp(q)>(st + opp(q) * W + A - cx(q) + tid);
-						else
-							site.f[q] = S::template load_smem<q>(st + q * W + tid);
-					}
-				);
-			}
-			__syncwarp();
-			if ((tid & 31) == 0)
-				mbar_arrive(&empty[s]);
-			if (!active)
-				continue;
-
-			const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-			const long long sidx = ((long long) z * a.Y + y) * a.X + x;
-			uint8_t geo = GEO_PERIODIC;
+		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+		const long long sidx = ((long long) z * a.Y + y) * a.X + x;
+		uint8_t geo = GEO_PERIODIC;
+		if constexpr (GENERAL)
+			geo = a.map[sidx];
+		const bool wrap = !GENERAL || geo == GEO_PERIODIC;
+		const Offsets o = neighbour_offsets(wrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		if constexpr (ODD) {
+			// sites on a periodic face: the wrapped neighbours are not in the window
+			bool face;
 			if constexpr (GENERAL)
-				geo = a.map[sidx];
-			const bool wrap = !GENERAL || geo == GEO_PERIODIC;
-			const Offsets o = neighbour_offsets(wrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-			if constexpr (ODD) {
-				// sites on a periodic face: the wrapped neighbours are not in the window
-				bool face;
-				if constexpr (GENERAL)
-					face = wrap && (x == 0 || x == a.X - 1 || y == 0 || y == a.Y - 1 || z == 0 || z == a.Z - 1);
-				else
-					face = x == 0 || x == a.X - 1;
-				if (face)
-					aa_read<S, true>(a.f, a.sq, base, o, site.f);
-			}
-			bool store = true, coll = true;
-			if constexpr (GENERAL) {
-				if (geo == GEO_NOTHING) {
-					site.rho = R(1);
-					site.vx = site.vy = site.vz = R(0);
-					store = false;
-					coll = false;
-				}
-				else {
-					coll = apply_boundary(site, geo, a, z, y);
-				}
+				face = wrap && (x == 0 || x == a.X - 1 || y == 0 || y == a.Y - 1 || z == 0 || z == a.Z - 1);
+			else
+				face = x == 0 || x == a.X - 1;
+			if (face)
+				aa_read<S, true>(a.f, a.sq, base, o, site.f);
+		}
+		bool store = true, coll = true;
+		if constexpr (GENERAL) {
+			if (geo == GEO_NOTHING) {
+				site.rho = R(1);
+				site.vx = site.vy = site.vz = R(0);
+				store = false;
+				coll = false;
 			}
 			else {
-				density_velocity(site, a.p);
-			}
-			if (coll)
-				collide<R, COLL, CUMF>(site, a.p);
-			if (store)
-				aa_write<S, ODD>(a.f, a.sq, base, o, site.f);
-			if (a.macro) {
-				const long long nsites = (long long) a.X * a.Y * a.Z;
-				a.macro[sidx] = site.rho;
-				a.macro[nsites + sidx] = site.vx;
-				a.macro[2 * nsites + sidx] = site.vy;
-				a.macro[3 * nsites + sidx] = site.vz;
-			}
-			if (a.partials) {
-				const double rho = (double) site.rho, vx = (double) site.vx, vy = (double) site.vy, vz = (double) site.vz;
-				red[0] += rho;
-				red[1] += rho * vx;
-				red[2] += rho * vy;
-				red[3] += rho * vz;
-				red[4] += rho * (vx * vx + vy * vy + vz * vz);
-				red[5] += isfinite(rho) ? 0.0 : 1.0;
+				coll = apply_boundary(site, geo, a, z, y);
 			}
 		}
-		if (timed_out && (tid & 31) == 0)
-			atomicOr(status, STATUS_TIMEOUT);
+		else {
+			density_velocity(site, a.p);
+		}
+		if (coll)
+			collide<R, COLL, CUMF>(site, a.p);
+		if (store)
+			aa_write<S, ODD>(a.f, a.sq, base, o, site.f);
+		if (a.macro) {
+			const long long nsites = (long long) a.X * a.Y * a.Z;
+			a.macro[sidx] = site.rho;
+			a.macro[nsites + sidx] = site.vx;
+			a.macro[2 * nsites + sidx] = site.vy;
+			a.macro[3 * nsites + sidx] = site.vz;
+		}
+		if (a.partials) {
+			const double rho = (double) site.rho, vx = (double) site.vx, vy = (double) site.vy, vz = (double) site.vz;
+			red[0] += rho;
+			red[1] += rho * vx;
+			red[2] += rho * vy;
+			red[3] += rho * vz;
+			red[4] += rho * (vx * vx + vy * vy + vz * vz);
+			red[5] += isfinite(rho) ? 0.0 : 1.0;
+		}
+	}
+	if (timed_out && lane == 0)
+		atomicOr(status, STATUS_TIMEOUT);
+	// drain: no copy issued by this CTA may land after it exits (only reachable
+	// with copies outstanding after a timeout)
+	if (warp0 && lane == 0) {
+		const long long first = issued > STAGES ? issued - STAGES : 0;
+		for (long long i = first; i < issued; i++)
+			mbar_wait(&full[(int) (i % STAGES)], (uint32_t) ((i / STAGES) & 1));
 	}
 	if (a.partials)
 		block_reduce_store<R>(red, a.partials);

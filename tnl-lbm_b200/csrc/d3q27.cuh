@@ -38,6 +38,29 @@ __host__ __device__ constexpr int opp(int q)
 {
 	return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1);
 }
+// velocity components for a runtime direction index: (c + 1) packed in 2 bits
+// per direction into one 64-bit constant, so that no table is materialised
+__host__ __device__ constexpr unsigned long long pack_components(int axis)
+{
+	unsigned long long p = 0;
+	for (int q = 0; q < 27; q++) {
+		const int c = axis == 0 ? cx(q) : (axis == 1 ? cy(q) : cz(q));
+		p |= (unsigned long long) (c + 1) << (2 * q);
+	}
+	return p;
+}
+__host__ __device__ __forceinline__ int cx_rt(int q)
+{
+	return (int) ((pack_components(0) >> (2 * q)) & 3ull) - 1;
+}
+__host__ __device__ __forceinline__ int cy_rt(int q)
+{
+	return (int) ((pack_components(1) >> (2 * q)) & 3ull) - 1;
+}
+__host__ __device__ __forceinline__ int cz_rt(int q)
+{
+	return (int) ((pack_components(2) >> (2 * q)) & 3ull) - 1;
+}
 // number of non-zero velocity components: 0 rest, 1 face, 2 edge, 3 corner
 __host__ __device__ constexpr int nnz(int q)
 {
