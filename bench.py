@@ -174,7 +174,7 @@ def max_over_ranks(dist, value, device):
     return float(t.item())
 
 
-def make_lattice(pl, spec, storage, device, kernel="tile"):
+def make_lattice(pl, spec, storage, device, kernel="direct"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
@@ -299,7 +299,7 @@ def run_ours(args):
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
                        "step_kernel": args.kernel,
-                       "block": list(block) if args.kernel == "direct" else "persistent tile kernel, 128+32 threads"},
+                       "block": list(block) if args.kernel == "direct" else "persistent tile kernel, 128 threads"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -432,7 +432,7 @@ def main():
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--autotune", action="store_true")
-    ap.add_argument("--kernel", default="tile", choices=["tile", "direct"])
+    ap.add_argument("--kernel", default="direct", choices=["direct", "tile"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

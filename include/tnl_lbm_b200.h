@@ -168,10 +168,10 @@ LBM_API int lbm_get_block(lbm_handle h, int* bx, int* by);
  * get_optimal_block_size (include/lbm3d/block_size_optimizer.h:18-111). */
 LBM_API int lbm_autotune(lbm_handle h, int ntrials);
 
-/* Step kernel: LBM_KERNEL_TILE (default) is the persistent kernel that
- * streams population rows into shared memory with bulk copies;
- * LBM_KERNEL_DIRECT is one thread per site with direct loads.  Both compute
- * the same update. */
+/* Step kernel: LBM_KERNEL_DIRECT (default) is one thread per site with
+ * direct coalesced loads and stores; LBM_KERNEL_TILE is a persistent kernel
+ * that streams population rows into shared memory with bulk copies.  Both
+ * compute the same update, bit for bit. */
 #define LBM_KERNEL_DIRECT 0
 #define LBM_KERNEL_TILE 1
 LBM_API int lbm_set_kernel(lbm_handle h, int kernel);

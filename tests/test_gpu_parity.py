@@ -287,7 +287,7 @@ def test_nonfinite_density_is_reported(pl):
 
 
 @pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S"])
-@pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5)])
+@pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5), (37, 9, 7), (5, 4, 3)])
 def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
     """The two step kernels are the same update: equal results, bit for bit,
     on lattices whose width is a multiple of, larger than, or smaller than a

@@ -118,19 +118,31 @@ __device__ __forceinline__ void aa_write(typename S::T* __restrict__ f, long lon
 	);
 }
 
-// mirror copy of a symmetry plane: directions whose AXIS component equals
-// SIDE take the value of their mirror image (bc.h:222-293)
-template <int AXIS, int SIDE, typename R>
-__device__ __forceinline__ void symmetry(R* f)
+// mirror copy of a symmetry plane (bc.h:222-293): directions whose component
+// along the plane normal equals `side` take the value of their mirror image.
+// One code path for all six GEO_SYM_* types, selected at run time: axis 0/1/2
+// = x/y/z; the sources (component -side) are never overwritten.
+template <typename R>
+__device__ __forceinline__ void symmetry(R* f, int axis, int side)
 {
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			constexpr int c = AXIS == 0 ? cx(q) : (AXIS == 1 ? cy(q) : cz(q));
-			if constexpr (c == SIDE) {
-				constexpr int m = dir(AXIS == 0 ? -cx(q) : cx(q), AXIS == 1 ? -cy(q) : cy(q), AXIS == 2 ? -cz(q) : cz(q));
-				f[q] = f[m];
+			if constexpr (cx(q) != 0) {
+				constexpr int m = dir(-cx(q), cy(q), cz(q));
+				if (axis == 0 && cx(q) == side)
+					f[q] = f[m];
+			}
+			if constexpr (cy(q) != 0) {
+				constexpr int m = dir(cx(q), -cy(q), cz(q));
+				if (axis == 1 && cy(q) == side)
+					f[q] = f[m];
+			}
+			if constexpr (cz(q) != 0) {
+				constexpr int m = dir(cx(q), cy(q), -cz(q));
+				if (axis == 2 && cz(q) == side)
+					f[q] = f[m];
 			}
 		}
 	);
@@ -220,29 +232,19 @@ __device__ __forceinline__ bool apply_boundary(Site<R>& s, uint8_t geo, const St
 			}
 			return false;
 		case GEO_SYM_TOP:
-			symmetry<2, -1>(s.f);
-			density_velocity(s, a.p);
-			return false;
 		case GEO_SYM_BOTTOM:
-			symmetry<2, 1>(s.f);
-			density_velocity(s, a.p);
-			return false;
 		case GEO_SYM_LEFT:
-			symmetry<0, 1>(s.f);
-			density_velocity(s, a.p);
-			return false;
 		case GEO_SYM_RIGHT:
-			symmetry<0, -1>(s.f);
-			density_velocity(s, a.p);
-			return false;
 		case GEO_SYM_BACK:
-			symmetry<1, 1>(s.f);
+		case GEO_SYM_FRONT: {
+			// TOP/BOTTOM: z, LEFT/RIGHT: x, BACK/FRONT: y; the overwritten side
+			// is -1 for TOP, RIGHT, FRONT and +1 for BOTTOM, LEFT, BACK
+			const int axis = geo <= GEO_SYM_BOTTOM ? 2 : (geo <= GEO_SYM_RIGHT ? 0 : 1);
+			const int side = (geo == GEO_SYM_TOP || geo == GEO_SYM_RIGHT || geo == GEO_SYM_FRONT) ? -1 : 1;
+			symmetry(s.f, axis, side);
 			density_velocity(s, a.p);
 			return false;
-		case GEO_SYM_FRONT:
-			symmetry<1, -1>(s.f);
-			density_velocity(s, a.p);
-			return false;
+		}
 		default:  // GEO_FLUID, GEO_PERIODIC
 			density_velocity(s, a.p);
 			return true;
@@ -279,12 +281,14 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* pa
 	}
 }
 
-// One A-A step over the whole lattice.  GENERAL = false: every site is
+// One A-A step over the whole lattice.  OUT = true compiles the macro-field
+// output and the FP64 partial sums (used on observation steps only), so the
+// plain step carries none of their registers.  GENERAL = false: every site is
 // periodic (no map read).  GENERAL = true: per-site GEO type from the map with
 // the boundary conditions of D3Q27_BC_All (bc.h:60-422) that are free of
 // cross-site ordering in the A-A pattern.
-template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, int MINB>
-__global__ void __launch_bounds__(256, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
 {
 	using R = typename S::R;
 	const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -319,14 +323,14 @@ __global__ void __launch_bounds__(256, MINB) aa_step_kernel(const StepArgs<typen
 			aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
 		}
 		(void) store;
-		if (a.macro) {
+		if (OUT && a.macro) {
 			const long long n = (long long) a.X * a.Y * a.Z;
 			a.macro[site] = s.rho;
 			a.macro[n + site] = s.vx;
 			a.macro[2 * n + site] = s.vy;
 			a.macro[3 * n + site] = s.vz;
 		}
-		if (a.partials) {
+		if (OUT && a.partials) {
 			const double rho = (double) s.rho, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
 			red[0] = rho;
 			red[1] = rho * vx;
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(256, MINB) aa_step_kernel(const StepArgs<typen
 			red[5] = isfinite(rho) ? 0.0 : 1.0;
 		}
 	}
-	if (a.partials)
+	if (OUT && a.partials)
 		block_reduce_store<R>(red, a.partials);
 }
 

@@ -1,5 +1,4 @@
 // Kernel instantiations for the bf16s population storage (StoreBF16S).
-#define LBM_STORE_MINB 2
 #define LBM_TILE_MINB 4
 #include "aa_store_impl.cuh"
 

@@ -1,5 +1,4 @@
 // Kernel instantiations for the f32s population storage (StoreF32S).
-#define LBM_STORE_MINB 2
 #define LBM_TILE_MINB 4
 #include "aa_store_impl.cuh"
 

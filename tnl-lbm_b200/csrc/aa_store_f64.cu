@@ -1,5 +1,4 @@
 // Kernel instantiations for the f64 population storage (StoreF64).
-#define LBM_STORE_MINB 1
 #define LBM_TILE_MINB 2
 #include "aa_store_impl.cuh"
 

@@ -1,6 +1,6 @@
 // Kernel instantiations for one population storage format.  Included by
-// aa_store_<format>.cu with LBM_STORE (the StoreXXX type), LBM_STORE_NAME and
-// LBM_STORE_MINB (min resident blocks in __launch_bounds__) defined.
+// aa_store_<format>.cu, which defines LBM_TILE_MINB (resident blocks of the
+// tile kernel) and names the storage type in LBM_DEFINE_STORAGE_OPS.
 #pragma once
 
 #include "aa_kernels.cuh"
@@ -41,6 +41,26 @@ inline CollParams<R> make_coll_params(const CollParamsD& d)
 	p.tau2 = (R) (d.tau * d.tau);
 	p.eq = d.eq;
 	return p;
+}
+
+// Resident 128-thread blocks per SM requested from the compiler for the
+// direct step kernel; __launch_bounds__(128, n) caps registers at
+// 65536 / (128 n): 4 -> 128, 5 -> 102 (96 used), 6 -> 85 (80 used).  The
+// values are the largest n at which each instantiation compiles without
+// register spills (-Xptxas -v on sm_100a): more resident warps keep more HBM
+// requests in flight.  The FP64 kernels need twice the registers per value.
+template <typename R, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
+constexpr int direct_minb()
+{
+	if (sizeof(R) == 8)
+		return 2;
+	if (OUT)
+		return 4;
+	if (!ODD && GENERAL)
+		return 6;
+	if (COLL == COLL_CUM || COLL == COLL_MRT)
+		return 5;
+	return 4;  // SRT and BGK spill at 5
 }
 
 template <typename S>
@@ -103,7 +123,12 @@ struct StorageUnit
 			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
 		if (L.dry_run)
 			return cudaSuccess;
-		aa_step_kernel<S, COLL, CUMF, ODD, GENERAL, LBM_STORE_MINB><<<L.grid, L.block, 0, L.stream>>>(a);
+		if (L.macro || L.partials)
+			aa_step_kernel<S, COLL, CUMF, ODD, GENERAL, true, direct_minb<R, COLL, CUMF, ODD, GENERAL, true>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a);
+		else
+			aa_step_kernel<S, COLL, CUMF, ODD, GENERAL, false, direct_minb<R, COLL, CUMF, ODD, GENERAL, false>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a);
 		return cudaGetLastError();
 	}
 

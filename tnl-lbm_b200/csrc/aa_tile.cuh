@@ -89,13 +89,60 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 				 : "memory");
 }
 
+// Tile t of the grid-stride walk, decomposed as t = (z*Y + y)*tiles_x + xt.
+// Consecutive tiles of one CTA differ by gridDim.x, so the cursor is advanced
+// with additions and at most two carries instead of 64-bit divisions.
+struct TileCursor
+{
+	int xt, y, z;
+};
+
+struct TileStride
+{
+	int dxt, dy, dz;
+};
+
+__device__ __forceinline__ TileCursor tile_at(long long t, int tiles_x, int Y)
+{
+	TileCursor c;
+	c.xt = (int) (t % tiles_x);
+	const long long row = t / tiles_x;
+	c.y = (int) (row % Y);
+	c.z = (int) (row / Y);
+	return c;
+}
+
+__device__ __forceinline__ TileStride tile_stride(long long g, int tiles_x, int Y)
+{
+	const TileCursor c = tile_at(g, tiles_x, Y);
+	return TileStride{c.xt, c.y, c.z};
+}
+
+__device__ __forceinline__ void tile_advance(TileCursor& c, const TileStride& d, int tiles_x, int Y)
+{
+	c.xt += d.dxt;
+	int carry = 0;
+	if (c.xt >= tiles_x) {
+		c.xt -= tiles_x;
+		carry = 1;
+	}
+	c.y += d.dy + carry;
+	carry = 0;
+	if (c.y >= Y) {
+		c.y -= Y;
+		carry = 1;
+	}
+	c.z += d.dz + carry;
+}
+
 template <typename T, int TX, bool ODD>
 struct TileShape
 {
 	static constexpr int A = 16 / (int) sizeof(T);	 // elements per 16 bytes
 	static constexpr int W = ODD ? TX + 2 * A : TX;	 // window width in elements
 	static constexpr int ROW_BYTES = W * (int) sizeof(T);
-	static constexpr int STAGE_BYTES = 27 * ROW_BYTES;
+	static constexpr int MAP_BYTES = TX + 32;		 // map row of the tile, from a 16-byte aligned start
+	static constexpr int STAGE_BYTES = 27 * ROW_BYTES + MAP_BYTES;
 };
 
 template <typename T, int TX, bool ODD, int STAGES>
@@ -108,26 +155,42 @@ constexpr int tile_smem_bytes()
 // copies the window of slot q).
 template <typename S, bool ODD, bool GENERAL, int TX, int STAGES>
 __device__ __forceinline__ void issue_tile(const StepArgs<typename S::T, typename S::R>& a, typename S::T* ring,
-										   uint64_t* full, int s, long long t, int tiles_x, int lane)
+										   uint64_t* full, int s, const TileCursor& c, int lane)
 {
 	using T = typename S::T;
 	using Shape = TileShape<T, TX, ODD>;
 	constexpr int A = Shape::A;
 	constexpr int W = Shape::W;
-	const int xt = (int) (t % tiles_x);
-	const long long row = t / tiles_x;
-	const int y = (int) (row % a.Y);
-	const int z = (int) (row / a.Y);
-	const int xs = xt * TX;
+	const int y = c.y, z = c.z;
+	const int xs = c.xt * TX;
 	const int n = min(TX, a.X - xs);
 	const int n_al = (n + A - 1) / A * A;
 	const uint32_t bytes = (uint32_t) ((ODD ? n_al + 2 * A : n_al) * (int) sizeof(T));
+	// periodic lattice, odd step: the x neighbours of the row's first and last
+	// sites wrap around.  When X is a multiple of A, the 16-byte margins of the
+	// window come from the other end of the row instead of the ghost columns;
+	// the main copy then leaves those margins out, so no two copies of a stage
+	// write the same bytes.
+	const bool wrap_margins = ODD && !GENERAL && (a.X % A) == 0;
+	const bool left = wrap_margins && xs == 0;
+	const bool right = wrap_margins && xs + n == a.X;
+	const int lo = left ? A : 0;
+	const int hi = right ? A + n_al : n_al + 2 * A;
+	// map row of the tile (general kernels): 16-byte aligned source window
+	uint32_t map_bytes = 0;
+	long long map_src = 0;
+	if (GENERAL) {
+		const long long m0 = ((long long) z * a.Y + y) * a.X + xs;
+		map_src = m0 & ~15ll;
+		map_bytes = (uint32_t) ((m0 - map_src + n + 15) & ~15ll);
+	}
 	if (lane == 0)
-		mbar_arrive_expect_tx(&full[s], 27 * bytes);
+		mbar_arrive_expect_tx(&full[s], 27 * bytes + map_bytes);
 	__syncwarp();
+	unsigned char* stage = reinterpret_cast<unsigned char*>(ring) + (long long) s * Shape::STAGE_BYTES;
+	T* win = reinterpret_cast<T*>(stage);
 	if (lane < 27) {
 		const int q = lane;
-		long long src;
 		if (ODD) {
 			// slot q of the sites x + c_q: read there by site x as direction opp(q)
 			int yy = y + cy_rt(q), zz = z + cz_rt(q);
@@ -135,12 +198,21 @@ __device__ __forceinline__ void issue_tile(const StepArgs<typename S::T, typenam
 				yy = yy < 0 ? a.Y - 1 : (yy >= a.Y ? 0 : yy);
 				zz = zz < 0 ? a.Z - 1 : (zz >= a.Z ? 0 : zz);
 			}
-			src = (long long) q * a.sq + (long long) (zz + 1) * a.sz + (long long) (yy + 1) * a.sy + a.x0 + xs - A;
+			const long long row = (long long) q * a.sq + (long long) (zz + 1) * a.sz + (long long) (yy + 1) * a.sy + a.x0;
+			// window element j holds site xs - A + j
+			bulk_g2s(win + q * W + lo, a.f + row + xs - A + lo, (uint32_t) ((hi - lo) * (int) sizeof(T)), &full[s]);
+			if (left)  // window [0, A) <- sites [X - A, X)
+				bulk_g2s(win + q * W, a.f + row + a.X - A, 16u, &full[s]);
+			if (right)	// window [A + n, 2A + n) <- sites [0, A)
+				bulk_g2s(win + q * W + A + n_al, a.f + row, 16u, &full[s]);
 		}
 		else {
-			src = (long long) q * a.sq + (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + xs;
+			const long long src = (long long) q * a.sq + (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + xs;
+			bulk_g2s(win + q * W, a.f + src, bytes, &full[s]);
 		}
-		bulk_g2s(ring + (long long) s * 27 * W + q * W, a.f + src, bytes, &full[s]);
+	}
+	else if (GENERAL && lane == 27) {
+		bulk_g2s(stage + 27 * Shape::ROW_BYTES, a.map + map_src, map_bytes, &full[s]);
 	}
 }
 
@@ -177,28 +249,45 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 	double red[NRED] = {0, 0, 0, 0, 0, 0};
 	bool timed_out = false;
 	long long issued = 0;
+	const TileStride stride = tile_stride(gridDim.x, tiles_x, a.Y);
+	TileCursor cur = tile_at(blockIdx.x, tiles_x, a.Y);	  // tile consumed in iteration i
+	TileCursor pre = cur;									  // next tile warp 0 copies
 
 	// prologue: warp 0 fills the ring
 	if (warp0) {
-		for (long long i = 0; i < STAGES && i < my_tiles; i++)
-			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, (int) i, blockIdx.x + i * gridDim.x, tiles_x, lane);
+		for (long long i = 0; i < STAGES && i < my_tiles; i++) {
+			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, (int) i, pre, lane);
+			tile_advance(pre, stride, tiles_x, a.Y);
+		}
 		issued = my_tiles < STAGES ? my_tiles : STAGES;
 	}
 
+	int s = 0;
+	uint32_t phase = 0;
 	for (long long i = 0; i < my_tiles; i++) {
-		const int s = (int) (i % STAGES);
-		if (!mbar_wait(&full[s], (uint32_t) ((i / STAGES) & 1))) {
+		if (i > 0) {
+			tile_advance(cur, stride, tiles_x, a.Y);
+			if (++s == STAGES) {
+				s = 0;
+				phase ^= 1u;
+			}
+		}
+		if (!mbar_wait(&full[s], phase)) {
 			timed_out = true;
 			break;
 		}
-		const long long t = blockIdx.x + i * gridDim.x;
-		const int xt = (int) (t % tiles_x);
-		const long long row = t / tiles_x;
-		const int y = (int) (row % a.Y);
-		const int z = (int) (row / a.Y);
-		const int x = xt * TX + tid;
+		const int y = cur.y;
+		const int z = cur.z;
+		const int x = cur.xt * TX + tid;
 		const bool active = x < a.X;
-		const T* st = ring + (long long) s * 27 * W;
+		const unsigned char* stage = reinterpret_cast<const unsigned char*>(ring) + (long long) s * Shape::STAGE_BYTES;
+		const T* st = reinterpret_cast<const T*>(stage);
+		uint8_t geo = GEO_PERIODIC;
+		if constexpr (GENERAL) {
+			const long long m0 = ((long long) z * a.Y + y) * a.X + cur.xt * TX;
+			if (active)
+				geo = stage[27 * Shape::ROW_BYTES + (int) (m0 & 15) + tid];
+		}
 
 		Site<R> site;
 		// slot q's window holds direction opp(q) of the tile's sites (odd step)
@@ -222,13 +311,14 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 		if (warp0 && i + STAGES < my_tiles) {
 			bool ok = true;
 			if (lane == 0)
-				ok = mbar_wait(&empty[s], (uint32_t) ((i / STAGES) & 1));
+				ok = mbar_wait(&empty[s], phase);
 			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 			if (!ok) {
 				timed_out = true;
 				break;
 			}
-			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, s, blockIdx.x + (i + STAGES) * gridDim.x, tiles_x, lane);
+			issue_tile<S, ODD, GENERAL, TX, STAGES>(a, ring, full, s, pre, lane);
+			tile_advance(pre, stride, tiles_x, a.Y);
 			issued = i + STAGES + 1;
 		}
 		if (!active)
@@ -236,9 +326,6 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 
 		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		const long long sidx = ((long long) z * a.Y + y) * a.X + x;
-		uint8_t geo = GEO_PERIODIC;
-		if constexpr (GENERAL)
-			geo = a.map[sidx];
 		const bool wrap = !GENERAL || geo == GEO_PERIODIC;
 		const Offsets o = neighbour_offsets(wrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 		if constexpr (ODD) {
@@ -247,7 +334,7 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 			if constexpr (GENERAL)
 				face = wrap && (x == 0 || x == a.X - 1 || y == 0 || y == a.Y - 1 || z == 0 || z == a.Z - 1);
 			else
-				face = x == 0 || x == a.X - 1;
+				face = (a.X % A) != 0 && (x == 0 || x == a.X - 1);
 			if (face)
 				aa_read<S, true>(a.f, a.sq, base, o, site.f);
 		}

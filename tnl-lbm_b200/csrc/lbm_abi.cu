@@ -129,7 +129,7 @@ struct lbm_lattice
 	bool sums_valid = false;
 	long long iteration = 0;
 	int bx = 0, by = 0;	 // 0: default
-	int kernel = lbm::KERNEL_TILE;
+	int kernel = lbm::KERNEL_DIRECT;
 	int sms = 148;
 	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
 	long long last_blocks = 0;	// blocks of the last step launch
@@ -382,7 +382,11 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 		return cleanup(fail(LBM_ERR_CUDA, "population allocation of %zu bytes failed: %s", h->pop_bytes, cudaGetErrorString(e)));
 	if (cudaMemsetAsync(h->g.f, 0, h->pop_bytes, h->stream) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "population memset failed"));
-	if (!d.periodic && cudaMalloc(&h->map, (size_t) h->sites()) != cudaSuccess)
+	// the tile kernel copies map rows from 16-byte aligned windows that can end
+	// up to 15 bytes past the last site: pad the allocation
+	if (!d.periodic
+		&& (cudaMalloc(&h->map, (size_t) h->sites() + 64) != cudaSuccess
+			|| cudaMemsetAsync(h->map, 0, (size_t) h->sites() + 64, h->stream) != cudaSuccess))
 		return cleanup(fail(LBM_ERR_CUDA, "map allocation failed"));
 	if (cudaMalloc(&h->sums_dev, lbm::NRED_HOST * sizeof(double)) != cudaSuccess
 		|| cudaMallocHost(&h->sums_host, lbm::NRED_HOST * sizeof(double)) != cudaSuccess)
@@ -729,8 +733,8 @@ int lbm_set_block(lbm_handle h, int bx, int by)
 		h->bx = h->by = 0;
 	}
 	else {
-		if (bx < 32 || bx % 32 != 0 || by < 1 || bx * by > 256)
-			return fail(LBM_ERR_INVALID, "block (%d, %d): bx must be a multiple of 32 and bx*by <= 256", bx, by);
+		if (bx < 32 || bx % 32 != 0 || by < 1 || bx * by > 128)
+			return fail(LBM_ERR_INVALID, "block (%d, %d): bx must be a multiple of 32 and bx*by <= 128", bx, by);
 		h->bx = bx;
 		h->by = by;
 	}
@@ -763,7 +767,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	LBM_CUDA(cudaMalloc(&backup, h->pop_bytes));
 	LBM_CUDA(cudaMemcpyAsync(backup, h->g.f, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream));
 	const long long it0 = h->iteration;
-	static const int cands[][2] = {{32, 4}, {64, 2}, {128, 1}, {32, 8}, {64, 4}, {128, 2}, {256, 1}, {32, 2}, {64, 1}};
+	static const int cands[][2] = {{128, 1}, {64, 2}, {32, 4}, {64, 1}, {32, 2}};
 	cudaEvent_t e0, e1;
 	cudaEventCreate(&e0);
 	cudaEventCreate(&e1);
