@@ -66,7 +66,26 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+    build_examples(force)
     return LIB
+
+
+def build_examples(force: bool = False) -> list:
+    """C++ host programs over the C-ABI (tnl-lbm_b200/host/examples), built
+    with g++ against lib/libtnl_lbm_b200.so."""
+    out = []
+    host = os.path.join(PKG, "host")
+    for src in sorted(glob.glob(os.path.join(host, "examples", "*.cpp"))):
+        exe = os.path.join(LIBDIR, os.path.basename(src)[:-4])
+        deps = [src, os.path.join(host, "lbm_b200.hpp"), os.path.join(ROOT, "include", "tnl_lbm_b200.h"), LIB]
+        if force or not os.path.exists(exe) or os.path.getmtime(exe) < _newest(deps):
+            cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), "-I" + host, src,
+                   "-L" + LIBDIR, "-ltnl_lbm_b200", "-Wl,-rpath,$ORIGIN", "-o", exe]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError("host example build failed:\n" + r.stdout + r.stderr)
+        out.append(exe)
+    return out
 
 
 if __name__ == "__main__":
