@@ -195,6 +195,28 @@ typedef struct lbm_device_view {
 } lbm_device_view;
 LBM_API int lbm_device_view_get(lbm_handle h, lbm_device_view* out);
 
+/* Allocation-free FP64 sums of a macro field, for callers that cannot
+ * allocate device memory where they need the result: code being captured
+ * into a CUDA graph, an application whose own pool allocator owns the device
+ * memory, a real-time loop that must not take an allocation's implicit
+ * synchronisation.  No counterpart in the reference.
+ *   macro   device pointer to a field [4][nsites] (rho, vx, vy, vz) of
+ *           LBM_DTYPE_F64 or LBM_DTYPE_F32 values, e.g. a lattice's macro
+ *           field from lbm_device_view_get
+ *   out     device pointer to 6 doubles: the sums of lbm_get_sums
+ *   stream  cudaStream_t (NULL: the default stream); the call is asynchronous
+ * The partial sums live in a file-scope device array of
+ * LBM_NOALLOC_SCRATCH_DOUBLES doubles (96 KiB per GPU that loads the library,
+ * kept until the process exits).  The call allocates nothing.  Its first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  nsites above
+ * LBM_NOALLOC_MAX_SITES returns LBM_ERR_SIZE. */
+#define LBM_NOALLOC_MAX_BLOCKS 2048
+#define LBM_NOALLOC_SCRATCH_DOUBLES (6 * LBM_NOALLOC_MAX_BLOCKS)
+#define LBM_NOALLOC_MAX_SITES ((int64_t) 1 << 40)
+LBM_API int lbm_macro_sums_noalloc(const void* macro, int dtype, int64_t nsites, double* out, void* stream);
+
 /* Library build information: sm architecture and version string. */
 LBM_API const char* lbm_version(void);
 

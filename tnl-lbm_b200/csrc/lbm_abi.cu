@@ -109,6 +109,14 @@ bool site_type_supported(uint8_t g)
 
 }  // namespace
 
+namespace lbm {
+// lets other translation units of the library set the message of lbm_last_error()
+int record_error(int code, const char* msg)
+{
+	return fail(code, "%s", msg);
+}
+}  // namespace lbm
+
 struct lbm_lattice
 {
 	lbm_desc d{};
