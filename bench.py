@@ -285,6 +285,15 @@ def run_ours(args):
     else:
         lat.close()
 
+    # the error each storage format costs: Taylor-Green 128^3, Re 1600, 5000
+    # steps (about 12 convective times, the span of the 512^3 20000-step case),
+    # kinetic energy and dissipation rate against the FP64-storage run
+    precision = None
+    if args.precision and rank == 0:
+        from pytnl_lbm import precision as prec
+        precision = prec.study(128, 5000, 100, ("f32", "f16s", "bf16s"), local)
+        precision.pop("series_f64")
+
     line = None
     if rank == 0:
         line = {
@@ -315,6 +324,8 @@ def run_ours(args):
         }
         if variants:
             line["storage_variants"] = variants
+        if precision is not None:
+            line["precision"] = precision
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(spec, args)
     if dist is not None:
@@ -431,6 +442,7 @@ def main():
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-precision", dest="precision", action="store_false")
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--kernel", default="direct", choices=["direct", "tile"])
     args = ap.parse_args()
