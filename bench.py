@@ -46,10 +46,173 @@ def workload_spec(name):
     if name == "tgv512":
         return dict(workload="periodic Taylor-Green vortex 512^3, U0=0.05, Re=1600", X=512, Y=512, Z=512, kind="tgv",
                     cum_flags=3)
+    if name == "ensemble64":
+        return dict(workload="ensemble of 64 periodic Taylor-Green lattices, edges U{32,48,64,96,128} (seeded, "
+                             "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
+                    X=0, Y=0, Z=0, kind="ensemble", cum_flags=3)
     if name == "tgv64":
         return dict(workload="periodic Taylor-Green vortex 64^3, U0=0.05, Re=1600", X=64, Y=64, Z=64, kind="tgv",
                     cum_flags=3)
     raise SystemExit(f"unknown workload {name}")
+
+
+def ensemble_setup(count=64, seed=4321, u0=0.05):
+    """Member sizes and viscosities of the ensemble workload: each edge drawn
+    from {32, 48, 64, 96, 128}, Re log-uniform in [100, 3200] on the x box
+    length, nu = u0 (X / 2 pi) / Re."""
+    rng = np.random.default_rng(seed)
+    edges = np.array([32, 48, 64, 96, 128])
+    sizes = [tuple(int(v) for v in rng.choice(edges, 3)) for _ in range(count)]
+    re = np.exp(rng.uniform(math.log(100.0), math.log(3200.0), count))
+    nus = [u0 * (sz[0] / (2 * math.pi)) / r for sz, r in zip(sizes, re)]
+    return sizes, nus
+
+
+def run_ensemble(args):
+    """One persistent launch per step over all members, against the same
+    members run one after the other as single lattices."""
+    import torch
+    import pytnl_lbm as pl
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, local, "nccl")
+    device = torch.device("cuda", local)
+    spec = workload_spec(args.workload)
+    sizes, nus = ensemble_setup()
+    sites = sum(x * y * z for x, y, z in sizes)
+    st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
+          "bf16s": pl.STORE_BF16S}[args.storage]
+    ens = pl.Ensemble(sizes, nus, cum_flags=3, storage=st, device=local)
+    ens.init_taylor_green(0.05)
+    shape = ens.autotune(3)
+    ens.init_taylor_green(0.05)
+    stream = torch.cuda.ExternalStream(ens.stream, device=device)
+    warm = max(args.warmup, 16) + (max(args.warmup, 16) % 2)
+    ens.step(warm)
+    ens.synchronize()
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    secs_max = max_over_ranks(dist, secs, device)
+    value = sites * args.steps * world / secs_max / 1e6
+    ens.step(2, sums=True)
+    ke_ens = ens.kinetic_energy()
+    # e2e through the public API: one step with the per-member sums and the
+    # sums read back to the host, every step
+    e2e_steps = max(10, min(args.steps // 4, 200))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ens.step(1, sums=True)
+        ens.sums()
+    e2e_secs = max_over_ranks(dist, time.perf_counter() - t0, device)
+    ens.close()
+
+    # the same members as single lattices, one after the other (device time of
+    # each run on its own stream, summed)
+    seq_secs = 0.0
+    ke_seq = []
+    for (X, Y, Z), nu in zip(sizes, nus):
+        lat = pl.LBM(X, Y, Z, viscosity=nu, cum_flags=3, storage=st, periodic=True, device=local)
+        lat.init_taylor_green(0.05)
+        lat.step(warm)
+        lat.synchronize()
+        ls = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(ls)
+        lat.step(args.steps)
+        a1.record(ls)
+        a1.synchronize()
+        seq_secs += a0.elapsed_time(a1) / 1e3
+        lat.step(2, sums=True)
+        ke_seq.append(pl.kinetic_energy(lat))
+        lat.close()
+    seq_value = sites * args.steps / seq_secs / 1e6
+    same = bool(np.array_equal(np.asarray(ke_seq), ke_ens))
+
+    bpe = BYTES_PER_ELEM[args.storage]
+    achieved = 2 * 27 * bpe * sites / (secs / args.steps) / 1e9
+    peak, peak_kind = read_peaks()
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(secs_max / args.steps * 1e3, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f64": "f64", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32"}.get(args.storage, "f32"),
+            "data": "synthetic (seeded member sizes, viscosities and Taylor-Green initial states)",
+            "config": {"workload": spec["workload"], "members": len(sizes), "sites": sites,
+                       "storage": args.storage, "parallelism": f"replicas x{world}",
+                       "launch": {"tile_sites": shape[0],
+                                  "grid": "persistent" if shape[1] == 0 else "one block per tile", "autotuned": True},
+                       "l2": "populations (%.2f GB) larger than L2; no flush" % (27 * bpe * sites / 1e9)},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s",
+                         "algorithmic_bytes_per_site_update": 2 * 27 * bpe},
+            "e2e": {"value": round(sites * e2e_steps * world / e2e_secs / 1e6, 2), "unit": "MLUPS",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 6 * 8 * len(sizes), "steps": e2e_steps,
+                    "per_step": "lbm_ensemble_step(1, LBM_STEP_SUMS) + lbm_ensemble_get_sums"},
+            "sequential": {"value": round(seq_value, 2), "unit": "MLUPS", "speedup": round(value / seq_value, 3),
+                           "kinetic_energy_identical": same,
+                           "how": "the same 64 members as single periodic lattices (lbm_create), one after the "
+                                  "other, each replayed from its CUDA graphs; summed device time"},
+            "clocks": clk.summary(),
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+
+
+def run_reference_ensemble(args, spec, oracle, cores):
+    """The reference's per-site code on each ensemble member in turn (the
+    reference runs one lattice per solver instance), on all host cores."""
+    sizes, nus = ensemble_setup()
+    prec = np.float64 if args.storage == "f64" else np.float32
+    impl = oracle.Reference(3, fast=True)
+    total_sites = sum(x * y * z for x, y, z in sizes)
+    # calibrate on the first member, then size the per-member step count so
+    # that the whole sample takes about 20 s
+    X, Y, Z = sizes[0]
+    f = impl.allocate(X, Y, Z, prec)
+    impl.init_equilibrium(f, X, Y, Z, eq="INV_CUM", fields=None)
+    _, el = impl.aa_run(f, np.full((Z, Y, X), 9, np.int16), coll="CUM", nu=nus[0], nsteps=2, nthreads=cores,
+                        return_time=True)
+    rate = X * Y * Z * 2 / max(el, 1e-6)
+    steps = int(max(2, min(args.steps, 20.0 * rate / total_sites)))
+    steps += steps % 2
+    elapsed = 0.0
+    for (X, Y, Z), nu in zip(sizes, nus):
+        f = impl.allocate(X, Y, Z, prec)
+        impl.init_equilibrium(f, X, Y, Z, eq="INV_CUM", fields=None)
+        _, el = impl.aa_run(f, np.full((Z, Y, X), 9, np.int16), coll="CUM", nu=nu, nsteps=steps, nthreads=cores,
+                            return_time=True)
+        elapsed += el
+    value = total_sites * steps / elapsed / 1e6
+    sample = (f"{steps} A-A steps of each of the {len(sizes)} members ({prec.__name__}), one after the other, "
+              f"OpenMP on {cores} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "MLUPS", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(elapsed / steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == np.float64 else "f32",
+        "data": "synthetic (seeded member sizes and viscosities)",
+        "config": {"workload": spec["workload"], "members": len(sizes), "sites": total_sites, "storage": args.storage,
+                   "implementation": "TNL-LBM per-site headers (oracle/_ref) + reference OpenMP loop"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
 
 
 def duct_setup(X, Y, Z, seed=1234):
@@ -177,6 +340,8 @@ def max_over_ranks(dist, value, device):
 def make_lattice(pl, spec, storage, device, kernel="direct"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S}[storage]
+    if spec["kind"] == "ensemble":
+        return run_reference_ensemble(args, spec, oracle, cores)
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
@@ -211,6 +376,8 @@ def time_steps(pl, lat, steps, warmup, stream):
 
 
 def run_ours(args):
+    if workload_spec(args.workload)["kind"] == "ensemble":
+        return run_ensemble(args)
     import torch
     import pytnl_lbm as pl
     rank, world, local = dist_env()
@@ -438,7 +605,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64"])
+    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64"])
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

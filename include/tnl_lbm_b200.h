@@ -217,6 +217,54 @@ LBM_API int lbm_device_view_get(lbm_handle h, lbm_device_view* out);
 #define LBM_NOALLOC_MAX_SITES ((int64_t) 1 << 40)
 LBM_API int lbm_macro_sums_noalloc(const void* macro, int dtype, int64_t nsites, double* out, void* stream);
 
+/* ---- Ensembles of periodic lattices ------------------------------------
+ * Many independent periodic lattices of different sizes and viscosities,
+ * advanced by one persistent launch per A-A step (captured in CUDA graphs).
+ * The reference has no ensemble driver: a TNL-LBM user runs one solver
+ * instance (State / LBM_BLOCK, include/lbm3d/state.h, lbm_block.h) per
+ * lattice, one after the other.  Each member's update equals, bit for bit,
+ * that of a single periodic lattice (lbm_create with periodic = 1) with the
+ * same size, viscosity and initial state.  Members share the storage format,
+ * collision slot and equilibrium. */
+typedef struct lbm_ensemble_desc {
+	int32_t count;            /* members, 1 .. LBM_ENSEMBLE_MAX_MEMBERS */
+	const int32_t* X;         /* [count] sites per axis of each member (X*Y*Z < 2^31) */
+	const int32_t* Y;
+	const int32_t* Z;
+	const double* viscosity;  /* [count] lattice viscosity of each member */
+	int32_t storage, collision, cum_flags, equilibrium; /* as lbm_desc */
+	int32_t device;
+	int32_t use_graphs;
+} lbm_ensemble_desc;
+#define LBM_ENSEMBLE_MAX_MEMBERS 65536
+typedef struct lbm_ensemble_t* lbm_ensemble;
+
+LBM_API int lbm_ensemble_create(const lbm_ensemble_desc* desc, lbm_ensemble* out);
+LBM_API int lbm_ensemble_destroy(lbm_ensemble e);
+/* Taylor-Green vortex in every member (each in its own box, as
+ * lbm_init_taylor_green), or a uniform equilibrium; iteration reset to 0. */
+LBM_API int lbm_ensemble_init_taylor_green(lbm_ensemble e, double u0, double rho0);
+LBM_API int lbm_ensemble_init_equilibrium(lbm_ensemble e, double rho0, double vx0, double vy0, double vz0);
+/* populations of one member, layouts and dtypes as lbm_set_populations */
+LBM_API int lbm_ensemble_set_populations(lbm_ensemble e, int member, const void* host, int layout, int dtype);
+LBM_API int lbm_ensemble_get_populations(lbm_ensemble e, int member, void* host, int layout, int dtype);
+/* nsteps A-A steps of every member; LBM_STEP_SUMS computes per-member sums
+ * in the last step (lbm_ensemble_get_sums). */
+LBM_API int lbm_ensemble_step(lbm_ensemble e, int64_t nsteps, int flags);
+/* out[count][6]: the sums of lbm_get_sums for each member */
+LBM_API int lbm_ensemble_get_sums(lbm_ensemble e, double* out);
+LBM_API int64_t lbm_ensemble_iteration(lbm_ensemble e);
+/* the ensemble's CUDA stream (cudaStream_t), for events and interop */
+LBM_API int lbm_ensemble_get_stream(lbm_ensemble e, void** stream);
+LBM_API int lbm_ensemble_synchronize(lbm_ensemble e);
+/* Launch shape: sites per tile (= threads per block) 128 or 256, and grid
+ * 0 (persistent: resident blocks per SM x SMs) or 1 (one block per tile). */
+LBM_API int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy);
+LBM_API int lbm_ensemble_get_shape(lbm_ensemble e, int* tile_sites, int* grid_policy);
+/* Times every launch shape on the current state (restored afterwards) and
+ * keeps the fastest. */
+LBM_API int lbm_ensemble_autotune(lbm_ensemble e, int ntrials);
+
 /* Library build information: sm architecture and version string. */
 LBM_API const char* lbm_version(void);
 

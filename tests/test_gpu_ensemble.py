@@ -1,0 +1,140 @@
+"""Ensembles of periodic lattices (lbm_ensemble_* of the C-ABI) on the GPU.
+
+An ensemble member must evolve exactly as a single periodic lattice of the
+same size, viscosity and initial state does (lbm_create with periodic = 1),
+which the single-lattice parity tests tie to the oracle: populations are
+compared bit for bit, sums to FP64 rounding (the per-tile partial sums of the
+ensemble add the same values in another order).  One member is also checked
+against the oracle directly.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_linf, seeded_state
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(32, 48, 16), (48, 32, 20), (37, 9, 7), (5, 4, 3), (64, 16, 8), (96, 24, 12)]
+NUS = [0.002, 0.01, 0.03, 0.005, 0.0007, 0.02]
+
+
+@pytest.fixture(scope="module")
+def pl():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import pytnl_lbm
+    return pytnl_lbm
+
+
+def single_run(pl, size, nu, storage, coll, flags, eq, steps, f0=None):
+    X, Y, Z = size
+    lat = pl.LBM(X, Y, Z, viscosity=nu, collision=coll, cum_flags=flags, equilibrium=eq, storage=storage,
+                 periodic=True)
+    if f0 is None:
+        lat.init_taylor_green(0.05)
+    else:
+        lat.set_populations(f0)
+    lat.step(steps, sums=True)
+    out = lat.get_populations(), lat.sums()
+    lat.close()
+    return out
+
+
+@pytest.mark.parametrize("storage", ["F32", "F64", "F16S"])
+@pytest.mark.parametrize("coll,flags,eq", [("CUM", 0, "INV_CUM"), ("CUM", 3, "INV_CUM"), ("SRT", 0, "EQ"),
+                                           ("MRT", 0, "EQ")])
+@pytest.mark.parametrize("steps", [7, 36])
+def test_members_equal_single_lattices(pl, storage, coll, flags, eq, steps):
+    st = getattr(pl, "STORE_" + storage)
+    cid = getattr(pl, "COLL_" + coll)
+    eid = pl.EQ_INV_CUM if eq == "INV_CUM" else pl.EQ_SECOND_ORDER
+    ens = pl.Ensemble(SIZES, NUS, collision=cid, cum_flags=flags, equilibrium=eid, storage=st)
+    ens.init_taylor_green(0.05)
+    ens.step(steps, sums=True)
+    assert ens.iteration == steps
+    sums = ens.sums()
+    for m, (size, nu) in enumerate(zip(SIZES, NUS)):
+        f_single, s_single = single_run(pl, size, nu, st, cid, flags, eid, steps)
+        assert np.array_equal(ens.get_populations(m), f_single), f"member {m}"
+        np.testing.assert_allclose(sums[m, :5], s_single[:5], rtol=1e-12, atol=1e-12 * abs(s_single[0]))
+        assert sums[m, 5] == 0
+    ens.close()
+
+
+@pytest.mark.parametrize("tile_sites,grid_policy", [(128, 0), (128, 1), (256, 0), (256, 1)])
+def test_launch_shapes_give_identical_results(pl, port, tile_sites, grid_policy):
+    rng = np.random.default_rng(5)
+    ens = pl.Ensemble(SIZES, NUS, cum_flags=3, storage=pl.STORE_F32)
+    states = [seeded_state(port, rng, *s) for s in SIZES]
+    for m, f0 in enumerate(states):
+        ens.set_populations(m, f0.astype(np.float32))
+    ens.set_shape(tile_sites, grid_policy)
+    assert ens.shape() == (tile_sites, grid_policy)
+    ens.step(21)
+    for m, (size, nu) in enumerate(zip(SIZES, NUS)):
+        f_single, _ = single_run(pl, size, nu, pl.STORE_F32, pl.COLL_CUM, 3, pl.EQ_INV_CUM, 21,
+                                 f0=states[m].astype(np.float32))
+        assert np.array_equal(ens.get_populations(m), f_single), f"member {m}"
+    ens.close()
+
+
+def test_member_against_oracle(pl, port):
+    """FP64 member vs the oracle port on a seeded state (the single-lattice tolerance)."""
+    rng = np.random.default_rng(11)
+    ens = pl.Ensemble(SIZES, NUS, cum_flags=3, storage=pl.STORE_F64)
+    ens.init_taylor_green(0.05)
+    m = 2
+    X, Y, Z = SIZES[m]
+    f0 = seeded_state(port, rng, X, Y, Z)
+    ens.set_populations(m, f0)
+    ens.step(9)
+    fo = np.ascontiguousarray(f0.copy())
+    geo = np.full((Z, Y, X), 9, np.int16)
+    port.aa_run(fo, geo, coll="CUM", eq="INV_CUM", cum_flags=3, nu=NUS[m], nsteps=9)
+    assert rel_linf(ens.get_populations(m), fo) <= 1e-12
+    ens.close()
+
+
+def test_taylor_green_init_matches_single_lattice(pl):
+    ens = pl.Ensemble(SIZES[:3], NUS[:3], cum_flags=3, storage=pl.STORE_F64)
+    ens.init_taylor_green(0.04, 1.0)
+    for m, size in enumerate(SIZES[:3]):
+        lat = pl.LBM(*size, viscosity=NUS[m], cum_flags=3, storage=pl.STORE_F64, periodic=True)
+        lat.init_taylor_green(0.04, 1.0)
+        assert np.array_equal(ens.get_populations(m), lat.get_populations())
+        lat.close()
+    ens.close()
+
+
+def test_autotune_restores_state_and_picks_a_shape(pl):
+    ens = pl.Ensemble(SIZES, NUS, cum_flags=3, storage=pl.STORE_F32)
+    ens.init_taylor_green(0.05)
+    ens.step(3)
+    before = [ens.get_populations(m) for m in range(len(SIZES))]
+    shape = ens.autotune(2)
+    assert shape[0] in (128, 256) and shape[1] in (0, 1)
+    assert ens.iteration == 3
+    for m in range(len(SIZES)):
+        assert np.array_equal(ens.get_populations(m), before[m])
+    ens.close()
+
+
+def test_invalid_ensembles_are_rejected(pl):
+    with pytest.raises(pl.LbmError) as e:
+        pl.Ensemble([(8, 8, 8), (0, 4, 4)], [0.01, 0.01])
+    assert e.value.code == 1
+    with pytest.raises(pl.LbmError) as e:
+        pl.Ensemble([(8, 8, 8)], [-0.01])
+    assert e.value.code == 1
+    with pytest.raises(pl.LbmError) as e:
+        pl.Ensemble([(2048, 1024, 1024)], [0.01])
+    assert e.value.code == 5
+    ens = pl.Ensemble([(8, 8, 8)], [0.01])
+    with pytest.raises(pl.LbmError):
+        ens.sums()  # no summed step yet
+    with pytest.raises(pl.LbmError):
+        ens.set_shape(64, 0)
+    with pytest.raises(pl.LbmError):
+        ens.get_populations(3)
+    ens.close()

@@ -3,8 +3,11 @@
 // tile kernel) and names the storage type in LBM_DEFINE_STORAGE_OPS.
 #pragma once
 
+#include <cstring>
+
 #include "aa_kernels.cuh"
 #include "aa_tile.cuh"
+#include "ensemble.cuh"
 #include "launch.h"
 
 namespace lbm {
@@ -182,6 +185,106 @@ struct StorageUnit
 		}
 	}
 
+	// ---- ensemble of periodic lattices
+	static void ens_entry(void* dst, const Geometry& g, const CollParamsD& pd, long long tile0)
+	{
+		EnsMember<T, R> e{};
+		e.f = (T*) g.f;
+		e.sq = g.sq;
+		e.sy = g.sy;
+		e.sz = g.sz;
+		e.x0 = g.x0;
+		e.X = g.X;
+		e.Y = g.Y;
+		e.Z = g.Z;
+		e.n = g.X * g.Y * g.Z;
+		e.tile0 = tile0;
+		e.dx = make_fast_div(g.X);
+		e.dy = make_fast_div(g.Y);
+		e.p = make_coll_params<R>(pd);
+		memcpy(dst, &e, sizeof(e));
+	}
+
+	template <int COLL, int CUMF, bool ODD, bool OUT, int TPB>
+	static cudaError_t ens_launch(const EnsLaunch& L)
+	{
+		// the member's collision constants live in registers here (kernel
+		// parameters in the single-lattice kernel): 128 registers per thread
+		constexpr int minb = sizeof(R) == 8 ? (TPB == 128 ? 2 : 1) : (TPB == 128 ? 4 : 2);
+		auto kern = ens_step_kernel<S, COLL, CUMF, ODD, OUT, TPB, minb>;
+		static int per_sm_cache[64] = {0};
+		static int sms_cache[64] = {0};
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (dev < 0 || dev >= 64)
+			return cudaErrorInvalidDevice;
+		if (per_sm_cache[dev] == 0) {
+			int per_sm = 0, sms = 0;
+			cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TPB, 0);
+			if (e != cudaSuccess)
+				return e;
+			e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+			if (e != cudaSuccess)
+				return e;
+			if (per_sm < 1)
+				return cudaErrorInvalidConfiguration;
+			per_sm_cache[dev] = per_sm;
+			sms_cache[dev] = sms;
+		}
+		long long grid = L.grid > 0 ? L.grid : (long long) per_sm_cache[dev] * sms_cache[dev];
+		if (grid > L.ntiles)
+			grid = L.ntiles;
+		if (grid > 0x7fffffffLL)
+			grid = 0x7fffffffLL;
+		if (L.blocks_out)
+			*L.blocks_out = grid;
+		if (L.dry_run || grid < 1)
+			return cudaSuccess;
+		kern<<<(unsigned) grid, TPB, 0, L.stream>>>((const EnsMember<T, R>*) L.members, L.tile_member, L.ntiles, L.partials);
+		return cudaGetLastError();
+	}
+
+	template <int COLL, int CUMF>
+	static cudaError_t ens_dispatch(const EnsLaunch& L)
+	{
+		const bool out = L.partials != nullptr;
+		if (L.tpb == 256) {
+			if (L.odd)
+				return out ? ens_launch<COLL, CUMF, true, true, 256>(L) : ens_launch<COLL, CUMF, true, false, 256>(L);
+			return out ? ens_launch<COLL, CUMF, false, true, 256>(L) : ens_launch<COLL, CUMF, false, false, 256>(L);
+		}
+		if (L.tpb != 128)
+			return cudaErrorInvalidValue;
+		if (L.odd)
+			return out ? ens_launch<COLL, CUMF, true, true, 128>(L) : ens_launch<COLL, CUMF, true, false, 128>(L);
+		return out ? ens_launch<COLL, CUMF, false, true, 128>(L) : ens_launch<COLL, CUMF, false, false, 128>(L);
+	}
+
+	static cudaError_t ens_step(const EnsLaunch& L)
+	{
+		switch (L.coll) {
+			case COLL_CUM:
+				switch (L.cum_flags) {
+					case 0:
+						return ens_dispatch<COLL_CUM, 0>(L);
+					case CUM_ANTIALIAS:
+						return ens_dispatch<COLL_CUM, CUM_ANTIALIAS>(L);
+					case CUM_2017 | CUM_ANTIALIAS:
+						return ens_dispatch<COLL_CUM, CUM_2017 | CUM_ANTIALIAS>(L);
+					default:
+						return cudaErrorInvalidValue;
+				}
+			case COLL_SRT:
+				return ens_dispatch<COLL_SRT, 0>(L);
+			case COLL_BGK:
+				return ens_dispatch<COLL_BGK, 0>(L);
+			case COLL_MRT:
+				return ens_dispatch<COLL_MRT, 0>(L);
+			default:
+				return cudaErrorInvalidValue;
+		}
+	}
+
 	static cudaError_t init_eq(const Geometry& g, const InitSpec& spec, cudaStream_t st);
 	static cudaError_t pack(const Geometry& g, void* dense, int dtype, int ghost, cudaStream_t st);
 	static cudaError_t unpack(const Geometry& g, const void* dense, int dtype, int ghost, cudaStream_t st);
@@ -310,6 +413,9 @@ cudaError_t StorageUnit<S>::unpack(const Geometry& g, const void* dense, int dty
 									   &StorageUnit<S>::init_eq,                                                     \
 									   &StorageUnit<S>::pack,                                                        \
 									   &StorageUnit<S>::unpack,                                                      \
+									   sizeof(EnsMember<typename S::T, typename S::R>),                              \
+									   &StorageUnit<S>::ens_entry,                                                   \
+									   &StorageUnit<S>::ens_step,                                                    \
 									   (int) sizeof(typename S::R),                                                  \
 									   (int) sizeof(typename S::T),                                                  \
 									   NAME};                                                                        \

@@ -76,6 +76,22 @@ enum : int
 // upper bound of the tile kernel's grid (blocks per SM x SMs)
 constexpr int TILE_MAX_BLOCKS_PER_SM = 8;
 
+// one A-A step of an ensemble of periodic lattices (ensemble.cuh)
+struct EnsLaunch
+{
+	const void* members;	 // device table of the storage's EnsMember entries
+	const int* tile_member;	 // member of each tile
+	long long ntiles;
+	int tpb;		   // sites per tile = threads per block: 128 or 256
+	long long grid;	   // blocks; 0 = resident blocks per SM x SMs (persistent)
+	double* partials;  // [NRED][ntiles] or null
+	int coll, cum_flags;
+	bool odd;
+	cudaStream_t stream;
+	bool dry_run;
+	long long* blocks_out;
+};
+
 struct StorageOps
 {
 	// one A-A step
@@ -86,6 +102,11 @@ struct StorageOps
 	// (dtype 0) or float (dtype 1); ghost = 1 includes the ghost layer
 	cudaError_t (*pack)(const Geometry&, void* dense, int dtype, int ghost, cudaStream_t);
 	cudaError_t (*unpack)(const Geometry&, const void* dense, int dtype, int ghost, cudaStream_t);
+	// ensemble: bytes of one member-table entry, host-side fill of an entry,
+	// and the step
+	size_t ens_entry_bytes;
+	void (*ens_entry)(void* dst, const Geometry&, const CollParamsD&, long long tile0);
+	cudaError_t (*ens_step)(const EnsLaunch&);
 	int compute_size;  // sizeof the compute type (8 or 4)
 	int elem_size;	   // sizeof the storage element
 	const char* name;

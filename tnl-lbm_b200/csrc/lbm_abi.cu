@@ -17,6 +17,7 @@
 
 #include "../../include/tnl_lbm_b200.h"
 #include "d3q27.cuh"
+#include "host_common.h"
 #include "launch.h"
 
 namespace lbm {
@@ -65,24 +66,6 @@ int fail(int code, const char* fmt, ...)
 			return fail(LBM_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, \
 						__LINE__);                                                                       \
 	} while (0)
-
-// Geier 2017 relaxation rates for omega2 = 1 (col_cum.h:195-228), evaluated
-// once per viscosity in double precision
-void cumulant_rates(double nu, lbm::CollParamsD& p)
-{
-	const double w1 = 1.0 / (3.0 * nu + 0.5);
-	const double w2 = 1.0;
-	p.w1 = w1;
-	p.w3 = 8 * (w1 - 2) * (w2 * (3 * w1 - 1) - 5 * w1) / (8 * (5 - 2 * w1) * w1 + w2 * (8 + w1 * (9 * w1 - 26)));
-	p.w4 = 8 * (w1 - 2) * (w1 + w2 * (3 * w1 - 7)) / (w2 * (56 - 42 * w1 + 9 * w1 * w1) - 8 * w1);
-	p.w5 = 24 * (w1 - 2) * (4 * w1 * w1 + w1 * w2 * (18 - 13 * w1) + w2 * w2 * (2 + w1 * (6 * w1 - 11)))
-		 / (16 * w1 * w1 * (w1 - 6) - 2 * w1 * w2 * (216 + 5 * w1 * (9 * w1 - 46))
-			+ w2 * w2 * (w1 * (3 * w1 - 10) * (15 * w1 - 28) - 48));
-	p.A = (4 * w1 * w1 + 2 * w1 * w2 * (w1 - 6) + w2 * w2 * (w1 * (10 - 3 * w1) - 4)) / (w1 - w2) / (w2 * (2 + 3 * w1) - 8 * w1);
-	p.B = (4 * w1 * w2 * (9 * w1 - 16) - 4 * w1 * w1 - 2 * w2 * w2 * (2 + 9 * w1 * (w1 - 2))) / 3.0 / (w1 - w2)
-		/ (w2 * (2 + 3 * w1) - 8 * w1);
-	p.tau = 3.0 * nu + 0.5;
-}
 
 bool site_type_supported(uint8_t g)
 {
@@ -359,20 +342,9 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 	h->d = d;
 	h->ops = &lbm::storage_ops(d.storage);
 	const int es = h->ops->elem_size;
-	const int align = 128 / es;	 // elements per 128 bytes
-	h->g.x0 = align;
-	// row: x0 elements of front pad (ghost x = -1 at x0 - 1), X interior sites,
-	// and room for the tile kernel's odd-step window, which reaches up to
-	// 2 x (16 bytes) beyond the last site
-	const int a16 = 16 / es;
-	h->g.sy = ((align + d.X + 2 * a16 + align - 1) / align) * align;
-	h->g.sz = h->g.sy * (d.Y + 2);
-	h->g.sq = (long long) h->g.sz * (d.Z + 2);
-	h->g.X = d.X;
-	h->g.Y = d.Y;
-	h->g.Z = d.Z;
+	h->g = lbm::make_geometry(d.X, d.Y, d.Z, es);
 	h->pop_bytes = (size_t) 27 * h->g.sq * es;
-	cumulant_rates(d.viscosity, h->p);
+	lbm::cumulant_rates(d.viscosity, h->p);
 	h->p.nu = d.viscosity;
 	h->p.fx = d.fx;
 	h->p.fy = d.fy;
@@ -499,7 +471,7 @@ int lbm_set_viscosity(lbm_handle h, double nu)
 	if (!(nu > 0.0) || !std::isfinite(nu))
 		return fail(LBM_ERR_INVALID, "viscosity must be positive and finite");
 	h->d.viscosity = nu;
-	cumulant_rates(nu, h->p);
+	lbm::cumulant_rates(nu, h->p);
 	h->p.nu = nu;
 	h->drop_graph();
 	return LBM_OK;

@@ -22,7 +22,7 @@ from ._abi import (  # noqa: F401  (re-exported constants)
     GEO, KERNEL_DIRECT, KERNEL_TILE, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
     STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
 
-__all__ = ["LBM", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
+__all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
 
 # D3Q27_MACRO_Default quantity order (include/lbm3d/d3q27/macro.h:61-68)
 macro_names = ("rho", "vx", "vy", "vz")
@@ -205,6 +205,119 @@ def _wrap_device(ptr, n, dtype, device):
 
     t = torch.as_tensor(_CudaArray(), device=f"cuda:{device}")
     return t.view(dtype) if dtype == torch.bfloat16 else t
+
+
+class Ensemble:
+    """Many independent periodic lattices of different sizes and viscosities,
+    advanced together by one launch per A-A step (lbm_ensemble_* of the C-ABI).
+
+    ``sizes`` is a sequence of (X, Y, Z); ``viscosities`` one value per member.
+    Each member evolves exactly as a periodic ``LBM`` of the same size and
+    viscosity would.
+    """
+
+    def __init__(self, sizes, viscosities, *, collision=COLL_CUM, cum_flags=0, equilibrium=EQ_INV_CUM,
+                 storage=STORE_F32, device=0, use_graphs=True):
+        self.lib = library()
+        sizes = [tuple(int(v) for v in s) for s in sizes]
+        if len(sizes) != len(viscosities):
+            raise ValueError("one viscosity per member")
+        n = len(sizes)
+        self._X = (ctypes.c_int32 * n)(*[s[0] for s in sizes])
+        self._Y = (ctypes.c_int32 * n)(*[s[1] for s in sizes])
+        self._Z = (ctypes.c_int32 * n)(*[s[2] for s in sizes])
+        self._nu = (ctypes.c_double * n)(*[float(v) for v in viscosities])
+        d = _abi.lbm_ensemble_desc()
+        d.count = n
+        d.X, d.Y, d.Z, d.viscosity = self._X, self._Y, self._Z, self._nu
+        d.storage, d.collision, d.cum_flags, d.equilibrium = storage, collision, cum_flags, equilibrium
+        d.device = int(device)
+        d.use_graphs = 1 if use_graphs else 0
+        self.sizes = sizes
+        self.storage = storage
+        h = ctypes.c_void_p()
+        _abi.check(self.lib.lbm_ensemble_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lbm_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_taylor_green(self, u0, rho0=1.0):
+        _abi.check(self.lib.lbm_ensemble_init_taylor_green(self.h, float(u0), float(rho0)))
+
+    def init_equilibrium(self, rho0=1.0, vx=0.0, vy=0.0, vz=0.0):
+        _abi.check(self.lib.lbm_ensemble_init_equilibrium(self.h, float(rho0), float(vx), float(vy), float(vz)))
+
+    def _pop_shape(self, member, layout):
+        X, Y, Z = self.sizes[member]
+        g = 2 if layout == LAYOUT_GHOST else 0
+        return (27, Z + g, Y + g, X + g)
+
+    def set_populations(self, member, f, layout=LAYOUT_GHOST):
+        dtype = 0 if f.dtype == np.float64 else 1
+        a = np.ascontiguousarray(f, dtype=np.float64 if dtype == 0 else np.float32)
+        if a.shape != self._pop_shape(member, layout):
+            raise ValueError(f"populations of member {member} must have shape {self._pop_shape(member, layout)}")
+        _abi.check(self.lib.lbm_ensemble_set_populations(self.h, int(member), a.ctypes.data, layout, dtype))
+
+    def get_populations(self, member, layout=LAYOUT_GHOST, dtype=np.float64):
+        if not 0 <= int(member) < len(self.sizes):
+            raise LbmError(1, f"member {member} out of range")
+        out = np.empty(self._pop_shape(member, layout), dtype)
+        _abi.check(self.lib.lbm_ensemble_get_populations(self.h, int(member), out.ctypes.data, layout,
+                                                         0 if dtype == np.float64 else 1))
+        return out
+
+    def step(self, nsteps=1, sums=False):
+        _abi.check(self.lib.lbm_ensemble_step(self.h, int(nsteps), STEP_SUMS if sums else 0))
+
+    def sums(self):
+        """[members, 6]: sum rho, rho vx, rho vy, rho vz, rho |u|^2, non-finite count."""
+        out = np.empty((len(self.sizes), 6), np.float64)
+        _abi.check(self.lib.lbm_ensemble_get_sums(self.h, _abi.dptr(out)))
+        return out
+
+    def kinetic_energy(self, rho0=1.0):
+        """E = sum rho |u|^2 / (2 rho0 V) of every member after the last summed step."""
+        vol = np.array([x * y * z for (x, y, z) in self.sizes], np.float64)
+        return self.sums()[:, 4] / rho0 / 2.0 / vol
+
+    @property
+    def iteration(self):
+        return int(self.lib.lbm_ensemble_iteration(self.h))
+
+    @property
+    def stream(self):
+        """the ensemble's cudaStream_t as an integer"""
+        s = ctypes.c_void_p()
+        _abi.check(self.lib.lbm_ensemble_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self):
+        _abi.check(self.lib.lbm_ensemble_synchronize(self.h))
+
+    def set_shape(self, tile_sites, grid_policy):
+        _abi.check(self.lib.lbm_ensemble_set_shape(self.h, int(tile_sites), int(grid_policy)))
+
+    def shape(self):
+        a, b = ctypes.c_int(0), ctypes.c_int(0)
+        _abi.check(self.lib.lbm_ensemble_get_shape(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def autotune(self, ntrials=4):
+        _abi.check(self.lib.lbm_ensemble_autotune(self.h, int(ntrials)))
+        return self.shape()
 
 
 def kinetic_energy(lbm: LBM, rho0=1.0):

@@ -44,6 +44,14 @@ class lbm_device_view(ctypes.Structure):
                 ("macro", ctypes.c_void_p), ("macro_elem_size", ctypes.c_int32), ("stream", ctypes.c_void_p)]
 
 
+class lbm_ensemble_desc(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int32), ("X", ctypes.POINTER(ctypes.c_int32)),
+                ("Y", ctypes.POINTER(ctypes.c_int32)), ("Z", ctypes.POINTER(ctypes.c_int32)),
+                ("viscosity", ctypes.POINTER(ctypes.c_double)), ("storage", ctypes.c_int32),
+                ("collision", ctypes.c_int32), ("cum_flags", ctypes.c_int32), ("equilibrium", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("use_graphs", ctypes.c_int32)]
+
+
 lbm_handle = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
 _H = lbm_handle
@@ -75,6 +83,21 @@ SIGNATURES = {
     "lbm_get_kernel": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_status": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_version": (ctypes.c_char_p, []),
+    "lbm_ensemble_create": (ctypes.c_int, [ctypes.POINTER(lbm_ensemble_desc), ctypes.POINTER(ctypes.c_void_p)]),
+    "lbm_ensemble_destroy": (ctypes.c_int, [_H]),
+    "lbm_ensemble_init_taylor_green": (ctypes.c_int, [_H, ctypes.c_double, ctypes.c_double]),
+    "lbm_ensemble_init_equilibrium": (ctypes.c_int, [_H, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_double]),
+    "lbm_ensemble_set_populations": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lbm_ensemble_get_populations": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lbm_ensemble_step": (ctypes.c_int, [_H, ctypes.c_int64, ctypes.c_int]),
+    "lbm_ensemble_get_sums": (ctypes.c_int, [_H, _dp]),
+    "lbm_ensemble_iteration": (ctypes.c_int64, [_H]),
+    "lbm_ensemble_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
+    "lbm_ensemble_synchronize": (ctypes.c_int, [_H]),
+    "lbm_ensemble_set_shape": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int]),
+    "lbm_ensemble_get_shape": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "lbm_ensemble_autotune": (ctypes.c_int, [_H, ctypes.c_int]),
 }
 
 _LIB = None
