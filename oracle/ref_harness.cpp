@@ -38,6 +38,7 @@
 #include "lbm3d/d3q27/col_cum.h"
 #include "lbm3d/d3q27/col_mrt.h"
 #include "lbm3d/d3q27/col_srt.h"
+#include "lbm3d/d3q27/col_srt_adjoint.h"
 #include "lbm3d/d3q27/eq.h"
 #include "lbm3d/d3q27/eq_inv_cum.h"
 #include "lbm3d/d3q27/macro.h"
@@ -452,9 +453,57 @@ int collide_dispatch(int coll, long n, void* f, void* m, double nu, double fx, d
 	}
 }
 
+// kernel struct of the adjoint configuration: the primary and the measured
+// macro quantities that D3Q27_COMMON_ADJOINT::setEquilibrium reads
+template <typename REAL>
+struct HarnessAdjointKS : D3Q27_KernelStruct<REAL>
+{
+	REAL rho_m = 1.0, vx_m = 0, vy_m = 0, vz_m = 0;
+};
+
+// direction vectors in slot order (the enum of lbm3d/defs.h)
+const int HCX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+const int HCY[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
+const int HCZ[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1};
+
 }  // namespace
 
 extern "C" {
+
+// The reference's adjoint SRT collision (col_srt_adjoint.h:50-109) on n
+// independent sites: fstar[n][27] updated in place, primary velocity u[n][3].
+int ref_srt_adjoint_collision(long n, double* fstar, const double* u, double nu)
+{
+	using T = HarnessTraits<double>;
+	for (long s = 0; s < n; s++) {
+		HarnessAdjointKS<double> KS;
+		for (int q = 0; q < 27; q++)
+			KS.f[q] = fstar[s * 27 + q];
+		KS.vx = u[s * 3 + 0];
+		KS.vy = u[s * 3 + 1];
+		KS.vz = u[s * 3 + 2];
+		KS.lbmViscosity = nu;
+		D3Q27_SRT_ADJOINT<T>::collision(KS);
+		for (int q = 0; q < 27; q++)
+			fstar[s * 27 + q] = KS.f[q];
+	}
+	return 0;
+}
+
+// The reference's adjoint data term D3Q27_EQ_ADJOINT::collisionWithData
+// (eq_adjoint.h:30-33) for every direction: macro[n][8] = primary rho, vx,
+// vy, vz and measured rho_m, vx_m, vy_m, vz_m; out[n][27].
+int ref_adjoint_data_term(long n, const double* macro, double* out)
+{
+	using EQ = D3Q27_EQ_ADJOINT<HarnessTraits<double>>;
+	for (long s = 0; s < n; s++) {
+		const double* m = macro + s * 8;
+		for (int q = 0; q < 27; q++)
+			out[s * 27 + q] = EQ::collisionWithData(HCX[q], HCY[q], HCZ[q], m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7]);
+	}
+	return 0;
+}
+
 
 // Flags this build was compiled with: bit0 USE_GEIER_CUM_2017, bit1 USE_GEIER_CUM_ANTIALIAS.
 int ref_cum_flags(void)

@@ -66,6 +66,10 @@ constexpr int direct_minb()
 	return 4;  // SRT and BGK spill at 5
 }
 
+#ifndef ENS_MINB128
+#define ENS_MINB128 5
+#endif
+
 template <typename S>
 struct StorageUnit
 {
@@ -208,9 +212,10 @@ struct StorageUnit
 	template <int COLL, int CUMF, bool ODD, bool OUT, int TPB>
 	static cudaError_t ens_launch(const EnsLaunch& L)
 	{
-		// the member's collision constants live in registers here (kernel
-		// parameters in the single-lattice kernel): 128 registers per thread
-		constexpr int minb = sizeof(R) == 8 ? (TPB == 128 ? 2 : 1) : (TPB == 128 ? 4 : 2);
+		// the member's collision constants are read from the member table (kernel
+		// parameters in the single-lattice kernel); the caps are the largest
+		// that compile without spills (-Xptxas -v)
+		constexpr int minb = sizeof(R) == 8 ? (TPB == 128 ? 2 : 1) : (TPB == 128 ? ENS_MINB128 : ENS_MINB128 / 2);
 		auto kern = ens_step_kernel<S, COLL, CUMF, ODD, OUT, TPB, minb>;
 		static int per_sm_cache[64] = {0};
 		static int sms_cache[64] = {0};

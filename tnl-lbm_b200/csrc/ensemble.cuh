@@ -69,8 +69,21 @@ __global__ void __launch_bounds__(TPB, MINB)
 {
 	using T = typename S::T;
 	using R = typename S::R;
+	// the current member's table entry, staged in shared memory: its fields are
+	// read where they are used instead of occupying registers
+	__shared__ EnsMember<T, R> M;
+	constexpr int WORDS = (int) (sizeof(EnsMember<T, R>) / 4);
+	static_assert(sizeof(EnsMember<T, R>) % 4 == 0 && WORDS <= TPB, "member entry size");
+	int cur = -1;
 	for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-		const EnsMember<T, R>& M = members[tile_member[t]];
+		const int m = tile_member[t];
+		if (m != cur) {
+			__syncthreads();  // every thread is done with the previous entry
+			if ((int) threadIdx.x < WORDS)
+				reinterpret_cast<unsigned*>(&M)[threadIdx.x] = reinterpret_cast<const unsigned*>(members + m)[threadIdx.x];
+			__syncthreads();
+			cur = m;
+		}
 		const unsigned i = (unsigned) ((t - M.tile0) * TPB) + threadIdx.x;
 		double red[NRED] = {0, 0, 0, 0, 0, 0};
 		if (i < (unsigned) M.n) {
