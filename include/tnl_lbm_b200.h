@@ -265,6 +265,35 @@ LBM_API int lbm_ensemble_get_shape(lbm_ensemble e, int* tile_sites, int* grid_po
  * keeps the fastest. */
 LBM_API int lbm_ensemble_autotune(lbm_ensemble e, int ntrials);
 
+/* ---- Discrete adjoint (SRT collision, per-site body force as the control) --
+ * Gradient of an objective on the state after nsteps A-A steps with respect
+ * to a per-site body force field F [3][Z][Y][X] and to the initial population
+ * array.  The objective is J = sum_i 1/2 [rho_weight (rho_i - rho*_i)^2 +
+ * |u_i - u*_i|^2] over sample sites i (site index (z*Y + y)*X + x, distinct
+ * fluid sites), with rho and u the moments the next step would compute at
+ * the final state and target[i] = {rho*, u*x, u*y, u*z}.  The time loop is
+ * differentiated exactly (discrete adjoint), with checkpoints every
+ * checkpoint_every steps (<= 0: ceil(sqrt(nsteps))) and recomputation; the
+ * force gradient is accumulated in FP64.
+ * Requirements: LBM_COLL_SRT with LBM_EQ_SECOND_ORDER, LBM_STORE_F64 or
+ * LBM_STORE_F32, site types FLUID, WALL, INFLOW, OUTFLOW_EQ, PERIODIC,
+ * NOTHING, SYM_*.  The reference's sim_adjoint (sim_adjoint/sim_adjoint.cu)
+ * solves a steady adjoint about a frozen flow with D3Q27_SRT_ADJOINT
+ * (col_srt_adjoint.h); the transpose applied here at each site reduces to
+ * that adjoint collision at rho = 1 and F = 0.
+ * lbm_adjoint_forward starts from the current populations and iteration,
+ * advances the lattice by nsteps (force NULL: the descriptor's uniform
+ * force) and returns the objective.  lbm_adjoint_backward returns seed * dJ/dF
+ * (host [3][Z][Y][X] doubles, or NULL) and seed * dJ/d(initial populations)
+ * (layout and dtype as lbm_get_populations, or NULL).
+ * lbm_adjoint_release frees the checkpoints. */
+LBM_API int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64_t checkpoint_every,
+                                const int64_t* samples, int32_t nsamples, const double* target, double rho_weight,
+                                double* loss);
+LBM_API int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, void* grad_populations, int layout,
+                                 int dtype);
+LBM_API int lbm_adjoint_release(lbm_handle h);
+
 /* Library build information: sm architecture and version string. */
 LBM_API const char* lbm_version(void);
 

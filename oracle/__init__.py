@@ -185,6 +185,10 @@ class Reference(_Base):
         L.ref_equilibrium.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, _dp, _dp, _dp, _dp, _vp]
         L.ref_cum_flags.restype = ctypes.c_int
         assert L.ref_cum_flags() == cum_flags
+        L.ref_srt_adjoint_collision.restype = ctypes.c_int
+        L.ref_srt_adjoint_collision.argtypes = [ctypes.c_long, _dp, _dp, ctypes.c_double]
+        L.ref_adjoint_data_term.restype = ctypes.c_int
+        L.ref_adjoint_data_term.argtypes = [ctypes.c_long, _dp, _dp]
 
     def aa_run(self, f, geo_map, coll="CUM", eq="INV_CUM", cum_flags=None, nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
                macro=None, start_iter=0, nsteps=1, nthreads=0, return_time=False):
@@ -220,4 +224,20 @@ class Reference(_Base):
         rho, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (rho, vx, vy, vz))
         out = np.zeros((rho.size, 27), dtype=dtype)
         self.lib.ref_equilibrium(_prec(dtype), EQ[eq], rho.size, _dptr(rho), _dptr(vx), _dptr(vy), _dptr(vz), _ptr(out))
+        return out
+
+    def srt_adjoint_collision(self, fstar, u, nu):
+        """D3Q27_SRT_ADJOINT::collision (col_srt_adjoint.h:50-109) of fstar[n, 27]
+        about the primary velocity u[n, 3]; returns the updated copy."""
+        out = np.ascontiguousarray(fstar, dtype=np.float64).copy()
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self.lib.ref_srt_adjoint_collision(out.shape[0], _dptr(out), _dptr(u), nu)
+        return out
+
+    def adjoint_data_term(self, macro):
+        """D3Q27_EQ_ADJOINT::collisionWithData (eq_adjoint.h:30-33) of
+        macro[n, 8] = (rho, vx, vy, vz, rho_m, vx_m, vy_m, vz_m) for every direction."""
+        macro = np.ascontiguousarray(macro, dtype=np.float64)
+        out = np.zeros((macro.shape[0], 27))
+        self.lib.ref_adjoint_data_term(macro.shape[0], _dptr(macro), _dptr(out))
         return out

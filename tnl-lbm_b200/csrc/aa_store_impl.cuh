@@ -6,45 +6,13 @@
 #include <cstring>
 
 #include "aa_kernels.cuh"
+#include "coll_params.cuh"
 #include "aa_tile.cuh"
 #include "ensemble.cuh"
 #include "launch.h"
 
 namespace lbm {
 
-template <typename R>
-inline CollParams<R> make_coll_params(const CollParamsD& d)
-{
-	CollParams<R> p{};
-	const double w1 = d.w1;
-	const double g = 1.0 / w1 - 0.5;
-	p.nu = (R) d.nu;
-	p.fx = (R) d.fx;
-	p.fy = (R) d.fy;
-	p.fz = (R) d.fz;
-	p.hfx = (R) (0.5 * d.fx);
-	p.hfy = (R) (0.5 * d.fy);
-	p.hfz = (R) (0.5 * d.fz);
-	p.w1 = (R) w1;
-	p.one_m_w1 = (R) (1.0 - w1);
-	p.k33 = (R) (3.0 * (1.0 - 0.5 * w1));
-	p.hw1 = (R) (0.5 * w1);
-	p.w1_3h = (R) (1.5 * w1);
-	p.w1_3 = (R) (3.0 * w1);
-	p.w3 = (R) d.w3;
-	p.w4 = (R) d.w4;
-	p.w5 = (R) d.w5;
-	p.c43 = (R) (2.0 / 3.0 * g * d.A);
-	p.c45 = (R) (-4.0 / 3.0 * g * d.A);
-	p.cB = (R) (-1.0 / 3.0 * g * d.B);
-	p.inv_tau = (R) (1.0 / d.tau);
-	p.srt_force = (R) (1.0 - 0.5 / d.tau);
-	p.bgk_force = (R) (1.0 - 0.5 * w1);
-	p.tau = (R) d.tau;
-	p.tau2 = (R) (d.tau * d.tau);
-	p.eq = d.eq;
-	return p;
-}
 
 // Resident 128-thread blocks per SM requested from the compiler for the
 // direct step kernel; __launch_bounds__(128, n) caps registers at

@@ -1,0 +1,377 @@
+// Discrete adjoint of the A-A step with the SRT collision and a per-site body
+// force (the control), for gradients of an objective on the final state.
+//
+// One A-A step is a map of the population memory M_n -> M_{n+1} that is
+// block-diagonal over sites: site x reads 27 locations R_q(x) and writes 27
+// locations W_q(x), and {R_q(x)} = {W_q(x)} as sets (streaming_AA.h:12-116);
+// locations no site touches (ghost slots nobody writes, GEO_NOTHING sites)
+// map to themselves.  The adjoint step therefore has the same access pattern:
+// each thread gathers the adjoint of its 27 outputs from W_q(x), applies the
+// transposed Jacobian of its per-site update at the primal state M_n, and
+// scatters the result to R_q(x), in place and race-free.  No linearisation
+// error: the result is the exact gradient of the discrete FP update, up to
+// rounding.
+//
+// Per-site update (GEO type from the map, bc.h:85-412) and its transpose:
+//   FLUID, PERIODIC  rho = sum f, u = (sum c f + F/2) / rho (common.h:17-50),
+//                    out = f + (feq - f)/tau + (1 - 1/(2 tau)) S feq with
+//                    S_q = 3 (c_q - u).F / rho (col_srt.h:14-105)
+//   WALL             out_q = f_opp(q) (full-way bounce-back, bc.h:201-221)
+//   INFLOW           out = feq(1, u_inlet): no dependence on f or F
+//   OUTFLOW_EQ       out = feq(1, u(f)) (bc.h:186-190)
+//   SYM_*            mirror copy of one half of the directions (bc.h:222-293)
+// With rho and u held fixed, the SRT transpose is the reference's adjoint
+// collision (col_srt_adjoint.h:50-109, eq_adjoint.h:13-27): at rho = 1 and
+// F = 0 both give f*_j + (sum_q f*_q w_q (feq_rho + feq_v)(q; c_j) - f*_j)/tau.
+// The equilibrium is the second-order one (D3Q27_EQ, eq.h).
+#pragma once
+
+#include "aa_kernels.cuh"
+
+namespace lbm {
+
+template <typename T, typename R>
+struct AdjArgs
+{
+	T* f;			   // primal populations (the step's input, or the state to observe)
+	R* lam;			   // adjoint populations, same layout as f
+	long long sq;
+	int sy, sz, x0;
+	int X, Y, Z;
+	const uint8_t* map;	 // null: every site periodic
+	const R* in_vx;		 // inlet profiles [Z][Y] (GEO_INFLOW) or null
+	const R* in_vy;
+	const R* in_vz;
+	const R* force;	  // per-site body force [3][Z][Y][X] or null (uniform p.fx..fz)
+	double* grad;	  // d objective / d force, [3][Z][Y][X], accumulated
+	CollParams<R> p;
+};
+
+// location of the value that direction q of a site reads (R_q) or writes
+// (W_q) in the A-A step of the given parity
+template <bool ODD, int q>
+__device__ __forceinline__ long long aa_read_loc(long long sq, long long base, const Offsets& o)
+{
+	if constexpr (ODD)
+		return opp(q) * sq + base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)];
+	else
+		return q * sq + base;
+}
+template <bool ODD, int q>
+__device__ __forceinline__ long long aa_write_loc(long long sq, long long base, const Offsets& o)
+{
+	if constexpr (ODD)
+		return q * sq + base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)];
+	else
+		return opp(q) * sq + base;
+}
+
+// collision constants of one site: the per-site force replaces the uniform one
+template <typename T, typename R>
+__device__ __forceinline__ CollParams<R> site_params(const AdjArgs<T, R>& a, long long site, long long nsites)
+{
+	CollParams<R> p = a.p;
+	if (a.force) {
+		p.fx = a.force[site];
+		p.fy = a.force[nsites + site];
+		p.fz = a.force[2 * nsites + site];
+		p.hfx = R(0.5) * p.fx;
+		p.hfy = R(0.5) * p.fy;
+		p.hfz = R(0.5) * p.fz;
+	}
+	return p;
+}
+
+// d feq_q(rho, u) / d u_a of the second-order equilibrium, contracted with a
+// per-direction weight: adds l_q * d feq_q / d u to (bx, by, bz)
+template <int q, typename R>
+__device__ __forceinline__ void add_dfeq_du(R lq, R rho, R vx, R vy, R vz, R& bx, R& by, R& bz)
+{
+	const R cu = R(cx(q)) * vx + R(cy(q)) * vy + R(cz(q)) * vz;
+	const R s = lq * R(weight(q)) * rho;
+	const R g = R(3) + R(9) * cu;
+	bx += s * (g * R(cx(q)) - R(3) * vx);
+	by += s * (g * R(cy(q)) - R(3) * vy);
+	bz += s * (g * R(cz(q)) - R(3) * vz);
+}
+
+// transpose of the SRT update with body force at one site: g = J^T l, and the
+// force gradient dF += (d out / d F)^T l
+template <typename R>
+__device__ __forceinline__ void srt_vjp(const Site<R>& s, const CollParams<R>& p, const R* l, R* g, double* dF)
+{
+	const R rho = s.rho, ir = s.rho == R(0) ? R(1) : s.ir;
+	const R vx = s.vx, vy = s.vy, vz = s.vz;
+	const R usq = vx * vx + vy * vy + vz * vz;
+	const R it = p.inv_tau, k = p.srt_force;
+	R A = 0, bx = 0, by = 0, bz = 0, hx = 0, hy = 0, hz = 0;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			const R feq = eq_second<q>(rho, vx, vy, vz, usq);
+			const R S = R(3) * ((R(cx(q)) - vx) * p.fx + (R(cy(q)) - vy) * p.fy + (R(cz(q)) - vz) * p.fz) * ir;
+			const R lq = l[q];
+			A += lq * feq;
+			// d feq / d u weighted by (it + k S)
+			add_dfeq_du<q>(lq * (it + k * S), rho, vx, vy, vz, bx, by, bz);
+			// k feq dS/du = -3 k feq F / rho ; k feq dS/dF_a = 3 k feq (c_a - u_a) / rho
+			const R lf = lq * feq;
+			hx += lf * (R(cx(q)) - vx);
+			hy += lf * (R(cy(q)) - vy);
+			hz += lf * (R(cz(q)) - vz);
+		}
+	);
+	// sum_q l_q feq_q, used by the density derivative and the dS/du term
+	const R sum_lf = A;
+	A = it * sum_lf * ir;
+	bx -= R(3) * k * sum_lf * p.fx * ir;
+	by -= R(3) * k * sum_lf * p.fy * ir;
+	bz -= R(3) * k * sum_lf * p.fz * ir;
+	const R omit = R(1) - it;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int j = decltype(Qc)::value;
+			g[j] = omit * l[j] + A + (bx * (R(cx(j)) - vx) + by * (R(cy(j)) - vy) + bz * (R(cz(j)) - vz)) * ir;
+		}
+	);
+	// d out / d F: through u (du/dF = 1 / (2 rho)) and through S directly
+	const R half_ir = R(0.5) * ir, three_k_ir = R(3) * k * ir;
+	dF[0] += (double) (bx * half_ir + three_k_ir * hx);
+	dF[1] += (double) (by * half_ir + three_k_ir * hy);
+	dF[2] += (double) (bz * half_ir + three_k_ir * hz);
+}
+
+// transpose of out = feq(1, u(f)) (GEO_OUTFLOW_EQ)
+template <typename R>
+__device__ __forceinline__ void outflow_eq_vjp(const Site<R>& s, const R* l, R* g, double* dF)
+{
+	const R ir = s.ir, vx = s.vx, vy = s.vy, vz = s.vz;
+	R bx = 0, by = 0, bz = 0;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			add_dfeq_du<q>(l[q], R(1), vx, vy, vz, bx, by, bz);
+		}
+	);
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int j = decltype(Qc)::value;
+			g[j] = (bx * (R(cx(j)) - vx) + by * (R(cy(j)) - vy) + bz * (R(cz(j)) - vz)) * ir;
+		}
+	);
+	const R half_ir = R(0.5) * ir;
+	dF[0] += (double) (bx * half_ir);
+	dF[1] += (double) (by * half_ir);
+	dF[2] += (double) (bz * half_ir);
+}
+
+// transpose of the mirror copy of a symmetry plane (see symmetry(), aa_kernels.cuh)
+template <typename R>
+__device__ __forceinline__ void symmetry_vjp(const R* l, R* g, int axis, int side)
+{
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			g[q] = l[q];
+		}
+	);
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (cx(q) != 0) {
+				constexpr int m = dir(-cx(q), cy(q), cz(q));
+				if (axis == 0 && cx(q) == side) {
+					g[m] += l[q];
+					g[q] = R(0);
+				}
+			}
+			if constexpr (cy(q) != 0) {
+				constexpr int m = dir(cx(q), -cy(q), cz(q));
+				if (axis == 1 && cy(q) == side) {
+					g[m] += l[q];
+					g[q] = R(0);
+				}
+			}
+			if constexpr (cz(q) != 0) {
+				constexpr int m = dir(cx(q), cy(q), -cz(q));
+				if (axis == 2 && cz(q) == side) {
+					g[m] += l[q];
+					g[q] = R(0);
+				}
+			}
+		}
+	);
+}
+
+// Primal A-A step with SRT collision and a per-site force: the per-site code
+// of aa_step_kernel (GENERAL, COLL_SRT) with the site's force in place of the
+// uniform one.  With a uniform force field it is the production SRT step.
+template <typename S, bool ODD>
+__global__ void __launch_bounds__(128) adj_primal_kernel(const AdjArgs<typename S::T, typename S::R> a)
+{
+	using R = typename S::R;
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int y = blockIdx.y, z = blockIdx.z;
+	if (x >= a.X)
+		return;
+	const long long nsites = (long long) a.X * a.Y * a.Z;
+	const long long site = ((long long) z * a.Y + y) * a.X + x;
+	const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
+	if (geo == GEO_NOTHING)
+		return;
+	StepArgs<typename S::T, R> sa{};
+	sa.Y = a.Y;
+	sa.in_vx = a.in_vx;
+	sa.in_vy = a.in_vy;
+	sa.in_vz = a.in_vz;
+	sa.p = site_params(a, site, nsites);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+	Site<R> s;
+	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+	if (apply_boundary(s, geo, sa, z, y))
+		collide<R, COLL_SRT, 0>(s, sa.p);
+	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+}
+
+// Adjoint of one A-A step: lam (adjoint of the step's output) is replaced in
+// place by the adjoint of its input, with f the step's primal input; grad
+// accumulates the force gradient of this step.
+template <typename S, bool ODD>
+__global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S::T, typename S::R> a)
+{
+	using R = typename S::R;
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int y = blockIdx.y, z = blockIdx.z;
+	if (x >= a.X)
+		return;
+	const long long nsites = (long long) a.X * a.Y * a.Z;
+	const long long site = ((long long) z * a.Y + y) * a.X + x;
+	const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
+	if (geo == GEO_NOTHING)
+		return;
+	const CollParams<R> p = site_params(a, site, nsites);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+	R l[27], g[27];
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			l[q] = a.lam[aa_write_loc<ODD, q>(a.sq, base, o)];
+		}
+	);
+	double dF[3] = {0, 0, 0};
+	switch (geo) {
+		case GEO_WALL:
+			static_for<27>(
+				[&](auto Qc)
+				{
+					constexpr int q = decltype(Qc)::value;
+					g[q] = l[opp(q)];
+				}
+			);
+			break;
+		case GEO_INFLOW:
+			static_for<27>(
+				[&](auto Qc)
+				{
+					constexpr int q = decltype(Qc)::value;
+					g[q] = R(0);
+				}
+			);
+			break;
+		case GEO_SYM_TOP:
+		case GEO_SYM_BOTTOM:
+		case GEO_SYM_LEFT:
+		case GEO_SYM_RIGHT:
+		case GEO_SYM_BACK:
+		case GEO_SYM_FRONT: {
+			const int axis = geo <= GEO_SYM_BOTTOM ? 2 : (geo <= GEO_SYM_RIGHT ? 0 : 1);
+			const int side = (geo == GEO_SYM_TOP || geo == GEO_SYM_RIGHT || geo == GEO_SYM_FRONT) ? -1 : 1;
+			symmetry_vjp(l, g, axis, side);
+			break;
+		}
+		default: {	// FLUID, PERIODIC, OUTFLOW_EQ: need the primal moments
+			Site<R> s;
+			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+			density_velocity(s, p);
+			if (geo == GEO_OUTFLOW_EQ)
+				outflow_eq_vjp(s, l, g, dF);
+			else
+				srt_vjp(s, p, l, g, dF);
+		}
+	}
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			a.lam[aa_read_loc<ODD, q>(a.sq, base, o)] = g[q];
+		}
+	);
+	if (a.grad && a.force && (dF[0] != 0.0 || dF[1] != 0.0 || dF[2] != 0.0)) {
+		a.grad[site] += dF[0];
+		a.grad[nsites + site] += dF[1];
+		a.grad[2 * nsites + site] += dF[2];
+	}
+}
+
+// Objective on the state f (the input of a step of the given parity):
+// J = sum_i 1/2 [w_rho (rho_i - rho*_i)^2 + |u_i - u*_i|^2] at the sample
+// sites, with rho and u the moments that step computes (density_velocity).
+// Writes the per-sample terms to loss[i]; with lam set, adds seed * dJ/df to
+// lam at the read locations and seed * dJ/dF to grad.  Sample sites are
+// distinct fluid sites.
+template <typename S, bool ODD>
+__global__ void adj_objective_kernel(const AdjArgs<typename S::T, typename S::R> a, const long long* __restrict__ samples,
+									 const double* __restrict__ target, int nsamples, double w_rho, double seed,
+									 double* __restrict__ loss)
+{
+	using R = typename S::R;
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nsamples)
+		return;
+	const long long site = samples[i];
+	const long long nsites = (long long) a.X * a.Y * a.Z;
+	const int x = (int) (site % a.X);
+	const int y = (int) ((site / a.X) % a.Y);
+	const int z = (int) (site / ((long long) a.X * a.Y));
+	const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
+	const CollParams<R> p = site_params(a, site, nsites);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+	Site<R> s;
+	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+	density_velocity(s, p);
+	const double drho = (double) s.rho - target[4 * i + 0];
+	const double dvx = (double) s.vx - target[4 * i + 1];
+	const double dvy = (double) s.vy - target[4 * i + 2];
+	const double dvz = (double) s.vz - target[4 * i + 3];
+	loss[i] = 0.5 * (w_rho * drho * drho + dvx * dvx + dvy * dvy + dvz * dvz);
+	if (!a.lam)
+		return;
+	const R ir = s.ir;
+	const R ex = (R) (seed * dvx), ey = (R) (seed * dvy), ez = (R) (seed * dvz), er = (R) (seed * w_rho * drho);
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			const R d = er + (ex * (R(cx(q)) - s.vx) + ey * (R(cy(q)) - s.vy) + ez * (R(cz(q)) - s.vz)) * ir;
+			a.lam[aa_read_loc<ODD, q>(a.sq, base, o)] += d;
+		}
+	);
+	if (a.grad && a.force) {
+		const double h = 0.5 / (double) s.rho;
+		a.grad[site] += seed * dvx * h;
+		a.grad[nsites + site] += seed * dvy * h;
+		a.grad[2 * nsites + site] += seed * dvz * h;
+	}
+}
+
+}  // namespace lbm

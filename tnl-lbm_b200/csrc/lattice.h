@@ -1,0 +1,90 @@
+// Host-side state of one lattice handle (lbm_handle of the C-ABI), shared by
+// the translation units that implement the C-ABI (lbm_abi.cu, lbm_adjoint.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tnl_lbm_b200.h"
+#include "launch.h"
+
+namespace lbm {
+struct AdjointState;  // lbm_adjoint.cu
+void adjoint_free(AdjointState*);
+}  // namespace lbm
+
+struct lbm_lattice
+{
+	lbm_desc d{};
+	const lbm::StorageOps* ops = nullptr;
+	lbm::Geometry g{};
+	size_t pop_bytes = 0;
+	cudaStream_t stream = nullptr;
+	uint8_t* map = nullptr;
+	bool map_set = false;
+	void* inflow[3] = {nullptr, nullptr, nullptr};
+	void* inflow_host = nullptr;  // pinned staging of the converted profiles
+	void* macro = nullptr;
+	bool macro_valid = false;
+	double* partials = nullptr;
+	long long partials_cap = 0;	 // in blocks
+	double* sums_dev = nullptr;
+	double* sums_host = nullptr;  // pinned [NRED]
+	bool sums_valid = false;
+	long long iteration = 0;
+	int bx = 0, by = 0;	 // 0: default
+	int kernel = lbm::KERNEL_DIRECT;
+	int sms = 148;
+	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
+	long long last_blocks = 0;	// blocks of the last step launch
+	lbm::CollParamsD p{};
+	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
+	cudaGraphExec_t graph = nullptr;
+	std::vector<uint8_t> map_host;			 // host copy of the accepted map
+	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
+	static constexpr int GRAPH_STEPS = 16;
+
+	long long sites() const
+	{
+		return (long long) d.X * d.Y * d.Z;
+	}
+	dim3 block() const
+	{
+		if (bx > 0)
+			return dim3(bx, by, 1);
+		const int bxd = d.X >= 128 ? 128 : ((d.X + 31) / 32) * 32;
+		return dim3(bxd, 128 / bxd, 1);
+	}
+	dim3 grid() const
+	{
+		const dim3 b = block();
+		return dim3((d.X + b.x - 1) / b.x, (d.Y + b.y - 1) / b.y, d.Z);
+	}
+	long long grid_blocks() const
+	{
+		const dim3 gr = grid();
+		return (long long) gr.x * gr.y * gr.z;
+	}
+	// partial-sum slots any step kernel variant may need
+	long long max_step_blocks() const
+	{
+		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
+		const long long direct = grid_blocks();
+		return tile > direct ? tile : direct;
+	}
+	void drop_graph()
+	{
+		if (graph) {
+			cudaGraphExecDestroy(graph);
+			graph = nullptr;
+		}
+	}
+};
+
+namespace lbm {
+// message of lbm_last_error() for the calling thread (lbm_abi.cu)
+int record_error(int code, const char* msg);
+}  // namespace lbm

@@ -18,6 +18,7 @@
 #include "../../include/tnl_lbm_b200.h"
 #include "d3q27.cuh"
 #include "host_common.h"
+#include "lattice.h"
 #include "launch.h"
 
 namespace lbm {
@@ -100,71 +101,6 @@ int record_error(int code, const char* msg)
 }
 }  // namespace lbm
 
-struct lbm_lattice
-{
-	lbm_desc d{};
-	const lbm::StorageOps* ops = nullptr;
-	lbm::Geometry g{};
-	size_t pop_bytes = 0;
-	cudaStream_t stream = nullptr;
-	uint8_t* map = nullptr;
-	bool map_set = false;
-	void* inflow[3] = {nullptr, nullptr, nullptr};
-	void* inflow_host = nullptr;  // pinned staging of the converted profiles
-	void* macro = nullptr;
-	bool macro_valid = false;
-	double* partials = nullptr;
-	long long partials_cap = 0;	 // in blocks
-	double* sums_dev = nullptr;
-	double* sums_host = nullptr;  // pinned [NRED]
-	bool sums_valid = false;
-	long long iteration = 0;
-	int bx = 0, by = 0;	 // 0: default
-	int kernel = lbm::KERNEL_DIRECT;
-	int sms = 148;
-	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
-	long long last_blocks = 0;	// blocks of the last step launch
-	lbm::CollParamsD p{};
-	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
-	cudaGraphExec_t graph = nullptr;
-	static constexpr int GRAPH_STEPS = 16;
-
-	long long sites() const
-	{
-		return (long long) d.X * d.Y * d.Z;
-	}
-	dim3 block() const
-	{
-		if (bx > 0)
-			return dim3(bx, by, 1);
-		const int bxd = d.X >= 128 ? 128 : ((d.X + 31) / 32) * 32;
-		return dim3(bxd, 128 / bxd, 1);
-	}
-	dim3 grid() const
-	{
-		const dim3 b = block();
-		return dim3((d.X + b.x - 1) / b.x, (d.Y + b.y - 1) / b.y, d.Z);
-	}
-	long long grid_blocks() const
-	{
-		const dim3 gr = grid();
-		return (long long) gr.x * gr.y * gr.z;
-	}
-	// partial-sum slots any step kernel variant may need
-	long long max_step_blocks() const
-	{
-		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
-		const long long direct = grid_blocks();
-		return tile > direct ? tile : direct;
-	}
-	void drop_graph()
-	{
-		if (graph) {
-			cudaGraphExecDestroy(graph);
-			graph = nullptr;
-		}
-	}
-};
 
 namespace {
 
@@ -389,6 +325,7 @@ int lbm_destroy(lbm_handle h)
 	if (h->stream)
 		cudaStreamSynchronize(h->stream);
 	h->drop_graph();
+	lbm::adjoint_free(h->adjoint);
 	cudaFree(h->g.f);
 	cudaFree(h->map);
 	for (auto* p : h->inflow)
@@ -424,6 +361,7 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 						(int) map[i], i);
 	LBM_CUDA(cudaMemcpyAsync(h->map, map, (size_t) n, cudaMemcpyHostToDevice, h->stream));
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	h->map_host.assign(map, map + n);
 	h->map_set = true;
 	return LBM_OK;
 }

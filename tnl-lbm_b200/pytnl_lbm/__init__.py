@@ -183,6 +183,39 @@ class LBM:
         _abi.check(self.lib.lbm_device_view_get(self.h, ctypes.byref(v)))
         return v
 
+    # -- discrete adjoint (SRT collision, per-site body force) -------------
+    def adjoint_forward(self, force, nsteps, samples, target, checkpoint_every=0, rho_weight=0.0):
+        """Run nsteps from the current state with the per-site force field
+        ``force`` [3, Z, Y, X] (None: the uniform force of the lattice) and
+        return J = sum_i 1/2 [rho_weight (rho_i - rho*_i)^2 + |u_i - u*_i|^2]
+        at the sample sites (flat indices (z*Y + y)*X + x) against
+        ``target`` [n, 4] = (rho*, u*x, u*y, u*z)."""
+        samples = np.ascontiguousarray(samples, dtype=np.int64)
+        target = np.ascontiguousarray(target, dtype=np.float64).reshape(len(samples), 4)
+        fp = None
+        if force is not None:
+            force = np.ascontiguousarray(force, dtype=np.float64)
+            if force.shape != (3,) + self.shape:
+                raise ValueError(f"force must have shape {(3,) + self.shape}")
+            fp = _abi.dptr(force)
+        loss = ctypes.c_double(0.0)
+        _abi.check(self.lib.lbm_adjoint_forward(
+            self.h, fp, int(nsteps), int(checkpoint_every), samples.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            len(samples), _abi.dptr(target), float(rho_weight), ctypes.byref(loss)))
+        return loss.value
+
+    def adjoint_backward(self, seed=1.0, populations=False, layout=LAYOUT_GHOST):
+        """seed * dJ/dF [3, Z, Y, X] and, with ``populations``, seed * dJ/d(initial
+        populations) in the layout of get_populations."""
+        g = np.empty((3,) + self.shape, np.float64)
+        gp = np.empty(self._pop_shape(layout), np.float64) if populations else None
+        _abi.check(self.lib.lbm_adjoint_backward(self.h, float(seed), _abi.dptr(g),
+                                                 gp.ctypes.data if gp is not None else None, layout, 0))
+        return (g, gp) if populations else g
+
+    def adjoint_release(self):
+        _abi.check(self.lib.lbm_adjoint_release(self.h))
+
     def populations_tensor(self):
         """torch view of the raw population storage [27, Z+2, Y+2, pitch] (no copy)."""
         import torch

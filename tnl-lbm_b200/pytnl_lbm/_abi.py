@@ -83,6 +83,10 @@ SIGNATURES = {
     "lbm_get_kernel": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_status": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_version": (ctypes.c_char_p, []),
+    "lbm_adjoint_forward": (ctypes.c_int, [_H, _dp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.c_int32, _dp, ctypes.c_double, _dp]),
+    "lbm_adjoint_backward": (ctypes.c_int, [_H, ctypes.c_double, _dp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lbm_adjoint_release": (ctypes.c_int, [_H]),
     "lbm_ensemble_create": (ctypes.c_int, [ctypes.POINTER(lbm_ensemble_desc), ctypes.POINTER(ctypes.c_void_p)]),
     "lbm_ensemble_destroy": (ctypes.c_int, [_H]),
     "lbm_ensemble_init_taylor_green": (ctypes.c_int, [_H, ctypes.c_double, ctypes.c_double]),
