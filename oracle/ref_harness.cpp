@@ -8,7 +8,13 @@
 // test-suite as a checker, by tests/golden/make_golden.py to produce fixtures,
 // and by bench.py's CPU-baseline leg.  The product library never links it.
 //
-// Streaming pattern: A-A (streaming_AA.h).  The reference's A-A kernel assumes
+// Streaming pattern: A-A (streaming_AA.h) by default; compiled with
+// -DAB_PATTERN the same file runs the reference's A-B pull scheme
+// (streaming_AB.h) with its two buffers swapped after every step
+// (lbm.hpp:314-322) and the clamped neighbour indices of a single block
+// (kernels.h:48-55), and exports ref_ab_run instead of ref_aa_run.  The two
+// headers define the same template name, so each pattern is its own library.
+// The reference's A-A kernel assumes
 // one ghost layer of lattice sites in every direction (kernels.h:30-37) that
 // is initialised together with the interior (lbm_block.hpp:248-278), so the
 // harness allocates that layer.  Storage order is the reference's own
@@ -21,6 +27,7 @@
 // USE_GEIER_CUM_ANTIALIAS are preprocessor switches in the reference
 // (defs.h:312-315), so this file is compiled once per flag set (see Makefile).
 
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstdlib>
@@ -42,7 +49,11 @@
 #include "lbm3d/d3q27/eq.h"
 #include "lbm3d/d3q27/eq_inv_cum.h"
 #include "lbm3d/d3q27/macro.h"
-#include "lbm3d/d3q27/streaming_AA.h"
+#ifdef AB_PATTERN
+	#include "lbm3d/d3q27/streaming_AB.h"
+#else
+	#include "lbm3d/d3q27/streaming_AA.h"
+#endif
 
 namespace {
 
@@ -57,6 +68,7 @@ struct HarnessTraits
 
 int g_unsupported_hit = 0;
 
+#ifndef AB_PATTERN
 // The reference's A-A streaming lacks the two members that D3Q27_BC_All calls
 // for adjoint and interpolated-outflow sites (bc.h:79, bc.h:196).  The harness
 // rejects maps containing those site types before stepping, so these bodies
@@ -78,6 +90,12 @@ struct HarnessStreamingAA : D3Q27_STREAMING<TRAITS>
 		g_unsupported_hit = 1;
 	}
 };
+template <typename TRAITS>
+using HarnessStreaming = HarnessStreamingAA<TRAITS>;
+#else
+template <typename TRAITS>
+using HarnessStreaming = D3Q27_STREAMING<TRAITS>;
+#endif
 
 // Kernel data: the members D3Q27_BC_All, D3Q27_STREAMING and
 // D3Q27_MACRO_Default touch (lbm_data.h:8-61 LBM_Data, :65-73 NSE_Data,
@@ -143,7 +161,7 @@ using HarnessConfig = LBM_CONFIG<
 	HarnessData<HarnessTraits<DREAL>>,
 	COLL,
 	EQ,
-	HarnessStreamingAA<HarnessTraits<DREAL>>,
+	HarnessStreaming<HarnessTraits<DREAL>>,
 	D3Q27_BC_All,
 	D3Q27_MACRO_Default<HarnessTraits<DREAL>>>;
 
@@ -173,12 +191,21 @@ inline void init_indices(
 		zm = (z == 0) ? (SD.Z() - 1) : (z - 1);
 	}
 	else {
+#ifdef AB_PATTERN
+		xp = std::min(x + 1, (long) SD.X() - 1);
+		xm = std::max(x - 1, 0L);
+		yp = std::min(y + 1, (long) SD.Y() - 1);
+		ym = std::max(y - 1, 0L);
+		zp = std::min(z + 1, (long) SD.Z() - 1);
+		zm = std::max(z - 1, 0L);
+#else
 		xp = x + 1;
 		xm = x - 1;
 		yp = y + 1;
 		ym = y - 1;
 		zp = z + 1;
 		zm = z - 1;
+#endif
 	}
 }
 
@@ -207,17 +234,29 @@ inline void site_update(typename NSE::DATA& SD, long x, long y, long z, bool out
 // these present the harness runs single-threaded in the reference loop order
 bool map_is_order_dependent(const short* map, long n)
 {
+#ifdef AB_PATTERN
+	(void) map;
+	(void) n;
+	return false;  // A-B reads only the previous step's buffer
+#else
 	for (long i = 0; i < n; i++)
 		if (map[i] == 4 || map[i] == 7)
 			return true;
 	return false;
+#endif
 }
 
 bool map_is_supported(const short* map, long n)
 {
-	for (long i = 0; i < n; i++)
+	for (long i = 0; i < n; i++) {
+#ifdef AB_PATTERN
+		if (map[i] < 0 || map[i] > 16)
+			return false;
+#else
 		if (map[i] < 0 || map[i] == 8 || map[i] > 16)
 			return false;
+#endif
+	}
 	return true;
 }
 
@@ -293,6 +332,12 @@ int run_aa(
 	SD.fy = (dreal) fy;
 	SD.fz = (dreal) fz;
 	SD.dfs[df_cur] = df.data();
+#ifdef AB_PATTERN
+	// the write buffer starts as a copy: ghost and GEO_NOTHING entries are
+	// never written and must hold the same values in both buffers
+	std::vector<dreal> df2(df);
+	SD.dfs[df_out] = df2.data();
+#endif
 	SD.dmacro = macro;
 	SD.dmap = map;
 	SD.inflow_vx = convert_profile(in_vx, pvx);
@@ -318,11 +363,14 @@ int run_aa(
 			for (long z = 0; z < Z; z++)
 				for (long y = 0; y < Y; y++)
 					site_update<NSE>(SD, x, y, z, output_macro);
+#ifdef AB_PATTERN
+		std::swap(SD.dfs[df_cur], SD.dfs[df_out]);	// pointer rotation of lbm.hpp:314-322
+#endif
 	}
 	const auto t1 = std::chrono::steady_clock::now();
 	if (elapsed_s)
 		*elapsed_s = std::chrono::duration<double>(t1 - t0).count();
-	ref_to_canonical(df.data(), f_canonical, X, Y, Z);
+	ref_to_canonical(SD.dfs[df_cur], f_canonical, X, Y, Z);
 	return g_unsupported_hit ? -3 : 0;
 }
 
@@ -522,7 +570,12 @@ int ref_cum_flags(void)
 // eq: 0 = D3Q27_EQ (eq.h), 1 = D3Q27_EQ_INV_CUM (eq_inv_cum.h).
 // f: [27][Z+2][Y+2][X+2] (x fastest), updated in place.  map: [Z][Y][X] GEO values.
 // inflow profiles: [Z][Y] or NULL.  macro: [4][Z][Y][X] (rho, vx, vy, vz) or NULL.
-int ref_aa_run(int prec, int coll, int eq, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy,
+#ifdef AB_PATTERN
+	#define LBM_HARNESS_RUN ref_ab_run
+#else
+	#define LBM_HARNESS_RUN ref_aa_run
+#endif
+int LBM_HARNESS_RUN(int prec, int coll, int eq, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy,
 			   double fz, const double* vx, const double* vy, const double* vz, void* macro, long start_iter, int nsteps,
 			   int nthreads, double* elapsed_s)
 {

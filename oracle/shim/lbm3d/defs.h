@@ -4,7 +4,7 @@
 // "lbm3d/defs.h", which pulls in TNL, MPI and the NDArray machinery.  None of
 // that is needed to evaluate the per-site arithmetic, so this header restates
 // only the pieces the operator headers reference:
-//   - the A-A pattern switch and the DF buffer enum      (defs.h:20-67)
+//   - the A-A / A-B pattern switch and the DF buffer enum (defs.h:20-67)
 //   - the D3Q27 kernel struct                             (defs.h:255-276)
 //   - the plugin composition template LBM_CONFIG          (defs.h:288-310)
 //   - the 27-direction enum, whose numbering is part of
@@ -18,18 +18,28 @@
 
 #include <TNL/Backend/Macros.h>
 
-#ifndef AA_PATTERN
+#if ! defined(AB_PATTERN) && ! defined(AA_PATTERN)
 	#define AA_PATTERN
 #endif
 
 #define CUDA_HOSTDEV
 
+#ifdef AB_PATTERN
+// A-B pattern: read buffer and write buffer, swapped every step (defs.h:54-60)
+enum : std::uint8_t
+{
+	df_cur,
+	df_out,
+	DFMAX
+};
+#else
 // A-A pattern keeps a single in-place population buffer (defs.h:61-66)
 enum : std::uint8_t
 {
 	df_cur,
 	DFMAX
 };
+#endif
 
 // KernelStruct - D3Q27 (field set and defaults as defs.h:257-263)
 template <typename REAL>
