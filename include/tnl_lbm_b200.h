@@ -104,8 +104,10 @@ LBM_API const char* lbm_last_error(void);
 /* Per-site GEO types, host [Z][Y][X] uint8; required unless desc.periodic.
  * Replaces LBM_BLOCK map setup + copyMapToDevice (lbm_block.hpp, state.hpp:1151-1232).
  * Supported: GEO_FLUID, WALL, INFLOW, INFLOW_LEFT, INFLOW_EQ_LEFT, OUTFLOW_EQ,
- * PERIODIC, NOTHING, SYM_TOP..SYM_FRONT.  Returns LBM_ERR_UNSUPPORTED for
- * INFLOW_BB_LEFT, OUTFLOW_RIGHT, OUTFLOW_RIGHT_INTERP and the adjoint types. */
+ * PERIODIC, NOTHING, SYM_TOP..SYM_FRONT, and with LBM_STREAMING_AB also
+ * INFLOW_BB_LEFT, OUTFLOW_RIGHT, OUTFLOW_RIGHT_INTERP.  Returns
+ * LBM_ERR_UNSUPPORTED for those three under A-A (their A-A update depends on
+ * the order in which sites run) and for the adjoint types. */
 LBM_API int lbm_set_map(lbm_handle h, const uint8_t* map);
 
 /* Inlet velocity profiles, host [Z][Y] doubles; NULL means zero.
@@ -176,6 +178,20 @@ LBM_API int lbm_autotune(lbm_handle h, int ntrials);
 #define LBM_KERNEL_TILE 1
 LBM_API int lbm_set_kernel(lbm_handle h, int kernel);
 LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
+
+/* Streaming pattern (STREAMING of LBM_CONFIG).  LBM_STREAMING_AA (default):
+ * in place, one buffer, streaming_AA.h.  LBM_STREAMING_AB: the pull scheme of
+ * streaming_AB.h with a second population buffer, swapped after every step
+ * (lbm.hpp:314-322); boundary sites read clamped neighbours as a single
+ * block does (kernels.h:48-55), and the map may also hold GEO_INFLOW_BB_LEFT,
+ * GEO_OUTFLOW_RIGHT and GEO_OUTFLOW_RIGHT_INTERP.  Switching to A-B copies the
+ * current populations into the second buffer; switching back is refused
+ * while the map holds one of those three types.  The discrete adjoint
+ * (lbm_adjoint_*) runs on A-A lattices only. */
+#define LBM_STREAMING_AA 0
+#define LBM_STREAMING_AB 1
+LBM_API int lbm_set_streaming(lbm_handle h, int streaming);
+LBM_API int lbm_get_streaming(lbm_handle h, int* streaming);
 
 /* Device status word: bit LBM_STATUS_TIMEOUT is set when a bounded wait inside
  * a kernel gave up (the kernel then stops early; the step's result is invalid). */

@@ -241,3 +241,46 @@ class Reference(_Base):
         out = np.zeros((macro.shape[0], 27))
         self.lib.ref_adjoint_data_term(macro.shape[0], _dptr(macro), _dptr(out))
         return out
+
+
+_REF_AB_VARIANTS = {0: "libref_ab_default", CUM_ANTIALIAS: "libref_ab_aa", CUM_2017 | CUM_ANTIALIAS: "libref_ab_2017aa"}
+
+
+def reference_ab_available(cum_flags: int = 0) -> bool:
+    name = _REF_AB_VARIANTS.get(cum_flags)
+    return name is not None and os.path.exists(os.path.join(REFDIR, name + ".so"))
+
+
+class ReferenceAB(_Base):
+    """TNL-LBM's own per-site code with its A-B pull scheme (streaming_AB.h):
+    two buffers swapped after every step, clamped neighbours at non-periodic
+    boundary sites (kernels.h:48-55)."""
+
+    def __init__(self, cum_flags: int = 0):
+        path = os.path.join(REFDIR, _REF_AB_VARIANTS[cum_flags] + ".so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.cum_flags = cum_flags
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_ab_run.restype = ctypes.c_int
+        L.ref_ab_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_long, _vp,
+                                 _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp,
+                                 _vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_cum_flags.restype = ctypes.c_int
+        assert L.ref_cum_flags() == cum_flags
+
+    def ab_run(self, f, geo_map, coll="CUM", eq="INV_CUM", nu=0.01, force=(0.0, 0.0, 0.0), inflow=None, macro=None,
+               nsteps=1, nthreads=0):
+        """nsteps A-B steps of f [27, Z+2, Y+2, X+2] in place (the second buffer
+        starts as a copy of f); macro [4, Z, Y, X] of the last step or None."""
+        Z, Y, X = geo_map.shape
+        assert f.shape == (27, Z + 2, Y + 2, X + 2) and f.flags.c_contiguous
+        m = np.ascontiguousarray(geo_map, dtype=np.int16)
+        vx, vy, vz = _profiles(inflow)
+        el = ctypes.c_double(0.0)
+        rc = self.lib.ref_ab_run(_prec(f.dtype), COLL[coll], EQ[eq], X, Y, Z, _ptr(f), _ptr(m), nu, *force, _dptr(vx),
+                                 _dptr(vy), _dptr(vz), _ptr(macro), 0, nsteps, nthreads, ctypes.byref(el))
+        if rc != 0:
+            raise RuntimeError(f"ref_ab_run failed with {rc}")
+        return f

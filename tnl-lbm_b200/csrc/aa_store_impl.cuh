@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "aa_kernels.cuh"
+#include "ab_kernels.cuh"
 #include "coll_params.cuh"
 #include "aa_tile.cuh"
 #include "ensemble.cuh"
@@ -116,7 +117,7 @@ struct StorageUnit
 		return general ? launch_one<COLL, CUMF, false, true>(L, a) : launch_one<COLL, CUMF, false, false>(L, a);
 	}
 
-	static cudaError_t step(const StepLaunch& L)
+	static StepArgs<T, R> step_args(const StepLaunch& L)
 	{
 		StepArgs<T, R> a;
 		a.f = (T*) L.g.f;
@@ -134,6 +135,12 @@ struct StorageUnit
 		a.macro = (R*) L.macro;
 		a.partials = L.partials;
 		a.p = make_coll_params<R>(L.p);
+		return a;
+	}
+
+	static cudaError_t step(const StepLaunch& L)
+	{
+		const StepArgs<T, R> a = step_args(L);
 		switch (L.coll) {
 			case COLL_CUM:
 				switch (L.cum_flags) {
@@ -152,6 +159,49 @@ struct StorageUnit
 				return launch_parity<COLL_BGK, 0>(L, a);
 			case COLL_MRT:
 				return launch_parity<COLL_MRT, 0>(L, a);
+			default:
+				return cudaErrorInvalidValue;
+		}
+	}
+
+	// ---- A-B pull step
+	template <int COLL, int CUMF>
+	static cudaError_t ab_launch(const StepLaunch& L, const StepArgs<T, R>& a)
+	{
+		if (L.blocks_out)
+			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
+		if (L.dry_run)
+			return cudaSuccess;
+		if (L.macro || L.partials)
+			ab_step_kernel<S, COLL, CUMF, true, direct_minb<R, COLL, CUMF, true, true, true>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a, (T*) L.f_out);
+		else
+			ab_step_kernel<S, COLL, CUMF, false, direct_minb<R, COLL, CUMF, true, true, false>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a, (T*) L.f_out);
+		return cudaGetLastError();
+	}
+
+	static cudaError_t ab_step(const StepLaunch& L)
+	{
+		const StepArgs<T, R> a = step_args(L);
+		switch (L.coll) {
+			case COLL_CUM:
+				switch (L.cum_flags) {
+					case 0:
+						return ab_launch<COLL_CUM, 0>(L, a);
+					case CUM_ANTIALIAS:
+						return ab_launch<COLL_CUM, CUM_ANTIALIAS>(L, a);
+					case CUM_2017 | CUM_ANTIALIAS:
+						return ab_launch<COLL_CUM, CUM_2017 | CUM_ANTIALIAS>(L, a);
+					default:
+						return cudaErrorInvalidValue;
+				}
+			case COLL_SRT:
+				return ab_launch<COLL_SRT, 0>(L, a);
+			case COLL_BGK:
+				return ab_launch<COLL_BGK, 0>(L, a);
+			case COLL_MRT:
+				return ab_launch<COLL_MRT, 0>(L, a);
 			default:
 				return cudaErrorInvalidValue;
 		}
@@ -386,6 +436,7 @@ cudaError_t StorageUnit<S>::unpack(const Geometry& g, const void* dense, int dty
 									   &StorageUnit<S>::init_eq,                                                     \
 									   &StorageUnit<S>::pack,                                                        \
 									   &StorageUnit<S>::unpack,                                                      \
+									   &StorageUnit<S>::ab_step,                                                     \
 									   sizeof(EnsMember<typename S::T, typename S::R>),                              \
 									   &StorageUnit<S>::ens_entry,                                                   \
 									   &StorageUnit<S>::ens_step,                                                    \

@@ -44,6 +44,9 @@ struct lbm_lattice
 	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
 	cudaGraphExec_t graph = nullptr;
 	std::vector<uint8_t> map_host;			 // host copy of the accepted map
+	int streaming = LBM_STREAMING_AA;
+	void* f_out = nullptr;		// A-B: the write buffer (swapped with g.f after every step)
+	void* graph_in = nullptr;	// g.f when the graph was captured
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
 	static constexpr int GRAPH_STEPS = 16;
 

@@ -64,6 +64,7 @@ struct StepLaunch
 	cudaStream_t stream;
 	long long* blocks_out;	// number of blocks the launch used (partials)
 	bool dry_run;			// only resolve launch facts (attributes, grid), launch nothing
+	void* f_out;			// A-B step: the output buffer (g.f is the input)
 };
 
 // step kernel variants: one thread per site with direct loads, or the
@@ -102,6 +103,8 @@ struct StorageOps
 	// (dtype 0) or float (dtype 1); ghost = 1 includes the ghost layer
 	cudaError_t (*pack)(const Geometry&, void* dense, int dtype, int ghost, cudaStream_t);
 	cudaError_t (*unpack)(const Geometry&, const void* dense, int dtype, int ghost, cudaStream_t);
+	// one A-B step (ab_kernels.cuh) from L.g.f into L.f_out
+	cudaError_t (*ab_step)(const StepLaunch&);
 	// ensemble: bytes of one member-table entry, host-side fill of an entry,
 	// and the step
 	size_t ens_entry_bytes;

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -156,13 +157,26 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	long long blocks = 0;
 	L.blocks_out = &blocks;
 	L.dry_run = dry_run;
-	const cudaError_t err = h->ops->step(L);
+	L.f_out = h->f_out;
+	const bool ab = h->streaming == LBM_STREAMING_AB;
+	const cudaError_t err = ab ? h->ops->ab_step(L) : h->ops->step(L);
 	if (err != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(err));
 	if (dry_run)
 		return LBM_OK;
 	h->last_blocks = blocks;
 	h->iteration++;
+	if (ab)	 // pointer rotation of lbm.hpp:314-322
+		std::swap(h->g.f, h->f_out);
+	return LBM_OK;
+}
+
+// A-B: ghost and GEO_NOTHING entries are never written, so both buffers must
+// hold the same values; called after every write of the populations
+int sync_ab_buffers(lbm_handle h)
+{
+	if (h->streaming == LBM_STREAMING_AB && h->f_out)
+		LBM_CUDA(cudaMemcpyAsync(h->f_out, h->g.f, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream));
 	return LBM_OK;
 }
 
@@ -180,6 +194,7 @@ int build_graph(lbm_handle h)
 		}
 	}
 	h->iteration = 0;  // graph starts at an even step
+	h->graph_in = h->g.f;
 	cudaGraph_t graph = nullptr;
 	LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
 	int rc = LBM_OK;
@@ -212,7 +227,7 @@ int run_plain_steps(lbm_handle h, long long n)
 		n--;
 	}
 	if (h->d.use_graphs && n >= lbm_lattice::GRAPH_STEPS) {
-		if (!h->graph) {
+		if (!h->graph || h->graph_in != h->g.f) {
 			int rc = build_graph(h);
 			if (rc)
 				return rc;
@@ -327,6 +342,7 @@ int lbm_destroy(lbm_handle h)
 	h->drop_graph();
 	lbm::adjoint_free(h->adjoint);
 	cudaFree(h->g.f);
+	cudaFree(h->f_out);
 	cudaFree(h->map);
 	for (auto* p : h->inflow)
 		cudaFree(p);
@@ -354,7 +370,10 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		return fail(LBM_ERR_INVALID, "null map");
 	const long long n = h->sites();
 	for (long long i = 0; i < n; i++)
-		if (!site_type_supported(map[i]))
+		if (!site_type_supported(map[i])
+			&& !(h->streaming == LBM_STREAMING_AB
+				 && (map[i] == lbm::GEO_INFLOW_BB_LEFT || map[i] == lbm::GEO_OUTFLOW_RIGHT
+					 || map[i] == lbm::GEO_OUTFLOW_RIGHT_INTERP)))
 			return fail(LBM_ERR_UNSUPPORTED,
 						"site type %d at index %lld is not provided by the A-A kernels (reads a slot another site writes "
 						"in the same pass, or belongs to the adjoint set)",
@@ -447,6 +466,8 @@ int lbm_init_equilibrium(lbm_handle h, const double* rho, const double* vx, cons
 		cudaFreeAsync(dev, h->stream);
 	if (e != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "init kernel failed: %s", cudaGetErrorString(e));
+	if (int rc = sync_ab_buffers(h))
+		return rc;
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	h->iteration = 0;
 	h->macro_valid = h->sums_valid = false;
@@ -465,6 +486,8 @@ int lbm_init_taylor_green(lbm_handle h, double u0, double rho0)
 	const cudaError_t e = h->ops->init_eq(h->g, spec, h->stream);
 	if (e != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "init kernel failed: %s", cudaGetErrorString(e));
+	if (int rc = sync_ab_buffers(h))
+		return rc;
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	h->iteration = 0;
 	h->macro_valid = h->sums_valid = false;
@@ -491,6 +514,8 @@ int lbm_set_populations(lbm_handle h, const void* host, int layout, int dtype)
 	cudaFreeAsync(dev, h->stream);
 	if (e != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "unpack failed: %s", cudaGetErrorString(e));
+	if (int rc = sync_ab_buffers(h))
+		return rc;
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	return LBM_OK;
 }
@@ -738,6 +763,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	cudaEventDestroy(e1);
 	h->iteration = it0;
 	cudaMemcpyAsync(h->g.f, backup, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
+	sync_ab_buffers(h);
 	cudaStreamSynchronize(h->stream);
 	cudaFree(backup);
 	const cudaError_t err = cudaGetLastError();
@@ -751,6 +777,40 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	h->kernel = best_kernel;
 	h->drop_graph();
 	return ensure_partials(h, h->max_step_blocks());
+}
+
+int lbm_set_streaming(lbm_handle h, int streaming)
+{
+	if (int rc = check(h))
+		return rc;
+	if (streaming != LBM_STREAMING_AA && streaming != LBM_STREAMING_AB)
+		return fail(LBM_ERR_INVALID, "unknown streaming pattern %d", streaming);
+	if (streaming == h->streaming)
+		return LBM_OK;
+	if (streaming == LBM_STREAMING_AA) {
+		for (uint8_t g : h->map_host)
+			if (!site_type_supported(g))
+				return fail(LBM_ERR_UNSUPPORTED, "the map holds site type %d, which only the A-B pattern provides", (int) g);
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+		cudaFree(h->f_out);
+		h->f_out = nullptr;
+	}
+	else {
+		LBM_CUDA(cudaMalloc(&h->f_out, h->pop_bytes));
+		LBM_CUDA(cudaMemcpyAsync(h->f_out, h->g.f, h->pop_bytes, cudaMemcpyDeviceToDevice, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+	}
+	h->streaming = streaming;
+	h->drop_graph();
+	return LBM_OK;
+}
+
+int lbm_get_streaming(lbm_handle h, int* streaming)
+{
+	if (!h || !streaming)
+		return fail(LBM_ERR_INVALID, "null argument");
+	*streaming = h->streaming;
+	return LBM_OK;
 }
 
 int lbm_set_kernel(lbm_handle h, int kernel)

@@ -19,7 +19,7 @@ import numpy as np
 from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
     COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
-    GEO, KERNEL_DIRECT, KERNEL_TILE, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
+    GEO, KERNEL_DIRECT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
     STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
 
 __all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
@@ -162,6 +162,16 @@ class LBM:
 
     def set_kernel(self, kernel):
         _abi.check(self.lib.lbm_set_kernel(self.h, int(kernel)))
+
+    def set_streaming(self, streaming):
+        """STREAMING_AA (in place, default) or STREAMING_AB (two buffers, pull)."""
+        _abi.check(self.lib.lbm_set_streaming(self.h, int(streaming)))
+
+    @property
+    def streaming(self):
+        k = ctypes.c_int(0)
+        _abi.check(self.lib.lbm_get_streaming(self.h, ctypes.byref(k)))
+        return k.value
 
     @property
     def kernel(self):

@@ -16,6 +16,7 @@ EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
 LAYOUT_INTERIOR, LAYOUT_GHOST = 0, 1
 STEP_MACRO, STEP_SUMS = 1, 2
 KERNEL_DIRECT, KERNEL_TILE = 0, 1
+STREAMING_AA, STREAMING_AB = 0, 1
 STATUS_TIMEOUT = 1
 
 # GEO site types of D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43)
@@ -83,6 +84,8 @@ SIGNATURES = {
     "lbm_get_kernel": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_status": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_version": (ctypes.c_char_p, []),
+    "lbm_set_streaming": (ctypes.c_int, [_H, ctypes.c_int]),
+    "lbm_get_streaming": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_adjoint_forward": (ctypes.c_int, [_H, _dp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
                                            ctypes.c_int32, _dp, ctypes.c_double, _dp]),
     "lbm_adjoint_backward": (ctypes.c_int, [_H, ctypes.c_double, _dp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
