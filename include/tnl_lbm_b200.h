@@ -193,6 +193,16 @@ LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
 LBM_API int lbm_set_streaming(lbm_handle h, int streaming);
 LBM_API int lbm_get_streaming(lbm_handle h, int* streaming);
 
+/* Checkpoint / resume (the reference's State::saveState / loadState through
+ * ADIOS2, include/lbm3d/state.hpp:891-1012).  One binary file: the lattice
+ * description, the iteration counter (A-A parity), the streaming pattern,
+ * the map, the inlet profiles and the population buffer as stored on the
+ * device, so a resumed run continues bit for bit.  lbm_checkpoint_load needs
+ * a handle created with the same sizes, storage, collision slot, equilibrium,
+ * periodicity and body force; it restores the viscosity. */
+LBM_API int lbm_checkpoint_save(lbm_handle h, const char* path);
+LBM_API int lbm_checkpoint_load(lbm_handle h, const char* path);
+
 /* Device status word: bit LBM_STATUS_TIMEOUT is set when a bounded wait inside
  * a kernel gave up (the kernel then stops early; the step's result is invalid). */
 #define LBM_STATUS_TIMEOUT 1

@@ -163,6 +163,14 @@ class LBM:
     def set_kernel(self, kernel):
         _abi.check(self.lib.lbm_set_kernel(self.h, int(kernel)))
 
+    def save_checkpoint(self, path):
+        """Write the state (populations as stored, map, inflow, iteration) to ``path``."""
+        _abi.check(self.lib.lbm_checkpoint_save(self.h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Resume from a checkpoint written by a lattice of the same description."""
+        _abi.check(self.lib.lbm_checkpoint_load(self.h, os.fsencode(path)))
+
     def set_streaming(self, streaming):
         """STREAMING_AA (in place, default) or STREAMING_AB (two buffers, pull)."""
         _abi.check(self.lib.lbm_set_streaming(self.h, int(streaming)))
