@@ -193,6 +193,16 @@ LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
 LBM_API int lbm_set_streaming(lbm_handle h, int streaming);
 LBM_API int lbm_get_streaming(lbm_handle h, int* streaming);
 
+/* Running velocity statistics of D3Q27_MACRO_Mean (macro.h:89-180).  While
+ * enabled, every step also outputs the macro field and updates, per site, the
+ * mean velocity m (moving average) and the co-moments S_ab of the online
+ * covariance, Cov(a, b) = S_ab / count.  lbm_set_statistics(h, 1) allocates
+ * and zeroes 9 fields of the compute type (count = 0), 0 frees them.
+ * lbm_get_statistics: out[9][Z][Y][X] = m_x, m_y, m_z, S_xx, S_yy, S_zz,
+ * S_xy, S_xz, S_yz, and the number of accumulated steps. */
+LBM_API int lbm_set_statistics(lbm_handle h, int enable);
+LBM_API int lbm_get_statistics(lbm_handle h, double* out, int64_t* count);
+
 /* Checkpoint / resume (the reference's State::saveState / loadState through
  * ADIOS2, include/lbm3d/state.hpp:891-1012).  One binary file: the lattice
  * description, the iteration counter (A-A parity), the streaming pattern,

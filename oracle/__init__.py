@@ -189,6 +189,8 @@ class Reference(_Base):
         L.ref_srt_adjoint_collision.argtypes = [ctypes.c_long, _dp, _dp, ctypes.c_double]
         L.ref_adjoint_data_term.restype = ctypes.c_int
         L.ref_adjoint_data_term.argtypes = [ctypes.c_long, _dp, _dp]
+        L.ref_mean_update.restype = ctypes.c_int
+        L.ref_mean_update.argtypes = [ctypes.c_int, ctypes.c_long, _vp, _vp, ctypes.c_int]
 
     def aa_run(self, f, geo_map, coll="CUM", eq="INV_CUM", cum_flags=None, nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
                macro=None, start_iter=0, nsteps=1, nthreads=0, return_time=False):
@@ -233,6 +235,14 @@ class Reference(_Base):
         u = np.ascontiguousarray(u, dtype=np.float64)
         self.lib.ref_srt_adjoint_collision(out.shape[0], _dptr(out), _dptr(u), nu)
         return out
+
+    def mean_update(self, macro, stats, counter):
+        """D3Q27_MACRO_Mean::outputMacro (macro.h:117-171): one update of the
+        running statistics stats [9, n] from the macro field macro [4, n]."""
+        assert macro.dtype == stats.dtype and stats.flags.c_contiguous and stats.shape[0] == 9
+        macro = np.ascontiguousarray(macro)
+        self.lib.ref_mean_update(_prec(stats.dtype), stats.shape[1], _ptr(macro), _ptr(stats), counter)
+        return stats
 
     def adjoint_data_term(self, macro):
         """D3Q27_EQ_ADJOINT::collisionWithData (eq_adjoint.h:30-33) of

@@ -514,9 +514,51 @@ const int HCX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 
 const int HCY[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1};
 const int HCZ[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1};
 
+// data view for D3Q27_MACRO_Mean::outputMacro: 13 macro fields of n sites,
+// field-major, and the statistics counter (lbm_data.h:24)
+template <typename DREAL>
+struct MeanData
+{
+	DREAL* m;
+	long n;
+	int stat_counter;
+	DREAL& macro(int id, long x, long, long)
+	{
+		return m[id * n + x];
+	}
+};
+
+template <typename DREAL>
+int mean_update_typed(long n, const DREAL* macro4, DREAL* stats9, int counter)
+{
+	std::vector<DREAL> all((size_t) 13 * n);
+	std::memcpy(all.data() + 4 * n, stats9, sizeof(DREAL) * 9 * n);
+	MeanData<DREAL> SD{all.data(), n, counter};
+	for (long i = 0; i < n; i++) {
+		D3Q27_KernelStruct<DREAL> KS;
+		KS.rho = macro4[i];
+		KS.vx = macro4[n + i];
+		KS.vy = macro4[2 * n + i];
+		KS.vz = macro4[3 * n + i];
+		D3Q27_MACRO_Mean<HarnessTraits<DREAL>>::outputMacro(SD, KS, i, 0, 0);
+	}
+	std::memcpy(stats9, all.data() + 4 * n, sizeof(DREAL) * 9 * n);
+	return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+// One statistics update of D3Q27_MACRO_Mean::outputMacro (macro.h:117-171) on
+// n sites: macro4 [4][n] (rho, vx, vy, vz) of the step, stats9 [9][n] (mean
+// velocity, co-moments) updated in place, counter = SD.stat_counter.
+int ref_mean_update(int prec, long n, const void* macro4, void* stats9, int counter)
+{
+	if (prec == 0)
+		return mean_update_typed<double>(n, (const double*) macro4, (double*) stats9, counter);
+	return mean_update_typed<float>(n, (const float*) macro4, (float*) stats9, counter);
+}
 
 // The reference's adjoint SRT collision (col_srt_adjoint.h:50-109) on n
 // independent sites: fstar[n][27] updated in place, primary velocity u[n][3].

@@ -47,6 +47,8 @@ struct lbm_lattice
 	int streaming = LBM_STREAMING_AA;
 	void* f_out = nullptr;		// A-B: the write buffer (swapped with g.f after every step)
 	void* graph_in = nullptr;	// g.f when the graph was captured
+	void* stats = nullptr;		// D3Q27_MACRO_Mean fields [9][sites], compute type
+	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
 	static constexpr int GRAPH_STEPS = 16;
 

@@ -128,4 +128,8 @@ cudaError_t finish_sums(const double* partials, long long nblocks, double* stage
 cudaError_t enstrophy_partials(const void* macro, int compute_size, int X, int Y, int Z, double* partials, long long* nblocks,
 							   cudaStream_t);
 
+// running velocity statistics of D3Q27_MACRO_Mean from the macro field of one
+// step: stats [9][n] in the compute type (lbm_stats.cu)
+cudaError_t stats_update(const void* macro, void* stats, int compute_size, long long n, int counter, cudaStream_t);
+
 }  // namespace lbm

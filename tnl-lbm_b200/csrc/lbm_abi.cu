@@ -343,6 +343,7 @@ int lbm_destroy(lbm_handle h)
 	lbm::adjoint_free(h->adjoint);
 	cudaFree(h->g.f);
 	cudaFree(h->f_out);
+	cudaFree(h->stats);
 	cudaFree(h->map);
 	for (auto* p : h->inflow)
 		cudaFree(p);
@@ -552,6 +553,34 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 		return LBM_OK;
 	const bool macro = (flags & LBM_STEP_MACRO) != 0;
 	const bool sums = (flags & LBM_STEP_SUMS) != 0;
+	if (h->stats) {
+		// D3Q27_MACRO_Mean computes in every iteration (macro.h:113): every step
+		// outputs the macro field and updates the statistics
+		int rc = ensure_macro(h);
+		if (rc || (sums && (rc = ensure_partials(h, h->max_step_blocks()))))
+			return rc;
+		for (int64_t i = 0; i < nsteps; i++) {
+			const bool last_sums = sums && i == nsteps - 1;
+			if ((rc = launch_step(h, true, last_sums)))
+				return rc;
+			const cudaError_t e =
+				lbm::stats_update(h->macro, h->stats, h->ops->compute_size, h->sites(), (int) h->stats_count, h->stream);
+			if (e != cudaSuccess)
+				return fail(LBM_ERR_CUDA, "statistics update failed: %s", cudaGetErrorString(e));
+			h->stats_count++;
+		}
+		if (sums) {
+			const long long nb = h->last_blocks;
+			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->sums_dev, h->stream);
+			if (e != cudaSuccess)
+				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
+			LBM_CUDA(cudaMemcpyAsync(h->sums_host, h->sums_dev, lbm::NRED_HOST * sizeof(double), cudaMemcpyDeviceToHost,
+									 h->stream));
+		}
+		h->macro_valid = true;
+		h->sums_valid = sums;
+		return LBM_OK;
+	}
 	int rc = run_plain_steps(h, nsteps - ((macro || sums) ? 1 : 0));
 	if (rc)
 		return rc;
@@ -777,6 +806,48 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	h->kernel = best_kernel;
 	h->drop_graph();
 	return ensure_partials(h, h->max_step_blocks());
+}
+
+int lbm_set_statistics(lbm_handle h, int enable)
+{
+	if (int rc = check(h))
+		return rc;
+	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	cudaFree(h->stats);
+	h->stats = nullptr;
+	h->stats_count = 0;
+	if (enable) {
+		const size_t bytes = (size_t) 9 * h->sites() * h->ops->compute_size;
+		LBM_CUDA(cudaMalloc(&h->stats, bytes));
+		LBM_CUDA(cudaMemsetAsync(h->stats, 0, bytes, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+	}
+	return LBM_OK;
+}
+
+int lbm_get_statistics(lbm_handle h, double* out, int64_t* count)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!h->stats)
+		return fail(LBM_ERR_INVALID, "statistics are not enabled (lbm_set_statistics)");
+	if (!out || !count)
+		return fail(LBM_ERR_INVALID, "null output");
+	const size_t n = (size_t) 9 * h->sites();
+	const int cs = h->ops->compute_size;
+	if (cs == 8) {
+		LBM_CUDA(cudaMemcpyAsync(out, h->stats, n * 8, cudaMemcpyDeviceToHost, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+	}
+	else {
+		std::vector<float> tmp(n);
+		LBM_CUDA(cudaMemcpyAsync(tmp.data(), h->stats, n * 4, cudaMemcpyDeviceToHost, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+		for (size_t i = 0; i < n; i++)
+			out[i] = tmp[i];
+	}
+	*count = h->stats_count;
+	return LBM_OK;
 }
 
 int lbm_set_streaming(lbm_handle h, int streaming)

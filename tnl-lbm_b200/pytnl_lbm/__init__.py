@@ -163,6 +163,18 @@ class LBM:
     def set_kernel(self, kernel):
         _abi.check(self.lib.lbm_set_kernel(self.h, int(kernel)))
 
+    def set_statistics(self, enable=True):
+        """Running velocity mean and covariance of D3Q27_MACRO_Mean, updated every step."""
+        _abi.check(self.lib.lbm_set_statistics(self.h, 1 if enable else 0))
+
+    def statistics(self):
+        """(mean [3, Z, Y, X], covariance [6, Z, Y, X] in the order xx, yy, zz, xy, xz, yz, count)."""
+        out = np.empty((9,) + self.shape, np.float64)
+        n = ctypes.c_int64(0)
+        _abi.check(self.lib.lbm_get_statistics(self.h, _abi.dptr(out), ctypes.byref(n)))
+        cov = out[3:] / max(n.value, 1)
+        return out[:3], cov, n.value
+
     def save_checkpoint(self, path):
         """Write the state (populations as stored, map, inflow, iteration) to ``path``."""
         _abi.check(self.lib.lbm_checkpoint_save(self.h, os.fsencode(path)))

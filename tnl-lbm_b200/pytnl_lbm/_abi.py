@@ -84,6 +84,8 @@ SIGNATURES = {
     "lbm_get_kernel": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_status": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "lbm_version": (ctypes.c_char_p, []),
+    "lbm_set_statistics": (ctypes.c_int, [_H, ctypes.c_int]),
+    "lbm_get_statistics": (ctypes.c_int, [_H, _dp, ctypes.POINTER(ctypes.c_int64)]),
     "lbm_checkpoint_save": (ctypes.c_int, [_H, ctypes.c_char_p]),
     "lbm_checkpoint_load": (ctypes.c_int, [_H, ctypes.c_char_p]),
     "lbm_set_streaming": (ctypes.c_int, [_H, ctypes.c_int]),
