@@ -50,6 +50,11 @@ def workload_spec(name):
         return dict(workload="ensemble of 64 periodic Taylor-Green lattices, edges U{32,48,64,96,128} (seeded, "
                              "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
                     X=0, Y=0, Z=0, kind="ensemble", cum_flags=3)
+    if name == "adjoint":
+        return dict(workload="discrete adjoint: channel 256x64x64, SRT, velocity inlet u_max=0.03, per-cell x-force control "
+                             "(Gaussian bumps, amplitude 1e-3), L2 velocity mismatch on 8 cross-sections, 4000 steps, "
+                             "sqrt(N) checkpoints, FP32 storage, FP64 gradient accumulation",
+                    X=256, Y=64, Z=64, kind="adjoint", cum_flags=0)
     if name == "tgv64":
         return dict(workload="periodic Taylor-Green vortex 64^3, U0=0.05, Re=1600", X=64, Y=64, Z=64, kind="tgv",
                     cum_flags=3)
@@ -373,7 +378,79 @@ def time_steps(pl, lat, steps, warmup, stream):
     return e0.elapsed_time(e1) / 1e3
 
 
+def run_adjoint(args):
+    """Forward pass with checkpoints plus backward pass of the discrete adjoint;
+    value = sites x steps / (forward + backward device time)."""
+    import torch
+    import pytnl_lbm as pl
+    from pytnl_lbm import adjoint_check as ac
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, local, "nccl")
+    device = torch.device("cuda", local)
+    spec = workload_spec(args.workload)
+    steps = args.steps + (args.steps % 2)
+    lat, m = ac.make(pl.STORE_F32)
+    samples = ac.sample_sites(m)
+    target = np.zeros((len(samples), 4))
+    target[:, 0] = 1.0
+    target[:, 1] = 0.01
+    F = ac.bumps(seed=7)
+    stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
+    ac.run(lat, F, min(steps, 64), samples, target)  # warm-up: kernels, allocations
+    lat.adjoint_backward()
+    every = int(math.ceil(math.sqrt(steps)))
+    with ClockSampler(local) as clk:
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        lat.init_equilibrium()
+        e0.record(stream)
+        J = lat.adjoint_forward(F, steps, samples, target, checkpoint_every=every)
+        e1.record(stream)
+        g = lat.adjoint_backward()
+        e2.record(stream)
+        e2.synchronize()
+    t_fwd, t_bwd = e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
+    secs = max_over_ranks(dist, t_fwd + t_bwd, device)
+    sites = spec["X"] * spec["Y"] * spec["Z"]
+    value = sites * steps * world / secs / 1e6
+    v = lat.device_view()
+    pop_bytes = 27 * v.sq * v.elem_size
+    lat.close()
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": steps,
+            "warmup": 1, "ms_per_step": round(secs / steps * 1e3, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (gradient f64)",
+            "data": "synthetic (seeded control field and target)",
+            "config": {"workload": spec["workload"], "lattice": [spec["X"], spec["Y"], spec["Z"]],
+                       "samples": int(len(samples)), "checkpoint_every": every,
+                       "checkpoint_memory_gb": round((math.ceil(steps / every) + every + 2) * pop_bytes / 1e9, 2)},
+            "gpu_launches": 3 * steps,
+            "forward_s": round(t_fwd, 4), "backward_s": round(t_bwd, 4), "objective": J,
+            "grad_max_abs": float(np.max(np.abs(g[0]))),
+            "roofline": {"bound": "hbm", "achieved": None, "peak": read_peaks()[0], "unit": "GB/s", "frac": None,
+                         "traffic": None,
+                         "note": "per step: two primal A-A steps (216 B/site each) and one adjoint step "
+                                 "(27 primal reads + 27 adjoint reads + 27 adjoint writes, 324 B/site), "
+                                 "plus a 27-value copy per recomputed state"},
+            "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "per_run": "lbm_adjoint_forward + lbm_adjoint_backward through the C-ABI"},
+            "clocks": clk.summary(),
+        }
+        bytes_per_site_step = 2 * 216 + 324 + 2 * 108
+        line["roofline"]["achieved"] = round(bytes_per_site_step * sites * steps / secs / 1e9, 1)
+        line["roofline"]["frac"] = round(line["roofline"]["achieved"] / line["roofline"]["peak"], 4)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+
+
 def run_ours(args):
+    if workload_spec(args.workload)["kind"] == "adjoint":
+        return run_adjoint(args)
     if workload_spec(args.workload)["kind"] == "ensemble":
         return run_ensemble(args)
     import torch
@@ -563,6 +640,10 @@ def run_reference(args):
         return
     if spec["kind"] == "ensemble":
         return run_reference_ensemble(args, spec, oracle, cores)
+    if spec["kind"] == "adjoint":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no time-dependent adjoint of this "
+                          "workload (sim_adjoint solves a steady adjoint about a frozen flow)"}))
+        return
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
@@ -605,7 +686,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64"])
+    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64", "adjoint"])
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
