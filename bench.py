@@ -89,6 +89,17 @@ def run_ensemble(args):
           "bf16s": pl.STORE_BF16S}[args.storage]
     ens = pl.Ensemble(sizes, nus, cum_flags=3, storage=st, device=local)
     ens.init_taylor_green(0.05)
+    # every launch shape, timed over 256 steps, then the autotuner's choice
+    shapes = {}
+    for tile, gp in ((128, 0), (256, 0), (128, 1), (128, 2)):
+        ens.set_shape(tile, gp)
+        ens.step(16)
+        ens.synchronize()
+        s0 = time.perf_counter()
+        ens.step(256)
+        ens.synchronize()
+        shapes[f"{tile}/{gp}"] = round(sites * 256 / (time.perf_counter() - s0) / 1e6, 1)
+    ens.init_taylor_green(0.05)
     shape = ens.autotune(3)
     ens.init_taylor_green(0.05)
     stream = torch.cuda.ExternalStream(ens.stream, device=device)
@@ -156,7 +167,9 @@ def run_ensemble(args):
             "config": {"workload": spec["workload"], "members": len(sizes), "sites": sites,
                        "storage": args.storage, "parallelism": f"replicas x{world}",
                        "launch": {"tile_sites": shape[0],
-                                  "grid": "persistent" if shape[1] == 0 else "one block per tile", "autotuned": True},
+                                  "grid": ["persistent", "one block per tile",
+                                           "per-member launches in concurrent graph branches"][shape[1]],
+                                  "autotuned": True},
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (27 * bpe * sites / 1e9)},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -167,6 +180,7 @@ def run_ensemble(args):
             "e2e": {"value": round(sites * e2e_steps * world / e2e_secs / 1e6, 2), "unit": "MLUPS",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 6 * 8 * len(sizes), "steps": e2e_steps,
                     "per_step": "lbm_ensemble_step(1, LBM_STEP_SUMS) + lbm_ensemble_get_sums"},
+            "shapes_mlups": shapes,
             "sequential": {"value": round(seq_value, 2), "unit": "MLUPS", "speedup": round(value / seq_value, 3),
                            "kinetic_energy_max_rel_diff": ke_diff,
                            "how": "the same 64 members as single periodic lattices (lbm_create), one after the "

@@ -294,7 +294,10 @@ LBM_API int64_t lbm_ensemble_iteration(lbm_ensemble e);
 LBM_API int lbm_ensemble_get_stream(lbm_ensemble e, void** stream);
 LBM_API int lbm_ensemble_synchronize(lbm_ensemble e);
 /* Launch shape: sites per tile (= threads per block) 128 or 256, and grid
- * 0 (persistent: resident blocks per SM x SMs) or 1 (one block per tile). */
+ * 0 (persistent: resident blocks per SM x SMs), 1 (one block per tile), or
+ * 2 (every member runs the single-lattice kernel on one of up to 64 streams,
+ * the members being independent branches of the captured graph; steps with
+ * LBM_STEP_SUMS use the persistent kernel). */
 LBM_API int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy);
 LBM_API int lbm_ensemble_get_shape(lbm_ensemble e, int* tile_sites, int* grid_policy);
 /* Times every launch shape on the current state (restored afterwards) and

@@ -67,7 +67,7 @@ def test_members_equal_single_lattices(pl, storage, coll, flags, eq, steps):
     ens.close()
 
 
-@pytest.mark.parametrize("tile_sites,grid_policy", [(128, 0), (128, 1), (256, 0), (256, 1)])
+@pytest.mark.parametrize("tile_sites,grid_policy", [(128, 0), (128, 1), (256, 0), (256, 1), (128, 2)])
 def test_launch_shapes_give_identical_results(pl, port, tile_sites, grid_policy):
     rng = np.random.default_rng(5)
     ens = pl.Ensemble(SIZES, NUS, cum_flags=3, storage=pl.STORE_F32)
@@ -77,8 +77,9 @@ def test_launch_shapes_give_identical_results(pl, port, tile_sites, grid_policy)
     ens.set_shape(tile_sites, grid_policy)
     assert ens.shape() == (tile_sites, grid_policy)
     ens.step(21)
+    ens.step(20)  # graph replays (16-step graphs) after an odd start
     for m, (size, nu) in enumerate(zip(SIZES, NUS)):
-        f_single, _ = single_run(pl, size, nu, pl.STORE_F32, pl.COLL_CUM, 3, pl.EQ_INV_CUM, 21,
+        f_single, _ = single_run(pl, size, nu, pl.STORE_F32, pl.COLL_CUM, 3, pl.EQ_INV_CUM, 41,
                                  f0=states[m].astype(np.float32))
         assert rel_linf(ens.get_populations(m), f_single) <= TOL["F32"], f"member {m}"
     ens.close()
@@ -118,7 +119,7 @@ def test_autotune_restores_state_and_picks_a_shape(pl):
     ens.step(3)
     before = [ens.get_populations(m) for m in range(len(SIZES))]
     shape = ens.autotune(2)
-    assert shape[0] in (128, 256) and shape[1] in (0, 1)
+    assert shape[0] in (128, 256) and shape[1] in (0, 1, 2)
     assert ens.iteration == 3
     for m in range(len(SIZES)):
         assert np.array_equal(ens.get_populations(m), before[m])

@@ -101,6 +101,11 @@ struct lbm_ensemble_t
 	bool sums_valid = false;
 	long long iteration = 0;
 	cudaGraphExec_t graph = nullptr;
+	// grid policy 2: one stream per lane, members round-robin over the lanes
+	std::vector<cudaStream_t> lanes;
+	std::vector<cudaEvent_t> joins;
+	cudaEvent_t fork = nullptr;
+	static constexpr int MAX_LANES = 64;
 
 	void drop_graph()
 	{
@@ -166,8 +171,68 @@ int build_tiles(lbm_ensemble e)
 	return LBM_OK;
 }
 
+int ensure_lanes(lbm_ensemble e)
+{
+	if (!e->lanes.empty())
+		return LBM_OK;
+	const int n = e->count < lbm_ensemble_t::MAX_LANES ? e->count : lbm_ensemble_t::MAX_LANES;
+	ENS_CUDA(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+	for (int i = 0; i < n; i++) {
+		cudaStream_t st = nullptr;
+		cudaEvent_t ev = nullptr;
+		ENS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		e->lanes.push_back(st);
+		ENS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+		e->joins.push_back(ev);
+	}
+	return LBM_OK;
+}
+
+// grid policy 2: every member runs the single-lattice direct kernel on its
+// lane; the lanes fork from and join into the ensemble's stream, so under
+// graph capture the members become independent branches
+int ens_launch_members(lbm_ensemble e)
+{
+	if (int rc = ensure_lanes(e))
+		return rc;
+	const int nl = (int) e->lanes.size();
+	ENS_CUDA(cudaEventRecord(e->fork, e->stream));
+	for (int i = 0; i < nl; i++)
+		ENS_CUDA(cudaStreamWaitEvent(e->lanes[i], e->fork, 0));
+	for (int m = 0; m < e->count; m++) {
+		const lbm::Geometry& g = e->g[m];
+		lbm::StepLaunch L{};
+		L.g = g;
+		L.p = e->p[m];
+		L.coll = e->collision;
+		L.cum_flags = e->cum_flags;
+		L.odd = (e->iteration % 2) != 0;
+		const int bx = g.X >= 128 ? 128 : ((g.X + 31) / 32) * 32;
+		L.block = dim3(bx, 128 / bx, 1);
+		L.grid = dim3((g.X + bx - 1) / bx, (g.Y + L.block.y - 1) / L.block.y, g.Z);
+		L.stream = e->lanes[m % nl];
+		L.kernel = lbm::KERNEL_DIRECT;
+		const cudaError_t err = e->ops->step(L);
+		if (err != cudaSuccess)
+			return efail(LBM_ERR_CUDA, "member %d step launch failed: %s", m, cudaGetErrorString(err));
+	}
+	for (int i = 0; i < nl; i++) {
+		ENS_CUDA(cudaEventRecord(e->joins[i], e->lanes[i]));
+		ENS_CUDA(cudaStreamWaitEvent(e->stream, e->joins[i], 0));
+	}
+	return LBM_OK;
+}
+
 int ens_launch(lbm_ensemble e, bool sums, bool dry_run = false)
 {
+	if (e->grid_policy == 2 && !sums) {
+		if (dry_run)
+			return LBM_OK;
+		if (int rc = ens_launch_members(e))
+			return rc;
+		e->iteration++;
+		return LBM_OK;
+	}
 	lbm::EnsLaunch L{};
 	L.members = e->members_dev;
 	L.tile_member = e->tile_member_dev;
@@ -323,6 +388,10 @@ int lbm_ensemble_create(const lbm_ensemble_desc* d, lbm_ensemble* out)
 	size_t total = 0;
 	for (int m = 0; m < e->count; m++) {
 		e->g[m] = lbm::make_geometry(d->X[m], d->Y[m], d->Z[m], es);
+		if (e->g[m].sq > lbm::MAX_SLAB_ELEMENTS) {
+			delete e;
+			return efail(LBM_ERR_SIZE, "member %d needs more than 2^31 - 1 elements per direction", m);
+		}
 		offset[m] = total;
 		total += ((size_t) 27 * e->g[m].sq * es + 255) / 256 * 256;
 		lbm::CollParamsD& p = e->p[m];
@@ -366,6 +435,12 @@ int lbm_ensemble_destroy(lbm_ensemble e)
 	cudaFree(e->pops);
 	cudaFree(e->sums_dev);
 	cudaFreeHost(e->sums_host);
+	for (cudaStream_t st : e->lanes)
+		cudaStreamDestroy(st);
+	for (cudaEvent_t ev : e->joins)
+		cudaEventDestroy(ev);
+	if (e->fork)
+		cudaEventDestroy(e->fork);
 	if (e->stream)
 		cudaStreamDestroy(e->stream);
 	delete e;
@@ -506,8 +581,8 @@ int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy)
 {
 	if (int rc = echeck(e))
 		return rc;
-	if ((tile_sites != 128 && tile_sites != 256) || (grid_policy != 0 && grid_policy != 1))
-		return efail(LBM_ERR_INVALID, "launch shape: tile_sites 128 or 256, grid_policy 0 or 1");
+	if ((tile_sites != 128 && tile_sites != 256) || grid_policy < 0 || grid_policy > 2)
+		return efail(LBM_ERR_INVALID, "launch shape: tile_sites 128 or 256, grid_policy 0, 1 or 2");
 	if (tile_sites != e->tile_sites) {
 		ENS_CUDA(cudaStreamSynchronize(e->stream));
 		e->tile_sites = tile_sites;
@@ -545,16 +620,20 @@ int lbm_ensemble_autotune(lbm_ensemble e, int ntrials)
 	float best = 1e30f;
 	int best_tile = e->tile_sites, best_grid = e->grid_policy;
 	int rc = LBM_OK;
+	// every candidate timed the way plain steps run: graph replays when graphs
+	// are on (the first replay builds and warms the graph)
+	const long long chunk = e->use_graphs ? lbm_ensemble_t::GRAPH_STEPS : 2;
 	for (int tile : {128, 256}) {
-		for (int gp : {0, 1}) {
+		for (int gp : {0, 1, 2}) {
+			if (gp == 2 && tile != 128)
+				continue;  // the tile size does not apply to per-member launches
 			if ((rc = lbm_ensemble_set_shape(e, tile, gp)))
 				break;
-			e->iteration = it0 + (it0 % 2);	 // timed pairs start at an even step
-			for (int s = 0; s < 2 && rc == LBM_OK; s++)
-				rc = ens_launch(e, false);
+			e->iteration = it0 + (it0 % 2);	 // timed steps start at an even step
+			rc = ens_plain_steps(e, chunk);
 			cudaEventRecord(e0, e->stream);
-			for (int s = 0; s < 2 * ntrials && rc == LBM_OK; s++)
-				rc = ens_launch(e, false);
+			if (rc == LBM_OK)
+				rc = ens_plain_steps(e, chunk * ntrials);
 			cudaEventRecord(e1, e->stream);
 			cudaEventSynchronize(e1);
 			float ms = 0;
