@@ -50,6 +50,10 @@ def workload_spec(name):
         return dict(workload="ensemble of 64 periodic Taylor-Green lattices, edges U{32,48,64,96,128} (seeded, "
                              "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
                     X=0, Y=0, Z=0, kind="ensemble", cum_flags=3)
+    if name == "ensemble_small":
+        return dict(workload="ensemble of 512 small periodic Taylor-Green lattices, edges U{16,24,32} (seeded, "
+                             "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
+                    X=0, Y=0, Z=0, kind="ensemble", cum_flags=3, count=512, edges=(16, 24, 32))
     if name == "adjoint":
         return dict(workload="discrete adjoint: channel 256x64x64, SRT, velocity inlet u_max=0.03, per-cell x-force control "
                              "(Gaussian bumps, amplitude 1e-3), L2 velocity mismatch on 8 cross-sections, 4000 steps, "
@@ -61,12 +65,12 @@ def workload_spec(name):
     raise SystemExit(f"unknown workload {name}")
 
 
-def ensemble_setup(count=64, seed=4321, u0=0.05):
-    """Member sizes and viscosities of the ensemble workload: each edge drawn
-    from {32, 48, 64, 96, 128}, Re log-uniform in [100, 3200] on the x box
-    length, nu = u0 (X / 2 pi) / Re."""
+def ensemble_setup(count=64, seed=4321, u0=0.05, edges=(32, 48, 64, 96, 128)):
+    """Member sizes and viscosities of an ensemble workload: each edge drawn
+    from `edges`, Re log-uniform in [100, 3200] on the x box length,
+    nu = u0 (X / 2 pi) / Re."""
     rng = np.random.default_rng(seed)
-    edges = np.array([32, 48, 64, 96, 128])
+    edges = np.array(edges)
     sizes = [tuple(int(v) for v in rng.choice(edges, 3)) for _ in range(count)]
     re = np.exp(rng.uniform(math.log(100.0), math.log(3200.0), count))
     nus = [u0 * (sz[0] / (2 * math.pi)) / r for sz, r in zip(sizes, re)]
@@ -83,7 +87,7 @@ def run_ensemble(args):
     dist = init_dist(world, local, "nccl")
     device = torch.device("cuda", local)
     spec = workload_spec(args.workload)
-    sizes, nus = ensemble_setup()
+    sizes, nus = ensemble_setup(spec["count"], edges=spec["edges"])
     sites = sum(x * y * z for x, y, z in sizes)
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S}[args.storage]
@@ -183,7 +187,7 @@ def run_ensemble(args):
             "shapes_mlups": shapes,
             "sequential": {"value": round(seq_value, 2), "unit": "MLUPS", "speedup": round(value / seq_value, 3),
                            "kinetic_energy_max_rel_diff": ke_diff,
-                           "how": "the same 64 members as single periodic lattices (lbm_create), one after the "
+                           "how": f"the same {len(sizes)} members as single periodic lattices (lbm_create), one after the "
                                   "other, each replayed from its CUDA graphs; summed device time"},
             "clocks": clk.summary(),
         }
@@ -197,7 +201,7 @@ def run_ensemble(args):
 def run_reference_ensemble(args, spec, oracle, cores):
     """The reference's per-site code on each ensemble member in turn (the
     reference runs one lattice per solver instance), on all host cores."""
-    sizes, nus = ensemble_setup()
+    sizes, nus = ensemble_setup(spec["count"], edges=spec["edges"])
     prec = np.float64 if args.storage == "f64" else np.float32
     impl = oracle.Reference(3, fast=True)
     total_sites = sum(x * y * z for x, y, z in sizes)
@@ -700,7 +704,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64", "adjoint"])
+    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64", "ensemble_small", "adjoint"])
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -63,13 +63,10 @@ struct StepArgs
 };
 
 // Offsets (in elements) of the neighbour sites; periodic sites wrap, all
-// other sites reach into the ghost layer (kernels.h:21-37).  Index arithmetic
-// within one direction's slab is 32-bit: a slab holds fewer than 2^31
-// elements (checked when a lattice is created), so only the direction's base
-// pointer is 64-bit.
+// other sites reach into the ghost layer (kernels.h:21-37).
 struct Offsets
 {
-	int x[3], y[3], z[3];
+	long long x[3], y[3], z[3];
 };
 
 __device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, int z, int X, int Y, int Z, int sy, int sz)
@@ -78,24 +75,18 @@ __device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, in
 	o.x[0] = (wrap && x == 0) ? (X - 1) : -1;
 	o.x[1] = 0;
 	o.x[2] = (wrap && x == X - 1) ? -(X - 1) : 1;
-	o.y[0] = ((wrap && y == 0) ? (Y - 1) : -1) * sy;
+	o.y[0] = (long long) ((wrap && y == 0) ? (Y - 1) : -1) * sy;
 	o.y[1] = 0;
-	o.y[2] = ((wrap && y == Y - 1) ? -(Y - 1) : 1) * sy;
-	o.z[0] = ((wrap && z == 0) ? (Z - 1) : -1) * sz;
+	o.y[2] = (long long) ((wrap && y == Y - 1) ? -(Y - 1) : 1) * sy;
+	o.z[0] = (long long) ((wrap && z == 0) ? (Z - 1) : -1) * sz;
 	o.z[1] = 0;
-	o.z[2] = ((wrap && z == Z - 1) ? -(Z - 1) : 1) * sz;
+	o.z[2] = (long long) ((wrap && z == Z - 1) ? -(Z - 1) : 1) * sz;
 	return o;
-}
-
-// index of interior site (x, y, z) within one direction's slab
-__device__ __forceinline__ int site_index(int x, int y, int z, int sy, int sz, int x0)
-{
-	return (z + 1) * sz + (y + 1) * sy + x0 + x;
 }
 
 // A-A read of the 27 populations (streaming_AA.h:79-116)
 template <typename S, bool ODD>
-__device__ __forceinline__ void aa_read(const typename S::T* __restrict__ f, long long sq, int base, const Offsets& o,
+__device__ __forceinline__ void aa_read(const typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
 										typename S::R* v)
 {
 	static_for<27>(
@@ -103,7 +94,7 @@ __device__ __forceinline__ void aa_read(const typename S::T* __restrict__ f, lon
 		{
 			constexpr int q = decltype(Qc)::value;
 			if constexpr (ODD)
-				v[q] = S::template load<opp(q)>(f + opp(q) * sq + (base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]));
+				v[q] = S::template load<opp(q)>(f + opp(q) * sq + base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]);
 			else
 				v[q] = S::template load<q>(f + q * sq + base);
 		}
@@ -112,7 +103,7 @@ __device__ __forceinline__ void aa_read(const typename S::T* __restrict__ f, lon
 
 // A-A write of the 27 populations (streaming_AA.h:12-76)
 template <typename S, bool ODD>
-__device__ __forceinline__ void aa_write(typename S::T* __restrict__ f, long long sq, int base, const Offsets& o,
+__device__ __forceinline__ void aa_write(typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
 										 const typename S::R* v)
 {
 	static_for<27>(
@@ -120,7 +111,7 @@ __device__ __forceinline__ void aa_write(typename S::T* __restrict__ f, long lon
 		{
 			constexpr int q = decltype(Qc)::value;
 			if constexpr (ODD)
-				S::template store<q>(f + q * sq + (base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)]), v[q]);
+				S::template store<q>(f + q * sq + base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)], v[q]);
 			else
 				S::template store<opp(q)>(f + opp(q) * sq + base, v[q]);
 		}
@@ -307,7 +298,7 @@ __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typen
 
 	double red[NRED] = {0, 0, 0, 0, 0, 0};
 	if (active) {
-		const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		const long long site = ((long long) z * a.Y + y) * a.X + x;
 		uint8_t geo = GEO_PERIODIC;
 		if constexpr (GENERAL)

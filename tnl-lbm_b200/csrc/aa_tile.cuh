@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 		if (!active)
 			continue;
 
-		const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		const long long sidx = ((long long) z * a.Y + y) * a.X + x;
 		const bool wrap = !GENERAL || geo == GEO_PERIODIC;
 		const Offsets o = neighbour_offsets(wrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);

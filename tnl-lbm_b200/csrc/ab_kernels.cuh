@@ -27,12 +27,12 @@ __device__ __forceinline__ Offsets ab_offsets(uint8_t geo, int x, int y, int z, 
 	o.x[0] = x == 0 ? 0 : -1;
 	o.x[1] = 0;
 	o.x[2] = x == X - 1 ? 0 : 1;
-	o.y[0] = y == 0 ? 0 : -sy;
+	o.y[0] = y == 0 ? 0 : -(long long) sy;
 	o.y[1] = 0;
-	o.y[2] = y == Y - 1 ? 0 : sy;
-	o.z[0] = z == 0 ? 0 : -sz;
+	o.y[2] = y == Y - 1 ? 0 : (long long) sy;
+	o.z[0] = z == 0 ? 0 : -(long long) sz;
 	o.z[1] = 0;
-	o.z[2] = z == Z - 1 ? 0 : sz;
+	o.z[2] = z == Z - 1 ? 0 : (long long) sz;
 	if (geo == GEO_OUTFLOW_RIGHT)  // pull from x - 1 in every direction (bc.h:73-74)
 		o.x[1] = o.x[2] = o.x[0];
 	return o;
@@ -40,14 +40,14 @@ __device__ __forceinline__ Offsets ab_offsets(uint8_t geo, int x, int y, int z, 
 
 // pull streaming (streaming_AB.h:22-49)
 template <typename S>
-__device__ __forceinline__ void ab_read(const typename S::T* __restrict__ f, long long sq, int base, const Offsets& o,
+__device__ __forceinline__ void ab_read(const typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
 										typename S::R* v)
 {
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			v[q] = S::template load<q>(f + q * sq + (base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]));
+			v[q] = S::template load<q>(f + q * sq + base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]);
 		}
 	);
 }
@@ -56,7 +56,7 @@ __device__ __forceinline__ void ab_read(const typename S::T* __restrict__ f, lon
 // directions that leave through x = X-1 backwards (c_x = -1) are taken as a
 // blend of sites x - 1 and x weighted by the lattice speed of sound
 template <typename S>
-__device__ __forceinline__ void ab_read_interp(const typename S::T* __restrict__ f, long long sq, int base,
+__device__ __forceinline__ void ab_read_interp(const typename S::T* __restrict__ f, long long sq, long long base,
 											   const Offsets& o, typename S::R* v)
 {
 	using R = typename S::R;
@@ -65,7 +65,7 @@ __device__ __forceinline__ void ab_read_interp(const typename S::T* __restrict__
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			const typename S::T* p = f + q * sq + (base + o.y[1 - cy(q)] + o.z[1 - cz(q)]);
+			const typename S::T* p = f + q * sq + base + o.y[1 - cy(q)] + o.z[1 - cz(q)];
 			if constexpr (cx(q) == -1)
 				v[q] = cs * S::template load<q>(p + o.x[0]) + (R(1) - cs) * S::template load<q>(p);
 			else
@@ -77,7 +77,7 @@ __device__ __forceinline__ void ab_read_interp(const typename S::T* __restrict__
 // pre-collision part of the A-B step for one site (bc.h:60-403); returns
 // whether the site collides (bc.h:406-412)
 template <typename S, typename R, typename T>
-__device__ __forceinline__ bool ab_boundary(Site<R>& s, uint8_t geo, const StepArgs<T, R>& a, int base, int z, int y)
+__device__ __forceinline__ bool ab_boundary(Site<R>& s, uint8_t geo, const StepArgs<T, R>& a, long long base, int z, int y)
 {
 	switch (geo) {
 		case GEO_INFLOW_BB_LEFT: {
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(128, MINB)
 	const bool active = x < a.X && y < a.Y;
 	double red[NRED] = {0, 0, 0, 0, 0, 0};
 	if (active) {
-		const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		const long long site = ((long long) z * a.Y + y) * a.X + x;
 		const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
 		Site<R> s;

@@ -50,18 +50,18 @@ struct AdjArgs
 // location of the value that direction q of a site reads (R_q) or writes
 // (W_q) in the A-A step of the given parity
 template <bool ODD, int q>
-__device__ __forceinline__ long long aa_read_loc(long long sq, int base, const Offsets& o)
+__device__ __forceinline__ long long aa_read_loc(long long sq, long long base, const Offsets& o)
 {
 	if constexpr (ODD)
-		return opp(q) * sq + (base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)]);
+		return opp(q) * sq + base + o.x[1 - cx(q)] + o.y[1 - cy(q)] + o.z[1 - cz(q)];
 	else
 		return q * sq + base;
 }
 template <bool ODD, int q>
-__device__ __forceinline__ long long aa_write_loc(long long sq, int base, const Offsets& o)
+__device__ __forceinline__ long long aa_write_loc(long long sq, long long base, const Offsets& o)
 {
 	if constexpr (ODD)
-		return q * sq + (base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)]);
+		return q * sq + base + o.x[1 + cx(q)] + o.y[1 + cy(q)] + o.z[1 + cz(q)];
 	else
 		return opp(q) * sq + base;
 }
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(128) adj_primal_kernel(const AdjArgs<typename 
 	sa.in_vy = a.in_vy;
 	sa.in_vz = a.in_vz;
 	sa.p = site_params(a, site, nsites);
-	const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 	Site<R> s;
 	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 	if (geo == GEO_NOTHING)
 		return;
 	const CollParams<R> p = site_params(a, site, nsites);
-	const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 	R l[27], g[27];
 	static_for<27>(
@@ -344,7 +344,7 @@ __global__ void adj_objective_kernel(const AdjArgs<typename S::T, typename S::R>
 	const int z = (int) (site / ((long long) a.X * a.Y));
 	const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
 	const CollParams<R> p = site_params(a, site, nsites);
-	const int base = site_index(x, y, z, a.sy, a.sz, a.x0);
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 	Site<R> s;
 	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);

@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(TPB, MINB)
 			const CollParams<R>& p = M.p;
 			T* const f = M.f;
 			const long long sq = M.sq;
-			const int base = site_index(x, (int) y, (int) z, M.sy, M.sz, M.x0);
+			const long long base = (long long) (z + 1) * M.sz + (long long) (y + 1) * M.sy + M.x0 + x;
 			const Offsets o = neighbour_offsets(true, x, (int) y, (int) z, M.X, M.Y, M.Z, M.sy, M.sz);
 			Site<R> s;
 			aa_read<S, ODD>(f, sq, base, o, s.f);

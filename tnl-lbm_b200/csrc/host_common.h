@@ -26,9 +26,6 @@ inline Geometry make_geometry(int X, int Y, int Z, int es)
 	return g;
 }
 
-// The kernels index within one direction's slab with 32-bit integers.
-constexpr long long MAX_SLAB_ELEMENTS = (1ll << 31) - 1;
-
 // Geier 2017 relaxation rates for omega2 = 1 (col_cum.h:195-228), evaluated
 // once per viscosity in double precision
 inline void cumulant_rates(double nu, CollParamsD& p)

@@ -294,12 +294,6 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 	h->ops = &lbm::storage_ops(d.storage);
 	const int es = h->ops->elem_size;
 	h->g = lbm::make_geometry(d.X, d.Y, d.Z, es);
-	if (h->g.sq > lbm::MAX_SLAB_ELEMENTS) {
-		const long long sq = h->g.sq;
-		delete h;
-		return fail(LBM_ERR_SIZE, "%d x %d x %d sites need %lld elements per direction; the limit is 2^31 - 1", d.X, d.Y,
-					d.Z, sq);
-	}
 	h->pop_bytes = (size_t) 27 * h->g.sq * es;
 	lbm::cumulant_rates(d.viscosity, h->p);
 	h->p.nu = d.viscosity;

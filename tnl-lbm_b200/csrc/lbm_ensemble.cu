@@ -388,10 +388,6 @@ int lbm_ensemble_create(const lbm_ensemble_desc* d, lbm_ensemble* out)
 	size_t total = 0;
 	for (int m = 0; m < e->count; m++) {
 		e->g[m] = lbm::make_geometry(d->X[m], d->Y[m], d->Z[m], es);
-		if (e->g[m].sq > lbm::MAX_SLAB_ELEMENTS) {
-			delete e;
-			return efail(LBM_ERR_SIZE, "member %d needs more than 2^31 - 1 elements per direction", m);
-		}
 		offset[m] = total;
 		total += ((size_t) 27 * e->g[m].sq * es + 255) / 256 * 256;
 		lbm::CollParamsD& p = e->p[m];
