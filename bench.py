@@ -49,7 +49,7 @@ def workload_spec(name):
     if name == "ensemble64":
         return dict(workload="ensemble of 64 periodic Taylor-Green lattices, edges U{32,48,64,96,128} (seeded, "
                              "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
-                    X=0, Y=0, Z=0, kind="ensemble", cum_flags=3)
+                    X=0, Y=0, Z=0, kind="ensemble", cum_flags=3, count=64, edges=(32, 48, 64, 96, 128))
     if name == "ensemble_small":
         return dict(workload="ensemble of 512 small periodic Taylor-Green lattices, edges U{16,24,32} (seeded, "
                              "anisotropic), Re log-uniform in [100, 3200], U0=0.05, cumulant 2017+antialias",
