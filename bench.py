@@ -368,7 +368,7 @@ def make_lattice(pl, spec, storage, device, kernel="direct"):
         m, prof, nu, fields = duct_setup(X, Y, Z)
         lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                      equilibrium=pl.EQ_INV_CUM, storage=st, device=device)
-        lat.set_kernel(pl.KERNEL_TILE if kernel == "tile" else pl.KERNEL_DIRECT)
+        lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT}.get(kernel, pl.KERNEL_DIRECT))
         lat.set_map(m)
         lat.set_inflow(prof, None, None)
         lat.init_equilibrium(*fields)
@@ -376,7 +376,7 @@ def make_lattice(pl, spec, storage, device, kernel="direct"):
     nu = 0.05 * (X / (2 * math.pi)) / 1600.0
     lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                  equilibrium=pl.EQ_INV_CUM, storage=st, periodic=True, device=device)
-    lat.set_kernel(pl.KERNEL_TILE if kernel == "tile" else pl.KERNEL_DIRECT)
+    lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT}.get(kernel, pl.KERNEL_DIRECT))
     lat.init_taylor_green(0.05, 1.0)
     return lat, None
 
@@ -536,12 +536,14 @@ def run_ours(args):
                             "speedup_vs_f32": secs / vsecs,
                             "achieved_gbs": 2 * 27 * 2 * sites / (vsecs / args.steps) / 1e9}
             vl.close()
-        other = "direct" if args.kernel == "tile" else "tile"
-        vl, _ = make_lattice(pl, spec, "f32", local, other)
-        vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
-        vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
-        variants[f"f32_{other}_kernel"] = {"mlups": sites * args.steps / vsecs / 1e6}
-        vl.close()
+        for other in ("direct", "tile", "split"):
+            if other == args.kernel or (other == "split" and spec["kind"] != "duct"):
+                continue
+            vl, _ = make_lattice(pl, spec, "f32", local, other)
+            vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
+            vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
+            variants[f"f32_{other}_kernel"] = {"mlups": sites * args.steps / vsecs / 1e6}
+            vl.close()
     else:
         lat.close()
 
@@ -568,7 +570,7 @@ def run_ours(args):
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
                        "step_kernel": args.kernel,
-                       "block": list(block) if args.kernel == "direct" else "persistent tile kernel, 128 threads"},
+                       "block": list(block) if args.kernel == "direct" else f"{args.kernel} kernel, 128 threads"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -710,7 +712,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-precision", dest="precision", action="store_false")
     ap.add_argument("--autotune", action="store_true")
-    ap.add_argument("--kernel", default="direct", choices=["direct", "tile"])
+    ap.add_argument("--kernel", default="direct", choices=["direct", "tile", "split"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

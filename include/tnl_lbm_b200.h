@@ -176,6 +176,9 @@ LBM_API int lbm_autotune(lbm_handle h, int ntrials);
  * compute the same update, bit for bit. */
 #define LBM_KERNEL_DIRECT 0
 #define LBM_KERNEL_TILE 1
+#define LBM_KERNEL_SPLIT 3 /* lattices with a map: one launch over the tiles of 128
+                              x-sites that hold only GEO_FLUID (no map read, no
+                              boundary branch), one over the others */
 LBM_API int lbm_set_kernel(lbm_handle h, int kernel);
 LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
 

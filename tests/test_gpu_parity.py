@@ -77,7 +77,7 @@ CASES_PERIODIC = [("CUM", 0, "INV_CUM"), ("CUM", 2, "INV_CUM"), ("CUM", 3, "INV_
                   ("SRT", 0, "INV_CUM"), ("BGK", 0, "EQ"), ("MRT", 0, "EQ")]
 
 
-KERNELS = ["TILE", "DIRECT"]
+KERNELS = ["TILE", "DIRECT", "SPLIT"]
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -287,7 +287,7 @@ def test_nonfinite_density_is_reported(pl):
 
 
 @pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S"])
-@pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5), (37, 9, 7), (5, 4, 3)])
+@pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5), (37, 9, 7), (5, 4, 3), (300, 10, 8)])
 def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
     """The two step kernels are the same update: equal results, bit for bit,
     on lattices whose width is a multiple of, larger than, or smaller than a
@@ -299,7 +299,7 @@ def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
     dtype = np.float64 if storage == "F64" else np.float32
     for periodic in (True, False):
         out = []
-        for kernel in (pl.KERNEL_TILE, pl.KERNEL_DIRECT):
+        for kernel in (pl.KERNEL_TILE, pl.KERNEL_DIRECT, pl.KERNEL_SPLIT):
             lat = pl.LBM(X, Y, Z, viscosity=0.01, cum_flags=3, storage=st, periodic=periodic)
             if not periodic:
                 lat.set_map(duct_map(X, Y, Z))

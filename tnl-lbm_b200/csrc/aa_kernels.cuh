@@ -344,4 +344,46 @@ __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typen
 		block_reduce_store<R>(red, a.partials);
 }
 
+// Split step for lattices with a map: the host sorts the lattice's tiles of
+// 128 consecutive x-sites of one row into tiles whose sites are all
+// GEO_FLUID and tiles holding any other type (or lying partly outside the
+// lattice), and runs one launch over each list.  The fluid-only launch reads
+// no map and takes no boundary branch; with the duct's inlet, outlet and wall
+// rims about half of the tiles are fluid-only.  Both launches update disjoint
+// sites with the per-site code of aa_step_kernel, so the results are those of
+// the direct kernel.
+template <typename S, int COLL, int CUMF, bool ODD, bool INTERIOR, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	aa_split_kernel(const StepArgs<typename S::T, typename S::R> a, const unsigned* __restrict__ tiles, int tiles_x)
+{
+	using R = typename S::R;
+	const unsigned t = tiles[blockIdx.x];
+	const unsigned row = t / (unsigned) tiles_x;
+	const int x = (int) (t - row * (unsigned) tiles_x) * 128 + (int) threadIdx.x;
+	const int y = (int) (row % (unsigned) a.Y);
+	const int z = (int) (row / (unsigned) a.Y);
+	if (x >= a.X)
+		return;	 // the last tile of a row can be partial (never a fluid-only tile)
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+	Site<R> s;
+	if constexpr (INTERIOR) {
+		const Offsets o = neighbour_offsets(false, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+		density_velocity(s, a.p);
+		collide<R, COLL, CUMF>(s, a.p);
+		aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+	}
+	else {
+		const long long site = ((long long) z * a.Y + y) * a.X + x;
+		const uint8_t geo = a.map[site];
+		if (geo == GEO_NOTHING)
+			return;
+		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+		if (apply_boundary(s, geo, a, z, y))
+			collide<R, COLL, CUMF>(s, a.p);
+		aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+	}
+}
+
 }  // namespace lbm

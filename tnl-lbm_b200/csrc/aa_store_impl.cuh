@@ -35,9 +35,25 @@ constexpr int direct_minb()
 	return 4;  // SRT and BGK spill at 5
 }
 
+#ifndef SPLIT_MINB_FLUID
+#define SPLIT_MINB_FLUID 5
+#endif
+
 #ifndef ENS_MINB128
 #define ENS_MINB128 5
 #endif
+
+// Resident blocks per SM for the fluid-only launch of the split step (no map,
+// no boundary branch): the largest counts without register spills.
+template <typename R, int COLL, bool ODD>
+constexpr int split_minb()
+{
+	if (sizeof(R) == 8)
+		return 2;
+	if (COLL == COLL_SRT || COLL == COLL_BGK)
+		return 4;
+	return SPLIT_MINB_FLUID;
+}
 
 template <typename S>
 struct StorageUnit
@@ -90,11 +106,33 @@ struct StorageUnit
 		return cudaGetLastError();
 	}
 
+	template <int COLL, int CUMF, bool ODD>
+	static cudaError_t launch_split(const StepLaunch& L, const StepArgs<T, R>& a)
+	{
+		constexpr int minb_in = split_minb<R, COLL, ODD>();
+		constexpr int minb_bd = direct_minb<R, COLL, CUMF, ODD, true, false>();
+		if (L.blocks_out)
+			*L.blocks_out = L.split_n[0] + L.split_n[1];
+		if (L.dry_run)
+			return cudaSuccess;
+		if (L.split_n[0] > 0)
+			aa_split_kernel<S, COLL, CUMF, ODD, true, minb_in>
+				<<<(unsigned) L.split_n[0], 128, 0, L.stream>>>(a, L.split_tiles, L.split_tiles_x);
+		if (L.split_n[1] > 0)
+			aa_split_kernel<S, COLL, CUMF, ODD, false, minb_bd>
+				<<<(unsigned) L.split_n[1], 128, 0, L.stream>>>(a, L.split_tiles + L.split_n[0], L.split_tiles_x);
+		return cudaGetLastError();
+	}
+
 	template <int COLL, int CUMF, bool ODD, bool GENERAL>
 	static cudaError_t launch_one(const StepLaunch& L, const StepArgs<T, R>& a)
 	{
 		if (L.kernel == KERNEL_TILE)
 			return launch_tile<COLL, CUMF, ODD, GENERAL>(L, a);
+		// plain steps of a lattice with a map (observation steps run the direct kernel)
+		if constexpr (GENERAL)
+			if (L.kernel == KERNEL_SPLIT && L.split_tiles && !L.macro && !L.partials)
+				return launch_split<COLL, CUMF, ODD>(L, a);
 		if (L.blocks_out)
 			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
 		if (L.dry_run)

@@ -47,6 +47,9 @@ struct lbm_lattice
 	int streaming = LBM_STREAMING_AA;
 	void* f_out = nullptr;		// A-B: the write buffer (swapped with g.f after every step)
 	void* graph_in = nullptr;	// g.f when the graph was captured
+	unsigned* split_tiles = nullptr;  // split step: fluid-only tiles, then the others
+	long long split_n[2] = {0, 0};
+	int split_tiles_x = 0;
 	void* stats = nullptr;		// D3Q27_MACRO_Mean fields [9][sites], compute type
 	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward

@@ -58,13 +58,17 @@ struct StepLaunch
 	CollParamsD p;
 	int coll, cum_flags;
 	bool odd;
-	int kernel;		   // KERNEL_DIRECT or KERNEL_TILE
+	int kernel;		   // KERNEL_DIRECT, KERNEL_TILE or KERNEL_SPLIT
 	dim3 grid, block;  // direct kernel launch shape
 	int* status;	   // device status word (STATUS_* bits)
 	cudaStream_t stream;
 	long long* blocks_out;	// number of blocks the launch used (partials)
 	bool dry_run;			// only resolve launch facts (attributes, grid), launch nothing
 	void* f_out;			// A-B step: the output buffer (g.f is the input)
+	// split step: tiles [0, split_n[0]) fluid-only, then split_n[1] others
+	const unsigned* split_tiles;
+	long long split_n[2];
+	int split_tiles_x;
 };
 
 // step kernel variants: one thread per site with direct loads, or the
@@ -72,7 +76,8 @@ struct StepLaunch
 enum : int
 {
 	KERNEL_DIRECT = 0,
-	KERNEL_TILE = 1
+	KERNEL_TILE = 1,
+	KERNEL_SPLIT = 3
 };
 // upper bound of the tile kernel's grid (blocks per SM x SMs)
 constexpr int TILE_MAX_BLOCKS_PER_SM = 8;

@@ -158,6 +158,10 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.blocks_out = &blocks;
 	L.dry_run = dry_run;
 	L.f_out = h->f_out;
+	L.split_tiles = h->split_tiles;
+	L.split_n[0] = h->split_n[0];
+	L.split_n[1] = h->split_n[1];
+	L.split_tiles_x = h->split_tiles_x;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
 	const cudaError_t err = ab ? h->ops->ab_step(L) : h->ops->step(L);
 	if (err != cudaSuccess)
@@ -343,6 +347,7 @@ int lbm_destroy(lbm_handle h)
 	lbm::adjoint_free(h->adjoint);
 	cudaFree(h->g.f);
 	cudaFree(h->f_out);
+	cudaFree(h->split_tiles);
 	cudaFree(h->stats);
 	cudaFree(h->map);
 	for (auto* p : h->inflow)
@@ -383,6 +388,31 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	h->map_host.assign(map, map + n);
 	h->map_set = true;
+	// tiles of 128 x-sites for the split step: fluid-only ones first
+	{
+		const int tx = (h->d.X + 127) / 128;
+		std::vector<unsigned> fluid, other;
+		for (long long row = 0; row < (long long) h->d.Y * h->d.Z; row++)
+			for (int t = 0; t < tx; t++) {
+				bool all = (t + 1) * 128 <= h->d.X;
+				for (int i = 0; all && i < 128; i++)
+					all = map[row * h->d.X + t * 128 + i] == lbm::GEO_FLUID;
+				(all ? fluid : other).push_back((unsigned) (row * tx + t));
+			}
+		cudaFree(h->split_tiles);
+		h->split_tiles = nullptr;
+		const size_t nt = fluid.size() + other.size();
+		if (nt > 0xffffffffull)
+			return fail(LBM_ERR_SIZE, "too many tiles for the split step");
+		fluid.insert(fluid.end(), other.begin(), other.end());
+		LBM_CUDA(cudaMalloc(&h->split_tiles, nt * sizeof(unsigned)));
+		LBM_CUDA(cudaMemcpyAsync(h->split_tiles, fluid.data(), nt * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
+		h->split_n[0] = (long long) (nt - other.size());
+		h->split_n[1] = (long long) other.size();
+		h->split_tiles_x = tx;
+		h->drop_graph();
+	}
 	return LBM_OK;
 }
 
@@ -770,10 +800,13 @@ int lbm_autotune(lbm_handle h, int ntrials)
 			bby = c[1];
 		}
 	}
-	// the tile kernel (block shape does not apply to it)
+	// the tile kernel and, with a map, the split step (the block shape does
+	// not apply to them)
 	int best_kernel = lbm::KERNEL_DIRECT;
-	{
-		h->kernel = lbm::KERNEL_TILE;
+	for (int k : {(int) lbm::KERNEL_TILE, (int) lbm::KERNEL_SPLIT}) {
+		if (k == lbm::KERNEL_SPLIT && !h->split_tiles)
+			continue;
+		h->kernel = k;
 		launch_step(h, false, false);
 		launch_step(h, false, false);
 		cudaEventRecord(e0, h->stream);
@@ -785,7 +818,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 		cudaEventElapsedTime(&ms, e0, e1);
 		if (ms < best) {
 			best = ms;
-			best_kernel = lbm::KERNEL_TILE;
+			best_kernel = k;
 		}
 	}
 	cudaEventDestroy(e0);
@@ -888,7 +921,7 @@ int lbm_set_kernel(lbm_handle h, int kernel)
 {
 	if (int rc = check(h))
 		return rc;
-	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE)
+	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE && kernel != LBM_KERNEL_SPLIT)
 		return fail(LBM_ERR_INVALID, "unknown kernel %d", kernel);
 	h->kernel = kernel;
 	h->drop_graph();
