@@ -27,6 +27,7 @@ struct lbm_lattice
 	bool map_set = false;
 	void* inflow[3] = {nullptr, nullptr, nullptr};
 	void* inflow_host = nullptr;  // pinned staging of the converted profiles
+	cudaEvent_t inflow_ev = nullptr;  // recorded after the staging's last copy
 	void* macro = nullptr;
 	bool macro_valid = false;
 	double* partials = nullptr;

@@ -355,6 +355,8 @@ int lbm_destroy(lbm_handle h)
 	cudaFree(h->macro);
 	if (h->inflow_host)
 		cudaFreeHost(h->inflow_host);
+	if (h->inflow_ev)
+		cudaEventDestroy(h->inflow_ev);
 	cudaFree(h->partials);
 	cudaFree(h->sums_dev);
 	cudaFree(h->status_dev);
@@ -425,6 +427,11 @@ int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const doubl
 	const int cs = h->ops->compute_size;
 	if (!h->inflow_host)
 		LBM_CUDA(cudaMallocHost(&h->inflow_host, 3 * n * cs));
+	if (!h->inflow_ev)
+		LBM_CUDA(cudaEventCreateWithFlags(&h->inflow_ev, cudaEventDisableTiming));
+	// the staging buffer is reused: wait for the copies of the previous call
+	// (normally long done) instead of synchronising the stream after each call
+	LBM_CUDA(cudaEventSynchronize(h->inflow_ev));
 	bool realloc = false;
 	for (int k = 0; k < 3; k++) {
 		if (!src[k]) {
@@ -445,8 +452,7 @@ int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const doubl
 				((float*) stage)[i] = (float) src[k][i];
 		LBM_CUDA(cudaMemcpyAsync(h->inflow[k], stage, n * cs, cudaMemcpyHostToDevice, h->stream));
 	}
-	// the staging buffer is reused by the next call: wait for the copies
-	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	LBM_CUDA(cudaEventRecord(h->inflow_ev, h->stream));
 	if (realloc)
 		h->drop_graph();  // kernel arguments changed; new values alone need no new graph
 	return LBM_OK;
