@@ -58,7 +58,7 @@ struct StepArgs
 	const R* in_vy;
 	const R* in_vz;
 	R* macro;		   // [4][Z][Y][X] or null
-	double* partials;  // [NRED][blocks] or null
+	double* partials;  // [NRED][slots] or null
 	CollParams<R> p;
 };
 
@@ -251,6 +251,76 @@ __device__ __forceinline__ bool apply_boundary(Site<R>& s, uint8_t geo, const St
 	}
 }
 
+// Per-warp FP64 sums of the NRED quantities of one step, stored as
+// partials[k][slot] with one slot per warp of the launch.  No shared memory
+// and no barrier: a warp leaves as soon as its own sums are stored, so the
+// observation step keeps as many loads in flight as the plain step.  The
+// butterfly halves the set of values each warp lane carries at every level
+// (8 slots, the last two zero: 4 + 2 + 1 exchanges), then finishes with two
+// plain levels, 9 64-bit shuffles in all instead of 5 per quantity; lane 4q
+// ends with the warp sum of quantity q.  The order of the additions is fixed.
+// Requires blockDim.x to be a multiple of 32, so that a warp is one row of
+// the block.
+__device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], double* partials)
+{
+	constexpr unsigned FULL = 0xffffffffu;
+	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+	const int lane = tid & 31;
+	const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+	double a[4];
+#pragma unroll
+	for (int i = 0; i < 4; i++) {
+		const double lo = v[i];
+		const double hi = i + 4 < NRED ? v[(i + 4) % NRED] : 0.0;
+		a[i] = (h16 ? hi : lo) + __shfl_xor_sync(FULL, h16 ? lo : hi, 16);
+	}
+	double b[2];
+#pragma unroll
+	for (int i = 0; i < 2; i++)
+		b[i] = (h8 ? a[i + 2] : a[i]) + __shfl_xor_sync(FULL, h8 ? a[i] : a[i + 2], 8);
+	double c = (h4 ? b[1] : b[0]) + __shfl_xor_sync(FULL, h4 ? b[0] : b[1], 4);
+	c += __shfl_xor_sync(FULL, c, 2);
+	c += __shfl_xor_sync(FULL, c, 1);
+	const int q = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+	if ((lane & 3) == 0 && q < NRED) {
+		const int wpb = (blockDim.x * blockDim.y) >> 5;
+		const long long nslots = (long long) gridDim.x * gridDim.y * gridDim.z * wpb;
+		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
+		partials[q * nslots + block * wpb + (tid >> 5)] = c;
+	}
+}
+
+// Outputs of an observation step for one site: the macro field and the
+// per-warp FP64 sums.  Every lane of the warp calls it (lanes past the
+// lattice edge with active = false).  The step kernels call it between the
+// boundary treatment and the collision: the collision changes neither the
+// density nor the velocity, and the registers of the sums are free again
+// before the collision needs the most.
+template <typename T, typename R>
+__device__ __forceinline__ void step_outputs(const StepArgs<T, R>& a, bool active, long long site, const Site<R>& s)
+{
+	if (active && a.macro) {
+		const long long n = (long long) a.X * a.Y * a.Z;
+		a.macro[site] = s.rho;
+		a.macro[n + site] = s.vx;
+		a.macro[2 * n + site] = s.vy;
+		a.macro[3 * n + site] = s.vz;
+	}
+	if (a.partials) {
+		double red[NRED] = {0, 0, 0, 0, 0, 0};
+		if (active) {
+			const double rho = (double) s.rho, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
+			red[0] = rho;
+			red[1] = rho * vx;
+			red[2] = rho * vy;
+			red[3] = rho * vz;
+			red[4] = rho * (vx * vx + vy * vy + vz * vz);
+			red[5] = isfinite(rho) ? 0.0 : 1.0;
+		}
+		warp_reduce_store(red, a.partials);
+	}
+}
+
 template <typename R>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* partials)
 {
@@ -296,52 +366,39 @@ __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typen
 	const int z = blockIdx.z;
 	const bool active = x < a.X && y < a.Y;
 
-	double red[NRED] = {0, 0, 0, 0, 0, 0};
+	Site<R> s;
+	Offsets o;
+	long long base = 0, site = 0;
+	bool coll = false, write = false;
 	if (active) {
-		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-		const long long site = ((long long) z * a.Y + y) * a.X + x;
+		base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+		site = ((long long) z * a.Y + y) * a.X + x;
 		uint8_t geo = GEO_PERIODIC;
 		if constexpr (GENERAL)
 			geo = a.map[site];
-		Site<R> s;
-		bool store = true;
 		if (GENERAL && geo == GEO_NOTHING) {
 			s.rho = R(1);
 			s.vx = s.vy = s.vz = R(0);
-			store = false;
 		}
 		else {
-			const Offsets o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+			o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
-			bool coll = true;
 			if constexpr (GENERAL)
 				coll = apply_boundary(s, geo, a, z, y);
-			else
+			else {
 				density_velocity(s, a.p);
-			if (coll)
-				collide<R, COLL, CUMF>(s, a.p);
-			aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
-		}
-		(void) store;
-		if (OUT && a.macro) {
-			const long long n = (long long) a.X * a.Y * a.Z;
-			a.macro[site] = s.rho;
-			a.macro[n + site] = s.vx;
-			a.macro[2 * n + site] = s.vy;
-			a.macro[3 * n + site] = s.vz;
-		}
-		if (OUT && a.partials) {
-			const double rho = (double) s.rho, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
-			red[0] = rho;
-			red[1] = rho * vx;
-			red[2] = rho * vy;
-			red[3] = rho * vz;
-			red[4] = rho * (vx * vx + vy * vy + vz * vz);
-			red[5] = isfinite(rho) ? 0.0 : 1.0;
+				coll = true;
+			}
+			write = true;
 		}
 	}
-	if (OUT && a.partials)
-		block_reduce_store<R>(red, a.partials);
+	if constexpr (OUT)
+		step_outputs(a, active, site, s);
+	if (write) {
+		if (coll)
+			collide<R, COLL, CUMF>(s, a.p);
+		aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+	}
 }
 
 // Split step for lattices with a map: the host sorts the lattice's tiles of

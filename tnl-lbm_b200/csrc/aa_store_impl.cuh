@@ -18,21 +18,32 @@ namespace lbm {
 // Resident 128-thread blocks per SM requested from the compiler for the
 // direct step kernel; __launch_bounds__(128, n) caps registers at
 // 65536 / (128 n): 4 -> 128, 5 -> 102 (96 used), 6 -> 85 (80 used).  The
-// values are the largest n at which each instantiation compiles without
-// register spills (-Xptxas -v on sm_100a): more resident warps keep more HBM
-// requests in flight.  The FP64 kernels need twice the registers per value.
+// values are the largest n at which the instantiations compile without (or
+// with a few bytes of) register spills (-Xptxas -v on sm_100a): more
+// resident warps keep more HBM requests in flight.  The observation variant
+// (OUT) needs no more registers than the plain step: its outputs are written
+// before the collision.  The FP64 kernels need twice the registers per value.
 template <typename R, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
 constexpr int direct_minb()
 {
 	if (sizeof(R) == 8)
 		return 2;
-	if (OUT)
-		return 4;
 	if (!ODD && GENERAL)
-		return 6;
+		return 6;  // the even general step keeps no neighbour offsets: 80 registers
 	if (COLL == COLL_CUM || COLL == COLL_MRT)
 		return 5;
 	return 4;  // SRT and BGK spill at 5
+}
+
+// resident blocks of the A-B step; its observation variant spills at 5
+template <typename R, int COLL, int CUMF, bool OUT>
+constexpr int ab_minb()
+{
+	if (sizeof(R) == 8)
+		return 2;
+	if (OUT)
+		return 4;
+	return direct_minb<R, COLL, CUMF, true, true, false>();
 }
 
 #ifndef SPLIT_MINB_FLUID
@@ -133,8 +144,8 @@ struct StorageUnit
 		if constexpr (GENERAL)
 			if (L.kernel == KERNEL_SPLIT && L.split_tiles && !L.macro && !L.partials)
 				return launch_split<COLL, CUMF, ODD>(L, a);
-		if (L.blocks_out)
-			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
+		if (L.blocks_out)  // one partial-sum slot per warp
+			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z * ((L.block.x * L.block.y) / 32);
 		if (L.dry_run)
 			return cudaSuccess;
 		if (L.macro || L.partials)
@@ -206,15 +217,15 @@ struct StorageUnit
 	template <int COLL, int CUMF>
 	static cudaError_t ab_launch(const StepLaunch& L, const StepArgs<T, R>& a)
 	{
-		if (L.blocks_out)
-			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z;
+		if (L.blocks_out)  // one partial-sum slot per warp
+			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z * ((L.block.x * L.block.y) / 32);
 		if (L.dry_run)
 			return cudaSuccess;
 		if (L.macro || L.partials)
-			ab_step_kernel<S, COLL, CUMF, true, direct_minb<R, COLL, CUMF, true, true, true>()>
+			ab_step_kernel<S, COLL, CUMF, true, ab_minb<R, COLL, CUMF, true>()>
 				<<<L.grid, L.block, 0, L.stream>>>(a, (T*) L.f_out);
 		else
-			ab_step_kernel<S, COLL, CUMF, false, direct_minb<R, COLL, CUMF, true, true, false>()>
+			ab_step_kernel<S, COLL, CUMF, false, ab_minb<R, COLL, CUMF, false>()>
 				<<<L.grid, L.block, 0, L.stream>>>(a, (T*) L.f_out);
 		return cudaGetLastError();
 	}

@@ -133,12 +133,13 @@ __global__ void __launch_bounds__(128, MINB)
 	const int y = blockIdx.y * blockDim.y + threadIdx.y;
 	const int z = blockIdx.z;
 	const bool active = x < a.X && y < a.Y;
-	double red[NRED] = {0, 0, 0, 0, 0, 0};
+	Site<R> s;
+	long long base = 0, site = 0;
+	bool coll = false, write = false;
 	if (active) {
-		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-		const long long site = ((long long) z * a.Y + y) * a.X + x;
+		base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+		site = ((long long) z * a.Y + y) * a.X + x;
 		const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
-		Site<R> s;
 		if (geo == GEO_NOTHING) {
 			s.rho = R(1);
 			s.vx = s.vy = s.vz = R(0);
@@ -149,35 +150,23 @@ __global__ void __launch_bounds__(128, MINB)
 				ab_read_interp<S>(a.f, a.sq, base, o, s.f);
 			else
 				ab_read<S>(a.f, a.sq, base, o, s.f);
-			if (ab_boundary<S>(s, geo, a, base, z, y))
-				collide<R, COLL, CUMF>(s, a.p);
-			static_for<27>(
-				[&](auto Qc)
-				{
-					constexpr int q = decltype(Qc)::value;
-					S::template store<q>(fout + q * a.sq + base, s.f[q]);
-				}
-			);
-		}
-		if (OUT && a.macro) {
-			const long long n = (long long) a.X * a.Y * a.Z;
-			a.macro[site] = s.rho;
-			a.macro[n + site] = s.vx;
-			a.macro[2 * n + site] = s.vy;
-			a.macro[3 * n + site] = s.vz;
-		}
-		if (OUT && a.partials) {
-			const double rho = (double) s.rho, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
-			red[0] = rho;
-			red[1] = rho * vx;
-			red[2] = rho * vy;
-			red[3] = rho * vz;
-			red[4] = rho * (vx * vx + vy * vy + vz * vz);
-			red[5] = isfinite(rho) ? 0.0 : 1.0;
+			coll = ab_boundary<S>(s, geo, a, base, z, y);
+			write = true;
 		}
 	}
-	if (OUT && a.partials)
-		block_reduce_store<R>(red, a.partials);
+	if constexpr (OUT)
+		step_outputs(a, active, site, s);
+	if (write) {
+		if (coll)
+			collide<R, COLL, CUMF>(s, a.p);
+		static_for<27>(
+			[&](auto Qc)
+			{
+				constexpr int q = decltype(Qc)::value;
+				S::template store<q>(fout + q * a.sq + base, s.f[q]);
+			}
+		);
+	}
 }
 
 }  // namespace lbm

@@ -32,15 +32,16 @@ struct lbm_lattice
 	bool macro_valid = false;
 	double* partials = nullptr;
 	long long partials_cap = 0;	 // in blocks
-	double* sums_dev = nullptr;
 	double* sums_host = nullptr;  // pinned [NRED]
+	double* sums_mapped = nullptr;	// device address of sums_host (written by the finish kernel)
+	unsigned* finish_arrived = nullptr;	 // arrival counter of the finish kernel, zero between launches
 	bool sums_valid = false;
 	long long iteration = 0;
 	int bx = 0, by = 0;	 // 0: default
 	int kernel = lbm::KERNEL_DIRECT;
 	int sms = 148;
 	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
-	long long last_blocks = 0;	// blocks of the last step launch
+	long long last_blocks = 0;	// partial-sum slots of the last step launch
 	lbm::CollParamsD p{};
 	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
 	cudaGraphExec_t graph = nullptr;
@@ -77,11 +78,13 @@ struct lbm_lattice
 		const dim3 gr = grid();
 		return (long long) gr.x * gr.y * gr.z;
 	}
-	// partial-sum slots any step kernel variant may need
+	// partial-sum slots any step kernel variant may need: one per block of the
+	// persistent tile kernel, one per warp of the direct and A-B kernels
 	long long max_step_blocks() const
 	{
 		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
-		const long long direct = grid_blocks();
+		const dim3 b = block();
+		const long long direct = grid_blocks() * ((b.x * b.y) / 32);
 		return tile > direct ? tile : direct;
 	}
 	void drop_graph()

@@ -62,7 +62,7 @@ struct StepLaunch
 	dim3 grid, block;  // direct kernel launch shape
 	int* status;	   // device status word (STATUS_* bits)
 	cudaStream_t stream;
-	long long* blocks_out;	// number of blocks the launch used (partials)
+	long long* blocks_out;	// partial-sum slots the launch writes (blocks or warps)
 	bool dry_run;			// only resolve launch facts (attributes, grid), launch nothing
 	void* f_out;			// A-B step: the output buffer (g.f is the input)
 	// split step: tiles [0, split_n[0]) fluid-only, then split_n[1] others
@@ -124,10 +124,13 @@ const StorageOps& storage_ops(int storage);
 
 // FP64 reductions shared by all storages (lbm_reduce.cu)
 constexpr int NRED_HOST = 6;
-// partials are stored as [NRED][nblocks]; stage is scratch of
-// finish_scratch_doubles() doubles
+// partials are stored as [NRED][nslots]; stage is scratch of
+// finish_scratch_doubles() doubles; arrived is a device counter that holds
+// zero between launches (one per stream that runs finish_sums); out may be
+// device or mapped host memory
 long long finish_scratch_doubles();
-cudaError_t finish_sums(const double* partials, long long nblocks, double* stage, double* out, cudaStream_t);
+cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out,
+						cudaStream_t);
 // enstrophy-type sum rho * |grad u|^2 with central differences over the macro
 // field (compute type given by compute_size), periodic wrap as sim_4.cu:21-54
 cudaError_t enstrophy_partials(const void* macro, int compute_size, int X, int Y, int Z, double* partials, long long* nblocks,

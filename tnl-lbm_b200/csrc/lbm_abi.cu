@@ -323,8 +323,10 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 		&& (cudaMalloc(&h->map, (size_t) h->sites() + 64) != cudaSuccess
 			|| cudaMemsetAsync(h->map, 0, (size_t) h->sites() + 64, h->stream) != cudaSuccess))
 		return cleanup(fail(LBM_ERR_CUDA, "map allocation failed"));
-	if (cudaMalloc(&h->sums_dev, lbm::NRED_HOST * sizeof(double)) != cudaSuccess
-		|| cudaMallocHost(&h->sums_host, lbm::NRED_HOST * sizeof(double)) != cudaSuccess)
+	if (cudaHostAlloc(&h->sums_host, lbm::NRED_HOST * sizeof(double), cudaHostAllocMapped) != cudaSuccess
+		|| cudaHostGetDevicePointer((void**) &h->sums_mapped, h->sums_host, 0) != cudaSuccess
+		|| cudaMalloc(&h->finish_arrived, sizeof(unsigned)) != cudaSuccess
+		|| cudaMemsetAsync(h->finish_arrived, 0, sizeof(unsigned), h->stream) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "reduction buffers allocation failed"));
 	if (cudaMalloc(&h->status_dev, sizeof(int)) != cudaSuccess || cudaMemsetAsync(h->status_dev, 0, sizeof(int), h->stream) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "status word allocation failed"));
@@ -358,7 +360,7 @@ int lbm_destroy(lbm_handle h)
 	if (h->inflow_ev)
 		cudaEventDestroy(h->inflow_ev);
 	cudaFree(h->partials);
-	cudaFree(h->sums_dev);
+	cudaFree(h->finish_arrived);
 	cudaFree(h->status_dev);
 	if (h->sums_host)
 		cudaFreeHost(h->sums_host);
@@ -607,11 +609,11 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 		}
 		if (sums) {
 			const long long nb = h->last_blocks;
-			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->sums_dev, h->stream);
+			// the finish kernel writes the sums straight into the mapped pinned buffer
+			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
+												   h->sums_mapped, h->stream);
 			if (e != cudaSuccess)
 				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
-			LBM_CUDA(cudaMemcpyAsync(h->sums_host, h->sums_dev, lbm::NRED_HOST * sizeof(double), cudaMemcpyDeviceToHost,
-									 h->stream));
 		}
 		h->macro_valid = true;
 		h->sums_valid = sums;
@@ -629,11 +631,11 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 			return rc;
 		if (sums) {
 			const long long nb = h->last_blocks;
-			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->sums_dev, h->stream);
+			// the finish kernel writes the sums straight into the mapped pinned buffer
+			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
+												   h->sums_mapped, h->stream);
 			if (e != cudaSuccess)
 				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
-			LBM_CUDA(cudaMemcpyAsync(h->sums_host, h->sums_dev, lbm::NRED_HOST * sizeof(double), cudaMemcpyDeviceToHost,
-									 h->stream));
 		}
 		h->macro_valid = macro;
 		h->sums_valid = sums;
@@ -713,7 +715,7 @@ int lbm_enstrophy_sum(lbm_handle h, double* out)
 	LBM_CUDA(cudaMallocAsync((void**) &dres, lbm::NRED_HOST * sizeof(double), h->stream));
 	cudaError_t e = lbm::enstrophy_partials(h->macro, h->ops->compute_size, h->d.X, h->d.Y, h->d.Z, h->partials, &nb, h->stream);
 	if (e == cudaSuccess)
-		e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, dres, h->stream);
+		e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived, dres, h->stream);
 	double res[lbm::NRED_HOST];
 	if (e == cudaSuccess)
 		e = cudaMemcpyAsync(res, dres, sizeof(res), cudaMemcpyDeviceToHost, h->stream);

@@ -96,8 +96,8 @@ struct lbm_ensemble_t
 	int* tile_member_dev = nullptr;
 	long long* tile0_dev = nullptr;
 	double* partials = nullptr;	 // [NRED][ntiles]
-	double* sums_dev = nullptr;	 // [count][NRED]
-	double* sums_host = nullptr;
+	double* sums_host = nullptr;	 // pinned [count][NRED]
+	double* sums_mapped = nullptr;	 // device address of sums_host
 	bool sums_valid = false;
 	long long iteration = 0;
 	cudaGraphExec_t graph = nullptr;
@@ -410,8 +410,8 @@ int lbm_ensemble_create(const lbm_ensemble_desc* d, lbm_ensemble* out)
 		return cleanup(efail(LBM_ERR_CUDA, "population memset failed"));
 	for (int m = 0; m < e->count; m++)
 		e->g[m].f = (char*) e->pops + offset[m];
-	if (cudaMalloc(&e->sums_dev, sizeof(double) * NRED * e->count) != cudaSuccess
-		|| cudaMallocHost(&e->sums_host, sizeof(double) * NRED * e->count) != cudaSuccess)
+	if (cudaHostAlloc(&e->sums_host, sizeof(double) * NRED * e->count, cudaHostAllocMapped) != cudaSuccess
+		|| cudaHostGetDevicePointer((void**) &e->sums_mapped, e->sums_host, 0) != cudaSuccess)
 		return cleanup(efail(LBM_ERR_CUDA, "reduction buffers allocation failed"));
 	if (int rc = build_tiles(e))
 		return cleanup(rc);
@@ -429,7 +429,6 @@ int lbm_ensemble_destroy(lbm_ensemble e)
 	e->drop_graph();
 	e->free_tiles();
 	cudaFree(e->pops);
-	cudaFree(e->sums_dev);
 	cudaFreeHost(e->sums_host);
 	for (cudaStream_t st : e->lanes)
 		cudaStreamDestroy(st);
@@ -529,10 +528,9 @@ int lbm_ensemble_step(lbm_ensemble e, int64_t nsteps, int flags)
 	if (sums) {
 		if (int rc = ens_launch(e, true))
 			return rc;
-		ens_finish_kernel<<<e->count, 256, 0, e->stream>>>(e->partials, e->ntiles, e->tile0_dev, e->sums_dev);
+		// written straight into the mapped pinned buffer
+		ens_finish_kernel<<<e->count, 256, 0, e->stream>>>(e->partials, e->ntiles, e->tile0_dev, e->sums_mapped);
 		ENS_CUDA(cudaGetLastError());
-		ENS_CUDA(cudaMemcpyAsync(e->sums_host, e->sums_dev, sizeof(double) * NRED * e->count, cudaMemcpyDeviceToHost,
-								 e->stream));
 		e->sums_valid = true;
 	}
 	return LBM_OK;

@@ -11,55 +11,82 @@
 
 namespace lbm {
 
-// Two-stage deterministic finish of the per-block partial sums, stored as
-// partials[k][nblocks].  Stage 1: FINISH_BLOCKS blocks, each summing a fixed
-// contiguous chunk of every quantity in a fixed order; stage 2: one block
-// summing the stage-1 results.  The result does not depend on scheduling.
+// Deterministic finish of the partial sums, stored as partials[k][nslots], in
+// one launch.  FINISH_BLOCKS blocks each sum a fixed contiguous chunk of every
+// quantity in a fixed order and store the block results in stage; the block
+// that arrives last on the arrival counter sums the stage in a fixed order,
+// writes out[NRED] (device or mapped host memory) and resets the counter for
+// the next launch.  The result does not depend on scheduling.
 constexpr int FINISH_THREADS = 256;
 constexpr int FINISH_BLOCKS = 296;
+constexpr int FINISH_WARPS = FINISH_THREADS / 32;
 
-__device__ __forceinline__ double block_sum(double v, double* sh)
+// sums of NRED values over the block, valid in thread 0
+__device__ __forceinline__ void block_sums(double (&v)[NRED], double (*sh)[NRED])
 {
-	sh[threadIdx.x] = v;
+#pragma unroll
+	for (int k = 0; k < NRED; k++)
+#pragma unroll
+		for (int off = 16; off > 0; off >>= 1)
+			v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
+#pragma unroll
+		for (int k = 0; k < NRED; k++)
+			sh[warp][k] = v[k];
 	__syncthreads();
-	for (int s = FINISH_THREADS / 2; s > 0; s >>= 1) {
-		if ((int) threadIdx.x < s)
-			sh[threadIdx.x] += sh[threadIdx.x + s];
-		__syncthreads();
-	}
-	const double r = sh[0];
-	__syncthreads();
-	return r;
+	if (threadIdx.x == 0)
+#pragma unroll
+		for (int k = 0; k < NRED; k++) {
+			double acc = 0;
+			for (int w = 0; w < FINISH_WARPS; w++)
+				acc += sh[w][k];
+			v[k] = acc;
+		}
 }
 
-__global__ void __launch_bounds__(FINISH_THREADS) finish_stage1(const double* __restrict__ partials, long long nblocks,
-																double* __restrict__ stage)
-{
-	__shared__ double sh[FINISH_THREADS];
-	const long long chunk = (nblocks + gridDim.x - 1) / gridDim.x;
-	const long long b0 = blockIdx.x * chunk;
-	const long long b1 = b0 + chunk < nblocks ? b0 + chunk : nblocks;
-	for (int k = 0; k < NRED; k++) {
-		double v = 0;
-		for (long long b = b0 + threadIdx.x; b < b1; b += FINISH_THREADS)
-			v += partials[k * nblocks + b];
-		const double r = block_sum(v, sh);
-		if (threadIdx.x == 0)
-			stage[k * gridDim.x + blockIdx.x] = r;
-	}
-}
-
-__global__ void __launch_bounds__(FINISH_THREADS) finish_stage2(const double* __restrict__ stage, int nstage,
+__global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __restrict__ partials, long long nslots,
+																double* __restrict__ stage, unsigned* __restrict__ arrived,
 																double* __restrict__ out)
 {
-	__shared__ double sh[FINISH_THREADS];
+	__shared__ double sh[FINISH_WARPS][NRED];
+	__shared__ bool last;
+	const long long chunk = (nslots + gridDim.x - 1) / gridDim.x;
+	const long long b0 = blockIdx.x * chunk;
+	const long long b1 = b0 + chunk < nslots ? b0 + chunk : nslots;
+	double v[NRED];
+#pragma unroll
 	for (int k = 0; k < NRED; k++) {
-		double v = 0;
-		for (int b = threadIdx.x; b < nstage; b += FINISH_THREADS)
-			v += stage[k * nstage + b];
-		const double r = block_sum(v, sh);
-		if (threadIdx.x == 0)
-			out[k] = r;
+		v[k] = 0;
+		for (long long b = b0 + threadIdx.x; b < b1; b += FINISH_THREADS)
+			v[k] += partials[k * nslots + b];
+	}
+	block_sums(v, sh);
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int k = 0; k < NRED; k++)
+			stage[k * FINISH_BLOCKS + blockIdx.x] = v[k];
+		__threadfence();
+		last = atomicAdd(arrived, 1u) == gridDim.x - 1;
+	}
+	__syncthreads();
+	if (!last)
+		return;
+	__threadfence();
+	__syncthreads();  // sh is reused
+#pragma unroll
+	for (int k = 0; k < NRED; k++) {
+		v[k] = 0;
+		for (int b = threadIdx.x; b < (int) gridDim.x; b += FINISH_THREADS)
+			v[k] += __ldcg(stage + k * FINISH_BLOCKS + b);
+	}
+	block_sums(v, sh);
+	if (threadIdx.x == 0) {
+#pragma unroll
+		for (int k = 0; k < NRED; k++)
+			out[k] = v[k];
+		*arrived = 0;
+		__threadfence_system();
 	}
 }
 
@@ -68,10 +95,9 @@ long long finish_scratch_doubles()
 	return (long long) FINISH_BLOCKS * NRED;
 }
 
-cudaError_t finish_sums(const double* partials, long long nblocks, double* stage, double* out, cudaStream_t st)
+cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out, cudaStream_t st)
 {
-	finish_stage1<<<FINISH_BLOCKS, FINISH_THREADS, 0, st>>>(partials, nblocks, stage);
-	finish_stage2<<<1, FINISH_THREADS, 0, st>>>(stage, FINISH_BLOCKS, out);
+	finish_kernel<<<FINISH_BLOCKS, FINISH_THREADS, 0, st>>>(partials, nslots, stage, arrived, out);
 	return cudaGetLastError();
 }
 
