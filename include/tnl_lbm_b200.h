@@ -110,6 +110,11 @@ LBM_API const char* lbm_last_error(void);
  * the order in which sites run) and for the adjoint types. */
 LBM_API int lbm_set_map(lbm_handle h, const uint8_t* map);
 
+/* The map last set (by lbm_set_map or lbm_checkpoint_load), host [Z][Y][X];
+ * LBM_ERR_INVALID on a periodic lattice or before a map was set.  Replaces
+ * copyMapToHost (include/lbm3d/lbm.h:66). */
+LBM_API int lbm_get_map(lbm_handle h, uint8_t* map);
+
 /* Inlet velocity profiles, host [Z][Y] doubles; NULL means zero.
  * Replaces NSE_Data_InflowProfile (include/lbm3d/lbm_data.h:95-133). */
 LBM_API int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const double* vz);

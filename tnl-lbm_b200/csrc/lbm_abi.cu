@@ -420,6 +420,18 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 	return LBM_OK;
 }
 
+int lbm_get_map(lbm_handle h, uint8_t* map)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!map)
+		return fail(LBM_ERR_INVALID, "null map");
+	if (h->d.periodic || h->map_host.empty())
+		return fail(LBM_ERR_INVALID, "no map: the lattice is periodic or lbm_set_map was not called");
+	std::memcpy(map, h->map_host.data(), h->map_host.size());
+	return LBM_OK;
+}
+
 int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const double* vz)
 {
 	if (int rc = check(h))

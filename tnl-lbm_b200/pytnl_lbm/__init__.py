@@ -22,7 +22,8 @@ from ._abi import (  # noqa: F401  (re-exported constants)
     GEO, KERNEL_DIRECT, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
     STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
 
-__all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute"]
+__all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute", "Actions",
+           "Counter", "MAX_COUNTER", "NSE", "macro_from_populations"]
 
 # D3Q27_MACRO_Default quantity order (include/lbm3d/d3q27/macro.h:61-68)
 macro_names = ("rho", "vx", "vy", "vz")
@@ -86,6 +87,12 @@ class LBM:
         m = np.ascontiguousarray(geo_map, dtype=np.uint8)
         assert m.shape == self.shape, f"map shape {m.shape} != {self.shape}"
         _abi.check(self.lib.lbm_set_map(self.h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def get_map(self):
+        """The map last set or loaded from a checkpoint, [Z][Y][X] uint8."""
+        m = np.empty(self.shape, np.uint8)
+        _abi.check(self.lib.lbm_get_map(self.h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return m
 
     def set_inflow(self, vx=None, vy=None, vz=None):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (vx, vy, vz)]
@@ -390,4 +397,4 @@ def kinetic_energy(lbm: LBM, rho0=1.0):
     return s[4] / rho0 / 2.0 / (lbm.X * lbm.Y * lbm.Z)
 
 
-from ._state import State, execute  # noqa: E402,F401
+from ._state import MAX_COUNTER, NSE, Actions, Counter, State, execute, macro_from_populations  # noqa: E402,F401

@@ -62,6 +62,7 @@ SIGNATURES = {
     "lbm_destroy": (ctypes.c_int, [_H]),
     "lbm_last_error": (ctypes.c_char_p, []),
     "lbm_set_map": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_uint8)]),
+    "lbm_get_map": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_uint8)]),
     "lbm_set_inflow": (ctypes.c_int, [_H, _dp, _dp, _dp]),
     "lbm_set_viscosity": (ctypes.c_int, [_H, ctypes.c_double]),
     "lbm_init_equilibrium": (ctypes.c_int, [_H, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
