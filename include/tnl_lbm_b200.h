@@ -342,6 +342,64 @@ LBM_API int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, 
 LBM_API int lbm_adjoint_release(lbm_handle h);
 
 /* Library build information: sm architecture and version string. */
+/* Coupled D3Q7 advection-diffusion scalar (State_NSE_ADE with the coupled
+ * kernel of include/lbm3d/kernels.h:114-196).  Once enabled, every lbm_step
+ * also advances the scalar phi with the flow site's velocity, in the same
+ * kernel: the seven scalar populations use the A-A pattern and the flow
+ * lattice's neighbour indices.  Collisions (include/lbm3d/d3q7/): SRT, MRT
+ * and the central-moment CLBM, omega = 1 / (1/2 + 4 D).  Scalar site types
+ * (d3q7/bc.h:17-36, values LBM_ADE_GEO_*): FLUID, WALL, WALL_BODY, SOLID,
+ * INFLOW (phi = inflow_phi, ADE_Data_ConstInflow), PERIODIC, NOTHING and
+ * SYM_TOP..SYM_FRONT; the outflow and phase-transfer types are refused
+ * (their A-A update depends on the order of the sites).  Provided for FP64,
+ * FP32 and F32S storage on A-A lattices; the adjoint and checkpoints refuse a
+ * lattice with a scalar. */
+#define LBM_ADE_SRT 0
+#define LBM_ADE_MRT 1
+#define LBM_ADE_CLBM 2
+#define LBM_ADE_GEO_FLUID 0
+#define LBM_ADE_GEO_WALL 1
+#define LBM_ADE_GEO_WALL_BODY 2
+#define LBM_ADE_GEO_SOLID 3
+#define LBM_ADE_GEO_INFLOW 7
+#define LBM_ADE_GEO_PERIODIC 9
+#define LBM_ADE_GEO_NOTHING 10
+#define LBM_ADE_GEO_SYM_TOP 12
+#define LBM_ADE_GEO_SYM_BOTTOM 13
+#define LBM_ADE_GEO_SYM_LEFT 14
+#define LBM_ADE_GEO_SYM_RIGHT 15
+#define LBM_ADE_GEO_SYM_BACK 16
+#define LBM_ADE_GEO_SYM_FRONT 17
+
+typedef struct lbm_ade_desc
+{
+	int32_t collision;	/* LBM_ADE_SRT, LBM_ADE_MRT or LBM_ADE_CLBM */
+	double diffusion;	/* lattice diffusion coefficient (ADE lbmViscosity) */
+	double inflow_phi;	/* phi imposed at LBM_ADE_GEO_INFLOW sites */
+} lbm_ade_desc;
+
+/* Allocate the scalar (all sites LBM_ADE_GEO_FLUID, populations zero). */
+LBM_API int lbm_ade_enable(lbm_handle h, const lbm_ade_desc* desc);
+LBM_API int lbm_ade_disable(lbm_handle h);
+/* Scalar site types, host [Z][Y][X]. */
+LBM_API int lbm_ade_set_map(lbm_handle h, const uint8_t* map);
+/* Per-site diffusion coefficient, host [Z][Y][X] doubles (the
+ * diffusion_coefficient_ptr of ADE_Data, lbm_data.h:219-239); NULL returns
+ * to the descriptor's constant. */
+LBM_API int lbm_ade_set_diffusion(lbm_handle h, const double* field);
+/* Equilibrium of phi (host [Z][Y][X] or NULL for uniform_phi) with the given
+ * velocity (NULL for zero) on every site; ghost sites take the nearest
+ * lattice site's values (setEquilibriumLat, d3q7/common.h:51-61). */
+LBM_API int lbm_ade_init_equilibrium(lbm_handle h, const double* phi, const double* vx, const double* vy,
+									 const double* vz, double uniform_phi);
+/* Scalar populations, host [7][Z(+2)][Y(+2)][X(+2)] in the layouts and
+ * dtypes of lbm_set_populations. */
+LBM_API int lbm_ade_set_populations(lbm_handle h, const void* host, int layout, int dtype);
+LBM_API int lbm_ade_get_populations(lbm_handle h, void* host, int layout, int dtype);
+/* phi [Z][Y][X] of the last lbm_step with LBM_STEP_MACRO (outputMacro of
+ * D3Q7_MACRO_Default, d3q7/macro.h:33-37). */
+LBM_API int lbm_ade_get_phi(lbm_handle h, double* host);
+
 LBM_API const char* lbm_version(void);
 
 #ifdef __cplusplus

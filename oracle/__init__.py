@@ -32,6 +32,7 @@ REFDIR = os.path.join(HERE, "_ref")
 
 COLL = {"CUM": 0, "SRT": 1, "BGK": 2, "MRT": 3}
 EQ = {"EQ": 0, "INV_CUM": 1}
+ADE_COLL = {"SRT": 0, "MRT": 1, "CLBM": 2}
 CUM_2017 = 1
 CUM_ANTIALIAS = 2
 
@@ -191,6 +192,13 @@ class Reference(_Base):
         L.ref_adjoint_data_term.argtypes = [ctypes.c_long, _dp, _dp]
         L.ref_mean_update.restype = ctypes.c_int
         L.ref_mean_update.argtypes = [ctypes.c_int, ctypes.c_long, _vp, _vp, ctypes.c_int]
+        L.ref_aa_ade_run.restype = ctypes.c_int
+        L.ref_aa_ade_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long,
+                                     ctypes.c_long, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, _dp, _dp, _dp, _vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
+                                     _vp, ctypes.c_long, ctypes.c_int]
+        L.ref_ade_collide.restype = ctypes.c_int
+        L.ref_ade_collide.argtypes = [ctypes.c_int, ctypes.c_long, _dp, _dp, _dp, ctypes.c_double]
 
     def aa_run(self, f, geo_map, coll="CUM", eq="INV_CUM", cum_flags=None, nu=0.01, force=(0.0, 0.0, 0.0), inflow=None,
                macro=None, start_iter=0, nsteps=1, nthreads=0, return_time=False):
@@ -235,6 +243,35 @@ class Reference(_Base):
         u = np.ascontiguousarray(u, dtype=np.float64)
         self.lib.ref_srt_adjoint_collision(out.shape[0], _dptr(out), _dptr(u), nu)
         return out
+
+    def aa_ade_run(self, f, geo_map, g, ade_map, coll="CUM", eq="INV_CUM", ade_coll="SRT", nu=0.01, D=0.01,
+                   force=(0.0, 0.0, 0.0), inflow=None, dfield=None, inflow_phi=1.0, macro=None, phi=None, start_iter=0,
+                   nsteps=1):
+        """Coupled flow + D3Q7 scalar steps of cudaLBMKernel<NSE, ADE>
+        (kernels.h:114-196): f [27, Z+2, Y+2, X+2] and g [7, Z+2, Y+2, X+2]
+        updated in place; macro [4, Z, Y, X] and phi [Z, Y, X] outputs of every
+        step (both or neither)."""
+        Z, Y, X = geo_map.shape
+        assert f.shape == (27, Z + 2, Y + 2, X + 2) and f.flags.c_contiguous
+        assert g.shape == (7, Z + 2, Y + 2, X + 2) and g.flags.c_contiguous and g.dtype == f.dtype
+        m = np.ascontiguousarray(geo_map, dtype=np.int16)
+        am = np.ascontiguousarray(ade_map, dtype=np.int16)
+        vx, vy, vz = _profiles(inflow)
+        dfield = None if dfield is None else np.ascontiguousarray(dfield, dtype=np.float64)
+        rc = self.lib.ref_aa_ade_run(_prec(f.dtype), COLL[coll], EQ[eq], ADE_COLL[ade_coll], X, Y, Z, _ptr(f), _ptr(m), nu,
+                                     *force, _dptr(vx), _dptr(vy), _dptr(vz), _ptr(macro), _ptr(g), _ptr(am), D,
+                                     _dptr(dfield), inflow_phi, _ptr(phi), start_iter, nsteps)
+        if rc != 0:
+            raise RuntimeError(f"ref_aa_ade_run failed with {rc}")
+        return f, g
+
+    def ade_collide(self, g, v, D, ade_coll="SRT"):
+        """Per-site D3Q7 collision of g [n, 7] in place with velocities v [n, 3]; returns phi [n]."""
+        assert g.dtype == np.float64 and g.flags.c_contiguous and g.shape[1] == 7
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        phi = np.zeros(g.shape[0])
+        self.lib.ref_ade_collide(ADE_COLL[ade_coll], g.shape[0], _dptr(g), _dptr(v), _dptr(phi), D)
+        return phi
 
     def mean_update(self, macro, stats, counter):
         """D3Q27_MACRO_Mean::outputMacro (macro.h:117-171): one update of the

@@ -53,6 +53,14 @@
 	#include "lbm3d/d3q27/streaming_AB.h"
 #else
 	#include "lbm3d/d3q27/streaming_AA.h"
+	// the D3Q7 advection-diffusion operators (coupled to the flow in the A-A build)
+	#include "lbm3d/d3q7/bc.h"
+	#include "lbm3d/d3q7/col_clbm.h"
+	#include "lbm3d/d3q7/col_mrt.h"
+	#include "lbm3d/d3q7/col_srt.h"
+	#include "lbm3d/d3q7/eq.h"
+	#include "lbm3d/d3q7/macro.h"
+	#include "lbm3d/d3q7/streaming_AA.h"
 #endif
 
 namespace {
@@ -260,22 +268,22 @@ bool map_is_supported(const short* map, long n)
 	return true;
 }
 
-template <typename DREAL>
+template <typename DREAL, int Q = 27>
 void canonical_to_ref(const DREAL* src, DREAL* dst, long X, long Y, long Z)
 {
 	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
-	for (int q = 0; q < 27; q++)
+	for (int q = 0; q < Q; q++)
 		for (long z = 0; z < Z + 2; z++)
 			for (long y = 0; y < Y + 2; y++)
 				for (long x = 0; x < X + 2; x++)
 					dst[q * XYZ + (x * (Z + 2) + z) * (Y + 2) + y] = src[q * XYZ + (z * (Y + 2) + y) * (X + 2) + x];
 }
 
-template <typename DREAL>
+template <typename DREAL, int Q = 27>
 void ref_to_canonical(const DREAL* src, DREAL* dst, long X, long Y, long Z)
 {
 	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
-	for (int q = 0; q < 27; q++)
+	for (int q = 0; q < Q; q++)
 		for (long z = 0; z < Z + 2; z++)
 			for (long y = 0; y < Y + 2; y++)
 				for (long x = 0; x < X + 2; x++)
@@ -420,6 +428,244 @@ int dispatch_coll(int coll, long X, long Y, long Z, void* f, const short* map, d
 	}
 }
 
+#ifndef AB_PATTERN
+// ---- coupled D3Q7 advection-diffusion (State_NSE_ADE) ------------------------
+// Kernel data of the scalar: ADE_Data + ADE_Data_ConstInflow (lbm_data.h:211-262)
+// over the harness indexer.  The phase-transfer arrays are not provided; the
+// harness rejects maps that would read them.
+template <typename TRAITS>
+struct HarnessAdeData : HarnessData<TRAITS>
+{
+	using idx = typename TRAITS::idx;
+	using dreal = typename TRAITS::dreal;
+
+	const dreal* dcoef = nullptr;  // per-site diffusion [Z][Y][X] or null
+	dreal inflow_phi = 1;
+	dreal phiTransferCoefficient = 0;
+
+	dreal diffusionCoefficient(idx x, idx y, idx z) const
+	{
+		return dcoef ? dcoef[(z * this->ny + y) * this->nx + x] : this->lbmViscosity;
+	}
+
+	bool& phiTransferDirection(int, idx, idx, idx)
+	{
+		static bool none = false;
+		g_unsupported_hit = 1;
+		return none;
+	}
+
+	template <typename LBM_KS>
+	void inflow(LBM_KS& KS, idx, idx, idx)
+	{
+		KS.phi = inflow_phi;
+	}
+};
+
+template <typename DREAL, typename COLL>
+using HarnessAdeConfig = LBM_CONFIG<
+	HarnessTraits<DREAL>,
+	D3Q7_KernelStruct,
+	HarnessAdeData<HarnessTraits<DREAL>>,
+	COLL,
+	D3Q7_EQ<HarnessTraits<DREAL>>,
+	D3Q7_STREAMING<HarnessTraits<DREAL>>,
+	D3Q7_BC_All,
+	D3Q7_MACRO_Default<HarnessTraits<DREAL>>>;
+
+// one site of the coupled kernel cudaLBMKernel<NSE, ADE> (kernels.h:138-195)
+template <typename NSE, typename ADE>
+inline void coupled_update(typename NSE::DATA& SD, typename ADE::DATA& AD, long x, long y, long z, bool output_macro)
+{
+	using dreal = typename NSE::TRAITS::dreal;
+	const auto nse_map = SD.map(x, y, z);
+	const auto ade_map = AD.map(x, y, z);
+	long xp, xm, yp, ym, zp, zm;
+	init_indices<NSE>(SD, nse_map, x, y, z, xp, xm, yp, ym, zp, zm);
+
+	typename NSE::template KernelStruct<dreal> KS;
+	NSE::MACRO::copyQuantities(SD, KS, x, y, z);
+	NSE::MACRO::template computeForcing<typename NSE::BC>(SD, KS, xm, x, xp, ym, y, yp, zm, z, zp);
+	NSE::BC::preCollision(SD, KS, nse_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (NSE::BC::doCollision(nse_map))
+		NSE::COLL::collision(KS);
+	NSE::BC::postCollision(SD, KS, nse_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (output_macro)
+		NSE::MACRO::outputMacro(SD, KS, x, y, z);
+
+	typename ADE::template KernelStruct<dreal> AKS;
+	AKS.vx = KS.vx;
+	AKS.vy = KS.vy;
+	AKS.vz = KS.vz;
+	ADE::MACRO::copyQuantities(AD, AKS, x, y, z);
+	ADE::BC::preCollision(AD, AKS, ade_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (ADE::BC::doCollision(ade_map))
+		ADE::COLL::collision(AKS);
+	ADE::BC::postCollision(AD, AKS, ade_map, xm, x, xp, ym, y, yp, zm, z, zp);
+	if (output_macro)
+		ADE::MACRO::outputMacro(AD, AKS, x, y, z);
+}
+
+// scalar site types whose update depends on nothing but the site's own slots
+// (the outflow and phase-transfer types read slots other sites write)
+bool ade_map_is_supported(const short* map, long n)
+{
+	for (long i = 0; i < n; i++) {
+		const short g = map[i];
+		if (!(g == 0 || g == 1 || g == 2 || g == 3 || g == 7 || g == 9 || g == 10 || (g >= 12 && g <= 17)))
+			return false;
+	}
+	return true;
+}
+
+template <typename NSE, typename ADE>
+int run_aa_ade(long X, long Y, long Z, typename NSE::TRAITS::dreal* f_canonical, const short* map, double nu, double fx,
+			   double fy, double fz, const double* in_vx, const double* in_vy, const double* in_vz,
+			   typename NSE::TRAITS::dreal* macro, typename NSE::TRAITS::dreal* g_canonical, const short* ade_map, double D,
+			   const double* dfield, double inflow_phi, typename NSE::TRAITS::dreal* phi, long start_iter, int nsteps)
+{
+	using dreal = typename NSE::TRAITS::dreal;
+	const long n = X * Y * Z;
+	if (!map_is_supported(map, n) || map_is_order_dependent(map, n) || !ade_map_is_supported(ade_map, n))
+		return -2;
+	if ((macro == nullptr) != (phi == nullptr))
+		return -1;
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+	std::vector<dreal> df(27 * XYZ), dg(7 * XYZ);
+	canonical_to_ref<dreal, 27>(f_canonical, df.data(), X, Y, Z);
+	canonical_to_ref<dreal, 7>(g_canonical, dg.data(), X, Y, Z);
+	std::vector<dreal> pvx, pvy, pvz, pd;
+	auto convert = [](const double* src, long m, std::vector<dreal>& dst) -> const dreal*
+	{
+		if (!src)
+			return nullptr;
+		dst.resize(m);
+		for (long i = 0; i < m; i++)
+			dst[i] = (dreal) src[i];
+		return dst.data();
+	};
+
+	typename NSE::DATA SD;
+	SD.nx = X;
+	SD.ny = Y;
+	SD.nz = Z;
+	SD.XYZ = XYZ;
+	SD.lbmViscosity = (dreal) nu;
+	SD.fx = (dreal) fx;
+	SD.fy = (dreal) fy;
+	SD.fz = (dreal) fz;
+	SD.dfs[df_cur] = df.data();
+	SD.dmacro = macro;
+	SD.dmap = map;
+	SD.inflow_vx = convert(in_vx, Y * Z, pvx);
+	SD.inflow_vy = convert(in_vy, Y * Z, pvy);
+	SD.inflow_vz = convert(in_vz, Y * Z, pvz);
+
+	typename ADE::DATA AD;
+	AD.nx = X;
+	AD.ny = Y;
+	AD.nz = Z;
+	AD.XYZ = XYZ;
+	AD.lbmViscosity = (dreal) D;
+	AD.dfs[df_cur] = dg.data();
+	AD.dmacro = phi;
+	AD.dmap = ade_map;
+	AD.dcoef = convert(dfield, n, pd);
+	AD.inflow_phi = (dreal) inflow_phi;
+
+	g_unsupported_hit = 0;
+	for (int s = 0; s < nsteps; s++) {
+		SD.even_iter = AD.even_iter = ((start_iter + s) % 2) == 0;
+		const bool output_macro = macro != nullptr;
+		for (long x = 0; x < X; x++)
+			for (long z = 0; z < Z; z++)
+				for (long y = 0; y < Y; y++)
+					coupled_update<NSE, ADE>(SD, AD, x, y, z, output_macro);
+	}
+	ref_to_canonical<dreal, 27>(SD.dfs[df_cur], f_canonical, X, Y, Z);
+	ref_to_canonical<dreal, 7>(AD.dfs[df_cur], g_canonical, X, Y, Z);
+	return g_unsupported_hit ? -3 : 0;
+}
+
+template <typename T>
+struct TypeTag
+{
+	using type = T;
+};
+
+template <typename DREAL, typename NSE_COLL, typename EQ>
+int ade_dispatch(int ade_coll, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy, double fz,
+				 const double* vx, const double* vy, const double* vz, void* macro, void* g, const short* ade_map, double D,
+				 const double* dfield, double inflow_phi, void* phi, long it, int ns)
+{
+	using T = HarnessTraits<DREAL>;
+	using NSE = HarnessConfig<DREAL, NSE_COLL, EQ>;
+	auto run = [&](auto ade_tag) -> int
+	{
+		using ADE = HarnessAdeConfig<DREAL, typename decltype(ade_tag)::type>;
+		return run_aa_ade<NSE, ADE>(X, Y, Z, (DREAL*) f, map, nu, fx, fy, fz, vx, vy, vz, (DREAL*) macro, (DREAL*) g, ade_map, D,
+									dfield, inflow_phi, (DREAL*) phi, it, ns);
+	};
+	switch (ade_coll) {
+		case 0:
+			return run(TypeTag<D3Q7_SRT<T>>{});
+		case 1:
+			return run(TypeTag<D3Q7_MRT<T>>{});
+		case 2:
+			return run(TypeTag<D3Q7_CLBM<T>>{});
+		default:
+			return -1;
+	}
+}
+
+template <typename DREAL, typename EQ>
+int ade_dispatch_nse(int coll, int ade_coll, long X, long Y, long Z, void* f, const short* map, double nu, double fx, double fy,
+					 double fz, const double* vx, const double* vy, const double* vz, void* macro, void* g, const short* ade_map,
+					 double D, const double* dfield, double inflow_phi, void* phi, long it, int ns)
+{
+	using T = HarnessTraits<DREAL>;
+	switch (coll) {
+		case 0:
+			return ade_dispatch<DREAL, D3Q27_CUM<T, EQ>, EQ>(ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, g, ade_map, D,
+															 dfield, inflow_phi, phi, it, ns);
+		case 1:
+			return ade_dispatch<DREAL, D3Q27_SRT<T, EQ>, EQ>(ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, g, ade_map, D,
+															 dfield, inflow_phi, phi, it, ns);
+		case 2:
+			return ade_dispatch<DREAL, D3Q27_BGK<T, EQ>, EQ>(ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, g, ade_map, D,
+															 dfield, inflow_phi, phi, it, ns);
+		case 3:
+			return ade_dispatch<DREAL, D3Q27_MRT<T, EQ>, EQ>(ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz, macro, g, ade_map, D,
+															 dfield, inflow_phi, phi, it, ns);
+		default:
+			return -1;
+	}
+}
+
+// per-site scalar collision: computeDensityAndVelocity then COLL::collision
+// (d3q7/common.h:15-26, col_*.h) on n sites g[n][7] with velocities v[n][3]
+template <typename DREAL, typename COLL>
+int ade_collide_typed(long n, DREAL* g, const double* v, DREAL* phi_out, double D)
+{
+	for (long s = 0; s < n; s++) {
+		D3Q7_KernelStruct<DREAL> KS;
+		for (int q = 0; q < 7; q++)
+			KS.f[q] = g[s * 7 + q];
+		KS.vx = (DREAL) v[3 * s];
+		KS.vy = (DREAL) v[3 * s + 1];
+		KS.vz = (DREAL) v[3 * s + 2];
+		KS.lbmViscosity = (DREAL) D;
+		COLL::computeDensityAndVelocity(KS);
+		if (phi_out)
+			phi_out[s] = KS.phi;
+		COLL::collision(KS);
+		for (int q = 0; q < 7; q++)
+			g[s * 7 + q] = KS.f[q];
+	}
+	return 0;
+}
+#endif	// !AB_PATTERN
+
 // equilibrium of one site through the collision's inherited setEquilibriumLat
 // (common.h:127-158), which takes rho and u in `real` (double)
 template <typename DREAL, typename EQ>
@@ -549,6 +795,56 @@ int mean_update_typed(long n, const DREAL* macro4, DREAL* stats9, int counter)
 }  // namespace
 
 extern "C" {
+
+#ifndef AB_PATTERN
+// Coupled flow + D3Q7 scalar steps (cudaLBMKernel<NSE, ADE>, kernels.h:114-196),
+// single-threaded in the reference loop order.  prec, coll, eq, f, map,
+// inflow, macro as ref_aa_run; ade_coll: 0 D3Q7_SRT, 1 D3Q7_MRT, 2 D3Q7_CLBM;
+// g: [7][Z+2][Y+2][X+2] scalar populations, updated in place; ade_map:
+// [Z][Y][X] scalar GEO types; D: diffusion coefficient, dfield: per-site
+// [Z][Y][X] or NULL; inflow_phi: phi of GEO_INFLOW sites; phi: [Z][Y][X] output
+// (together with macro) or NULL.  Returns -2 for maps with order-dependent or
+// unprovided site types.
+int ref_aa_ade_run(int prec, int coll, int eq, int ade_coll, long X, long Y, long Z, void* f, const short* map, double nu,
+				   double fx, double fy, double fz, const double* vx, const double* vy, const double* vz, void* macro, void* g,
+				   const short* ade_map, double D, const double* dfield, double inflow_phi, void* phi, long start_iter,
+				   int nsteps)
+{
+	if (prec == 0) {
+		if (eq == 0)
+			return ade_dispatch_nse<double, D3Q27_EQ<HarnessTraits<double>>>(coll, ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy,
+																			 vz, macro, g, ade_map, D, dfield, inflow_phi, phi,
+																			 start_iter, nsteps);
+		return ade_dispatch_nse<double, D3Q27_EQ_INV_CUM<HarnessTraits<double>>>(coll, ade_coll, X, Y, Z, f, map, nu, fx, fy, fz,
+																				 vx, vy, vz, macro, g, ade_map, D, dfield,
+																				 inflow_phi, phi, start_iter, nsteps);
+	}
+	if (eq == 0)
+		return ade_dispatch_nse<float, D3Q27_EQ<HarnessTraits<float>>>(coll, ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy, vz,
+																	   macro, g, ade_map, D, dfield, inflow_phi, phi, start_iter,
+																	   nsteps);
+	return ade_dispatch_nse<float, D3Q27_EQ_INV_CUM<HarnessTraits<float>>>(coll, ade_coll, X, Y, Z, f, map, nu, fx, fy, fz, vx, vy,
+																		   vz, macro, g, ade_map, D, dfield, inflow_phi, phi,
+																		   start_iter, nsteps);
+}
+
+// Per-site scalar collision on n sites (FP64): g[n][7] in place, v[n][3]
+// velocities, phi_out[n] the pre-collision phi or NULL.
+int ref_ade_collide(int ade_coll, long n, double* g, const double* v, double* phi_out, double D)
+{
+	using T = HarnessTraits<double>;
+	switch (ade_coll) {
+		case 0:
+			return ade_collide_typed<double, D3Q7_SRT<T>>(n, g, v, phi_out, D);
+		case 1:
+			return ade_collide_typed<double, D3Q7_MRT<T>>(n, g, v, phi_out, D);
+		case 2:
+			return ade_collide_typed<double, D3Q7_CLBM<T>>(n, g, v, phi_out, D);
+		default:
+			return -1;
+	}
+}
+#endif
 
 // One statistics update of D3Q27_MACRO_Mean::outputMacro (macro.h:117-171) on
 // n sites: macro4 [4][n] (rho, vx, vy, vz) of the step, stats9 [9][n] (mean

@@ -41,6 +41,16 @@ enum : std::uint8_t
 };
 #endif
 
+// KernelStruct - D3Q7 (field set and defaults as defs.h:244-252)
+template <typename REAL>
+struct D3Q7_KernelStruct
+{
+	static constexpr int Q = 7;
+	REAL f[Q];
+	REAL vz = 0, vx = 0, vy = 0;
+	REAL phi = 1.0, lbmViscosity = 1.0;
+};
+
 // KernelStruct - D3Q27 (field set and defaults as defs.h:257-263)
 template <typename REAL>
 struct D3Q27_KernelStruct

@@ -9,6 +9,7 @@
 #include "ab_kernels.cuh"
 #include "coll_params.cuh"
 #include "aa_tile.cuh"
+#include "ade.cuh"
 #include "ensemble.cuh"
 #include "launch.h"
 
@@ -164,6 +165,74 @@ struct StorageUnit
 		if (L.odd)
 			return general ? launch_one<COLL, CUMF, true, true>(L, a) : launch_one<COLL, CUMF, true, false>(L, a);
 		return general ? launch_one<COLL, CUMF, false, true>(L, a) : launch_one<COLL, CUMF, false, false>(L, a);
+	}
+
+	// ---- coupled flow + D3Q7 scalar step (ade.cuh)
+	template <int COLL, int CUMF, bool ODD, bool GENERAL>
+	static cudaError_t ade_one(const StepLaunch& L, const StepArgs<T, R>& a, const AdeArgs<R>& d)
+	{
+		if (L.blocks_out)  // one partial-sum slot per warp
+			*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z * ((L.block.x * L.block.y) / 32);
+		if (L.dry_run)
+			return cudaSuccess;
+		if (L.macro || L.partials || d.phi)
+			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, true, direct_minb<R, COLL, CUMF, ODD, GENERAL, true>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a, d);
+		else
+			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, false, direct_minb<R, COLL, CUMF, ODD, GENERAL, false>()>
+				<<<L.grid, L.block, 0, L.stream>>>(a, d);
+		return cudaGetLastError();
+	}
+
+	template <int COLL, int CUMF>
+	static cudaError_t ade_parity(const StepLaunch& L, const StepArgs<T, R>& a, const AdeArgs<R>& d)
+	{
+		const bool general = L.map != nullptr;
+		if (L.odd)
+			return general ? ade_one<COLL, CUMF, true, true>(L, a, d) : ade_one<COLL, CUMF, true, false>(L, a, d);
+		return general ? ade_one<COLL, CUMF, false, true>(L, a, d) : ade_one<COLL, CUMF, false, false>(L, a, d);
+	}
+
+	static cudaError_t ade_step(const StepLaunch& L)
+	{
+		if constexpr (sizeof(T) != sizeof(R)) {
+			(void) L;
+			return cudaErrorNotSupported;
+		}
+		else {
+			if (!L.ade)
+				return cudaErrorInvalidValue;
+			const StepArgs<T, R> a = step_args(L);
+			AdeArgs<R> d;
+			d.g = (R*) L.ade->g;
+			d.map = L.ade->map;
+			d.dcoef = (const R*) L.ade->dcoef;
+			d.D = (R) L.ade->D;
+			d.inflow_phi = (R) L.ade->inflow_phi;
+			d.phi = (R*) L.ade->phi;
+			d.coll = L.ade->coll;
+			switch (L.coll) {
+				case COLL_CUM:
+					switch (L.cum_flags) {
+						case 0:
+							return ade_parity<COLL_CUM, 0>(L, a, d);
+						case CUM_ANTIALIAS:
+							return ade_parity<COLL_CUM, CUM_ANTIALIAS>(L, a, d);
+						case CUM_2017 | CUM_ANTIALIAS:
+							return ade_parity<COLL_CUM, CUM_2017 | CUM_ANTIALIAS>(L, a, d);
+						default:
+							return cudaErrorInvalidValue;
+					}
+				case COLL_SRT:
+					return ade_parity<COLL_SRT, 0>(L, a, d);
+				case COLL_BGK:
+					return ade_parity<COLL_BGK, 0>(L, a, d);
+				case COLL_MRT:
+					return ade_parity<COLL_MRT, 0>(L, a, d);
+				default:
+					return cudaErrorInvalidValue;
+			}
+		}
 	}
 
 	static StepArgs<T, R> step_args(const StepLaunch& L)
@@ -489,6 +558,7 @@ cudaError_t StorageUnit<S>::unpack(const Geometry& g, const void* dense, int dty
 									   sizeof(EnsMember<typename S::T, typename S::R>),                              \
 									   &StorageUnit<S>::ens_entry,                                                   \
 									   &StorageUnit<S>::ens_step,                                                    \
+									   &StorageUnit<S>::ade_step,                                                    \
 									   (int) sizeof(typename S::R),                                                  \
 									   (int) sizeof(typename S::T),                                                  \
 									   NAME};                                                                        \

@@ -14,6 +14,16 @@
 namespace lbm {
 struct AdjointState;  // lbm_adjoint.cu
 void adjoint_free(AdjointState*);
+
+// coupled D3Q7 scalar (lbm_ade.cu)
+struct AdeState
+{
+	AdeLaunch launch{};				// device buffers and parameters of the coupled step
+	std::vector<uint8_t> map_host;	// host copy of the accepted ADE map
+	void* phi_buf = nullptr;		// phi of the last observation step
+	bool phi_valid = false;
+};
+void ade_free(AdeState*);
 }  // namespace lbm
 
 struct lbm_lattice
@@ -55,6 +65,7 @@ struct lbm_lattice
 	void* stats = nullptr;		// D3Q27_MACRO_Mean fields [9][sites], compute type
 	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
+	lbm::AdeState* ade = nullptr;			 // coupled D3Q7 scalar, or null
 	static constexpr int GRAPH_STEPS = 16;
 
 	long long sites() const

@@ -69,6 +69,19 @@ struct StepLaunch
 	const unsigned* split_tiles;
 	long long split_n[2];
 	int split_tiles_x;
+	const struct AdeLaunch* ade;  // coupled D3Q7 scalar (ade.cuh), or null
+};
+
+// the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)
+struct AdeLaunch
+{
+	void* g;			  // compute-type [7][sq] populations, the flow lattice's geometry
+	const uint8_t* map;	  // ADE site types [Z][Y][X]
+	const void* dcoef;	  // compute-type per-site diffusion coefficient, or null
+	double D;			  // diffusion coefficient when dcoef is null
+	double inflow_phi;
+	void* phi;			  // compute-type [Z][Y][X] output of observation steps, or null
+	int coll;			  // 0 SRT, 1 MRT, 2 central-moment (CLBM)
 };
 
 // step kernel variants: one thread per site with direct loads, or the
@@ -115,6 +128,9 @@ struct StorageOps
 	size_t ens_entry_bytes;
 	void (*ens_entry)(void* dst, const Geometry&, const CollParamsD&, long long tile0);
 	cudaError_t (*ens_step)(const EnsLaunch&);
+	// one coupled flow + D3Q7 scalar step (L.ade set); cudaErrorNotSupported
+	// for storages whose element is not the compute type
+	cudaError_t (*ade_step)(const StepLaunch&);
 	int compute_size;  // sizeof the compute type (8 or 4)
 	int elem_size;	   // sizeof the storage element
 	const char* name;

@@ -163,7 +163,13 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.split_n[1] = h->split_n[1];
 	L.split_tiles_x = h->split_tiles_x;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
-	const cudaError_t err = ab ? h->ops->ab_step(L) : h->ops->step(L);
+	if (h->ade) {
+		h->ade->launch.phi = macro ? h->ade->phi_buf : nullptr;
+		L.ade = &h->ade->launch;
+		if (!dry_run)
+			h->ade->phi_valid = macro;
+	}
+	const cudaError_t err = h->ade ? h->ops->ade_step(L) : (ab ? h->ops->ab_step(L) : h->ops->step(L));
 	if (err != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(err));
 	if (dry_run)
@@ -347,6 +353,7 @@ int lbm_destroy(lbm_handle h)
 		cudaStreamSynchronize(h->stream);
 	h->drop_graph();
 	lbm::adjoint_free(h->adjoint);
+	lbm::ade_free(h->ade);
 	cudaFree(h->g.f);
 	cudaFree(h->f_out);
 	cudaFree(h->split_tiles);
@@ -911,6 +918,8 @@ int lbm_set_streaming(lbm_handle h, int streaming)
 		return fail(LBM_ERR_INVALID, "unknown streaming pattern %d", streaming);
 	if (streaming == h->streaming)
 		return LBM_OK;
+	if (h->ade)
+		return fail(LBM_ERR_UNSUPPORTED, "the coupled scalar runs on A-A lattices only (lbm_ade_disable first)");
 	if (streaming == LBM_STREAMING_AA) {
 		for (uint8_t g : h->map_host)
 			if (!site_type_supported(g))

@@ -216,6 +216,8 @@ int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64
 		return afail(LBM_ERR_CUDA, "cudaSetDevice(%d) failed", h->d.device);
 	if (h->d.collision != LBM_COLL_SRT || h->d.equilibrium != LBM_EQ_SECOND_ORDER)
 		return afail(LBM_ERR_UNSUPPORTED, "the adjoint is provided for the SRT collision with D3Q27_EQ (LBM_EQ_SECOND_ORDER)");
+	if (h->ade)
+		return afail(LBM_ERR_UNSUPPORTED, "the adjoint does not cover a coupled scalar (lbm_ade_disable first)");
 	if (h->streaming != LBM_STREAMING_AA)
 		return afail(LBM_ERR_UNSUPPORTED, "the adjoint is provided for the A-A streaming pattern");
 	if (h->d.storage != LBM_STORE_F64 && h->d.storage != LBM_STORE_F32)

@@ -75,6 +75,8 @@ int lbm_checkpoint_save(lbm_handle h, const char* path)
 		return cfail(LBM_ERR_INVALID, "null argument");
 	if (cudaSetDevice(h->d.device) != cudaSuccess)
 		return cfail(LBM_ERR_CUDA, "cudaSetDevice(%d) failed", h->d.device);
+	if (h->ade)
+		return cfail(LBM_ERR_UNSUPPORTED, "checkpoints do not hold a coupled scalar (lbm_ade_disable first)");
 	CheckpointHeader hd{};
 	memcpy(hd.magic, MAGIC, sizeof(MAGIC));
 	hd.version = VERSION;
@@ -133,6 +135,8 @@ int lbm_checkpoint_load(lbm_handle h, const char* path)
 		return cfail(LBM_ERR_INVALID, "null argument");
 	if (cudaSetDevice(h->d.device) != cudaSuccess)
 		return cfail(LBM_ERR_CUDA, "cudaSetDevice(%d) failed", h->d.device);
+	if (h->ade)
+		return cfail(LBM_ERR_UNSUPPORTED, "checkpoints do not hold a coupled scalar (lbm_ade_disable first)");
 	File in;
 	in.f = fopen(path, "rb");
 	if (!in.f)

@@ -19,7 +19,7 @@ import numpy as np
 from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
     COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
-    GEO, KERNEL_DIRECT, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
+    ADE_CLBM, ADE_GEO, ADE_MRT, ADE_SRT, GEO, KERNEL_DIRECT, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
     STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
 
 __all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute", "Actions",
@@ -181,6 +181,53 @@ class LBM:
         _abi.check(self.lib.lbm_get_statistics(self.h, _abi.dptr(out), ctypes.byref(n)))
         cov = out[3:] / max(n.value, 1)
         return out[:3], cov, n.value
+
+    # -- coupled D3Q7 scalar (lbm_ade_*) ---------------------------------
+    def ade_enable(self, diffusion, collision=ADE_SRT, inflow_phi=1.0):
+        """Advance a scalar phi with the flow in every step (kernels.h:114-196)."""
+        d = _abi.lbm_ade_desc(int(collision), float(diffusion), float(inflow_phi))
+        _abi.check(self.lib.lbm_ade_enable(self.h, ctypes.byref(d)))
+
+    def ade_disable(self):
+        _abi.check(self.lib.lbm_ade_disable(self.h))
+
+    def ade_set_map(self, geo_map):
+        m = np.ascontiguousarray(geo_map, dtype=np.uint8)
+        assert m.shape == self.shape, f"map shape {m.shape} != {self.shape}"
+        _abi.check(self.lib.lbm_ade_set_map(self.h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+
+    def ade_set_diffusion(self, field=None):
+        """Per-site diffusion coefficient [Z][Y][X]; None returns to the constant."""
+        a = None if field is None else np.ascontiguousarray(field, dtype=np.float64)
+        if a is not None:
+            assert a.shape == self.shape
+        _abi.check(self.lib.lbm_ade_set_diffusion(self.h, _abi.dptr(a)))
+
+    def ade_init_equilibrium(self, phi=None, vx=None, vy=None, vz=None, uniform_phi=0.0):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (phi, vx, vy, vz)]
+        _abi.check(self.lib.lbm_ade_init_equilibrium(self.h, *[_abi.dptr(a) for a in arrs], float(uniform_phi)))
+
+    def _ade_shape(self, layout):
+        g = 2 if layout == LAYOUT_GHOST else 0
+        return (7, self.Z + g, self.Y + g, self.X + g)
+
+    def ade_set_populations(self, g, layout=LAYOUT_GHOST):
+        g = np.ascontiguousarray(g)
+        assert g.shape == self._ade_shape(layout) and g.dtype in (np.float64, np.float32)
+        _abi.check(self.lib.lbm_ade_set_populations(self.h, g.ctypes.data_as(ctypes.c_void_p), layout,
+                                                    0 if g.dtype == np.float64 else 1))
+
+    def ade_get_populations(self, layout=LAYOUT_GHOST, dtype=np.float64):
+        out = np.empty(self._ade_shape(layout), dtype=dtype)
+        _abi.check(self.lib.lbm_ade_get_populations(self.h, out.ctypes.data_as(ctypes.c_void_p), layout,
+                                                    0 if out.dtype == np.float64 else 1))
+        return out
+
+    def ade_phi(self):
+        """phi [Z][Y][X] of the last step with macro=True."""
+        out = np.empty(self.shape, np.float64)
+        _abi.check(self.lib.lbm_ade_get_phi(self.h, _abi.dptr(out)))
+        return out
 
     def save_checkpoint(self, path):
         """Write the state (populations as stored, map, inflow, iteration) to ``path``."""

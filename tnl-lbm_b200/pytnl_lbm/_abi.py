@@ -18,6 +18,11 @@ STEP_MACRO, STEP_SUMS = 1, 2
 KERNEL_DIRECT, KERNEL_TILE, KERNEL_SPLIT = 0, 1, 3
 STREAMING_AA, STREAMING_AB = 0, 1
 STATUS_TIMEOUT = 1
+ADE_SRT, ADE_MRT, ADE_CLBM = 0, 1, 2
+
+# scalar site types of D3Q7_BC_All (include/lbm3d/d3q7/bc.h:17-36) that the coupled step provides
+ADE_GEO = dict(FLUID=0, WALL=1, WALL_BODY=2, SOLID=3, INFLOW=7, PERIODIC=9, NOTHING=10, SYM_TOP=12, SYM_BOTTOM=13,
+               SYM_LEFT=14, SYM_RIGHT=15, SYM_BACK=16, SYM_FRONT=17)
 
 # GEO site types of D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43)
 GEO = dict(FLUID=0, WALL=1, INFLOW=2, INFLOW_LEFT=3, INFLOW_BB_LEFT=4, INFLOW_EQ_LEFT=5, OUTFLOW_EQ=6,
@@ -51,6 +56,10 @@ class lbm_ensemble_desc(ctypes.Structure):
                 ("viscosity", ctypes.POINTER(ctypes.c_double)), ("storage", ctypes.c_int32),
                 ("collision", ctypes.c_int32), ("cum_flags", ctypes.c_int32), ("equilibrium", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("use_graphs", ctypes.c_int32)]
+
+
+class lbm_ade_desc(ctypes.Structure):
+    _fields_ = [("collision", ctypes.c_int32), ("diffusion", ctypes.c_double), ("inflow_phi", ctypes.c_double)]
 
 
 lbm_handle = ctypes.c_void_p
@@ -95,6 +104,14 @@ SIGNATURES = {
                                            ctypes.c_int32, _dp, ctypes.c_double, _dp]),
     "lbm_adjoint_backward": (ctypes.c_int, [_H, ctypes.c_double, _dp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "lbm_adjoint_release": (ctypes.c_int, [_H]),
+    "lbm_ade_enable": (ctypes.c_int, [_H, ctypes.POINTER(lbm_ade_desc)]),
+    "lbm_ade_disable": (ctypes.c_int, [_H]),
+    "lbm_ade_set_map": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_uint8)]),
+    "lbm_ade_set_diffusion": (ctypes.c_int, [_H, _dp]),
+    "lbm_ade_init_equilibrium": (ctypes.c_int, [_H, _dp, _dp, _dp, _dp, ctypes.c_double]),
+    "lbm_ade_set_populations": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lbm_ade_get_populations": (ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lbm_ade_get_phi": (ctypes.c_int, [_H, _dp]),
     "lbm_ensemble_create": (ctypes.c_int, [ctypes.POINTER(lbm_ensemble_desc), ctypes.POINTER(ctypes.c_void_p)]),
     "lbm_ensemble_destroy": (ctypes.c_int, [_H]),
     "lbm_ensemble_init_taylor_green": (ctypes.c_int, [_H, ctypes.c_double, ctypes.c_double]),
