@@ -43,6 +43,10 @@ def workload_spec(name):
     if name == "duct":
         return dict(workload="duct 512x128x128, walls + parabolic inlet u_max=0.04 + fixed-density outlet, Re=2000",
                     X=512, Y=128, Z=128, kind="duct", cum_flags=0)
+    if name == "duct_ade":
+        return dict(workload="duct 512x128x128 as 'duct' with a coupled D3Q7 scalar (central-moment collision, D = nu, "
+                             "phi = 1 at the inlet, symmetry outlet, bounce-back walls)",
+                    X=512, Y=128, Z=128, kind="duct", cum_flags=0, ade=True)
     if name == "tgv512":
         return dict(workload="periodic Taylor-Green vortex 512^3, U0=0.05, Re=1600", X=512, Y=512, Z=512, kind="tgv",
                     cum_flags=3)
@@ -372,6 +376,12 @@ def make_lattice(pl, spec, storage, device, kernel="direct"):
         lat.set_map(m)
         lat.set_inflow(prof, None, None)
         lat.init_equilibrium(*fields)
+        if spec.get("ade"):
+            # scalar types from the flow map: inlet -> INFLOW, outlet -> SYM_RIGHT, walls and rims alike
+            am = np.choose(m, [0, 1, 0, 7, 0, 0, 15, 0, 0, 9, 10]).astype(np.uint8)
+            lat.ade_enable(nu, collision=pl.ADE_CLBM, inflow_phi=1.0)
+            lat.ade_set_map(am)
+            lat.ade_init_equilibrium(uniform_phi=0.0)
         return lat, prof
     nu = 0.05 * (X / (2 * math.pi)) / 1600.0
     lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
@@ -499,7 +509,9 @@ def run_ours(args):
 
     # roofline of the step kernel (the only kernel of the timed region)
     bpe = BYTES_PER_ELEM[args.storage]
-    alg_bytes = 2 * 27 * bpe * sites
+    # populations read and written once per update; a coupled scalar adds its 7
+    bytes_per_site = 2 * 27 * bpe + (2 * 7 * bpe if spec.get("ade") else 0)
+    alg_bytes = bytes_per_site * sites
     achieved = alg_bytes / (secs / args.steps) / 1e9
     peak, peak_kind = read_peaks()
     traffic = read_traffic(f"{args.workload}_{args.storage}")
@@ -526,7 +538,7 @@ def run_ours(args):
 
     # FP16 / BF16 shifted storage on the same workload (the precision trade)
     variants = {}
-    if args.variants and args.storage == "f32":
+    if args.variants and args.storage == "f32" and not spec.get("ade"):
         lat.close()
         for st in ("f16s", "bf16s"):
             vl, _ = make_lattice(pl, spec, st, local, args.kernel)
@@ -576,7 +588,7 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "algorithmic_bytes_per_site_update": 2 * 27 * bpe,
+                         "algorithmic_bytes_per_site_update": bytes_per_site,
                          "achieved_vs_8TBs_spec": round(achieved / 8000.0, 4)},
             "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 48, "steps": e2e_steps,
@@ -588,7 +600,7 @@ def run_ours(args):
             line["storage_variants"] = variants
         if precision is not None:
             line["precision"] = precision
-        if args.cpu_baseline and world == 1:
+        if args.cpu_baseline and world == 1 and not spec.get("ade"):
             line["cpu_baseline"] = cpu_baseline(spec, args)
     if dist is not None:
         dist.barrier()
@@ -706,7 +718,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="duct", choices=["duct", "tgv512", "tgv64", "ensemble64", "ensemble_small", "adjoint"])
+    ap.add_argument("--workload", default="duct", choices=["duct", "duct_ade", "tgv512", "tgv64", "ensemble64", "ensemble_small", "adjoint"])
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -254,6 +254,10 @@ __device__ __forceinline__ void ade_write(R* __restrict__ g, long long sq, long 
 	);
 }
 
+#ifndef ADE_EARLY_READ
+#define ADE_EARLY_READ 1
+#endif
+
 // Coupled step: the direct kernel's flow update of a site, then the scalar's.
 template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
@@ -269,6 +273,8 @@ __global__ void __launch_bounds__(128, MINB)
 	Offsets o;
 	long long base = 0, site = 0;
 	bool coll = false, write = false;
+	uint8_t ag = ADE_NOTHING;
+	R g[7];
 	if (active) {
 		base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		site = ((long long) z * a.Y + y) * a.X + x;
@@ -277,6 +283,13 @@ __global__ void __launch_bounds__(128, MINB)
 			geo = a.map[site];
 		// the scalar uses the flow site's neighbour indices (kernels.h:155-156)
 		o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+#if ADE_EARLY_READ
+		// the scalar's loads go out together with the flow's, so that both are
+		// in flight at once
+		ag = d.map[site];
+		if (ag != ADE_NOTHING)
+			ade_read<ODD>(d.g, a.sq, base, o, g);
+#endif
 		if (GENERAL && geo == GEO_NOTHING) {
 			s.rho = R(1);
 			s.vx = s.vy = s.vz = R(0);
@@ -305,11 +318,13 @@ __global__ void __launch_bounds__(128, MINB)
 		return;
 
 	// scalar part (kernels.h:170-195), velocity of the flow site
-	const uint8_t ag = d.map[site];
+#if !ADE_EARLY_READ
+	ag = d.map[site];
+	if (ag != ADE_NOTHING)
+		ade_read<ODD>(d.g, a.sq, base, o, g);
+#endif
 	R phi = 0;
 	if (ag != ADE_NOTHING) {
-		R g[7];
-		ade_read<ODD>(d.g, a.sq, base, o, g);
 		if (ade_boundary(g, phi, ag, s.vx, s.vy, s.vz, d.inflow_phi))
 			ade_collide(g, phi, s.vx, s.vy, s.vz, d.dcoef ? d.dcoef[site] : d.D, d.coll);
 		ade_write<ODD>(d.g, a.sq, base, o, g);
