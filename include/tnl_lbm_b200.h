@@ -400,6 +400,29 @@ LBM_API int lbm_ade_get_populations(lbm_handle h, void* host, int layout, int dt
  * D3Q7_MACRO_Default, d3q7/macro.h:33-37). */
 LBM_API int lbm_ade_get_phi(lbm_handle h, double* host);
 
+/* Slabs of a lattice split along z (the reference's MPI decomposition,
+ * include/lbm3d/lattice_decomposition.h:16-55, lbm.hpp:189-273, on GPUs).
+ * A slab is a lattice of the slab's z extent marked distributed along z: its
+ * periodic sites do not wrap in z but reach their z neighbours through the
+ * ghost layer (kernelInitIndices with distributed.z(), kernels.h:21-37).
+ * Under the A-A pattern only odd steps cross a z face, and only the nine
+ * slots whose c_z points across it.  Per interface (lower slab L of Zl layers,
+ * upper slab U), before every odd step:
+ *   U plane -1 <- L plane Zl-1, slots c_z = -1;  L plane Zl <- U plane 0, slots c_z = +1
+ * and after it:
+ *   L plane Zl-1 <- U plane -1, slots c_z = -1;  U plane 0 <- L plane Zl, slots c_z = +1
+ * Planes are indexed in the ghost frame (z = -1 and z = Z are ghost planes).
+ * lbm_halo_copy moves the planes between two handles of one process (peer
+ * loads between GPUs), ordered after the sender's and before the receiver's
+ * later work; lbm_halo_pack / lbm_halo_unpack stage them in a device buffer of
+ * lbm_halo_bytes bytes on the handle's stream, for a transport between
+ * processes.  A-A only; not with a coupled scalar. */
+LBM_API int lbm_set_distributed_z(lbm_handle h, int distributed);
+LBM_API int64_t lbm_halo_bytes(lbm_handle h);
+LBM_API int lbm_halo_pack(lbm_handle h, int z, int cz, void* dev_buf);
+LBM_API int lbm_halo_unpack(lbm_handle h, int z, int cz, const void* dev_buf);
+LBM_API int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, int cz);
+
 LBM_API const char* lbm_version(void);
 
 #ifdef __cplusplus

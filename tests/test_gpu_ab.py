@@ -6,6 +6,8 @@ Covers every site type of D3Q27_BC_All, including the three the in-place A-A
 step cannot run (GEO_INFLOW_BB_LEFT, GEO_OUTFLOW_RIGHT,
 GEO_OUTFLOW_RIGHT_INTERP), with the tolerances of the A-A parity tests.
 """
+import zlib
+
 import numpy as np
 import pytest
 
@@ -14,7 +16,18 @@ from helpers import COLL_IDS, EQ_IDS, GEO, duct_map, rel_linf, rel_linf_fields, 
 
 pytestmark = pytest.mark.gpu
 
+
+def ke_of(macro):
+    m = macro.astype(np.float64)
+    return float((m[0] * (m[1] ** 2 + m[2] ** 2 + m[3] ** 2)).sum())
+
+
 TOL = {np.float64: 1e-12, np.float32: 1e-5}
+# the velocity is a quotient of differences of populations, which amplifies
+# their FP32 rounding; the FP32 parity bar is on the populations (TOL) and
+# the kinetic energy (KE_TOL)
+FIELD_TOL = {np.float64: 1e-12, np.float32: 3e-5}
+KE_TOL = {np.float64: 1e-12, np.float32: 1e-6}
 
 
 @pytest.fixture(scope="module")
@@ -67,7 +80,8 @@ def test_periodic_taylor_green(pl, port, coll, flags, eq, dtype):
     fg, fo, mg, mo = run_both(pl, f0, m, coll=coll, flags=flags, eq=eq, nu=0.004, force=force, steps=11, dtype=dtype,
                               periodic=True)
     assert rel_linf(fg, fo) <= TOL[dtype]
-    assert rel_linf_fields(mg, mo) <= TOL[dtype]
+    assert rel_linf_fields(mg, mo) <= FIELD_TOL[dtype]
+    assert abs(ke_of(mg) - ke_of(mo)) <= KE_TOL[dtype] * ke_of(mo)
 
 
 def ab_map(kind, rng, X, Y, Z):
@@ -87,7 +101,7 @@ def ab_map(kind, rng, X, Y, Z):
                                            ("MRT", 0, "EQ")])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_boundary_conditions(pl, port, kind, coll, flags, eq, dtype):
-    rng = np.random.default_rng(abs(hash((kind, coll, flags))) % 2 ** 32)
+    rng = np.random.default_rng(zlib.crc32(f"{kind}-{coll}-{flags}".encode()))
     X, Y, Z = 33, 11, 9
     m = ab_map(kind, rng, X, Y, Z)
     f0 = seeded_state(port, rng, X, Y, Z, eq=eq)
@@ -95,7 +109,8 @@ def test_boundary_conditions(pl, port, kind, coll, flags, eq, dtype):
     fg, fo, mg, mo = run_both(pl, f0, m, coll=coll, flags=flags, eq=eq, nu=0.02, force=(1e-5, 0.0, 2e-6),
                               inflow=prof, steps=7, dtype=dtype)
     assert rel_linf(fg, fo) <= TOL[dtype]
-    assert rel_linf_fields(mg, mo) <= TOL[dtype]
+    assert rel_linf_fields(mg, mo) <= FIELD_TOL[dtype]
+    assert abs(ke_of(mg) - ke_of(mo)) <= KE_TOL[dtype] * ke_of(mo)
 
 
 @pytest.mark.parametrize("steps", [16, 17, 40])

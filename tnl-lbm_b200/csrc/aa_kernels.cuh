@@ -59,6 +59,7 @@ struct StepArgs
 	const R* in_vz;
 	R* macro;		   // [4][Z][Y][X] or null
 	double* partials;  // [NRED][slots] or null
+	int zwrap;		   // 0: distributed along z, periodic sites do not wrap in z
 	CollParams<R> p;
 };
 
@@ -69,7 +70,11 @@ struct Offsets
 	long long x[3], y[3], z[3];
 };
 
-__device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, int z, int X, int Y, int Z, int sy, int sz)
+// wrap_z = false: a lattice distributed along z (a slab of a larger lattice,
+// kernelInitIndices with distributed.z(), kernels.h:21-37) reaches its z
+// neighbours through the ghost layer, which the halo exchange fills
+__device__ __forceinline__ Offsets neighbour_offsets(bool wrap, bool wrap_z, int x, int y, int z, int X, int Y, int Z, int sy,
+													int sz)
 {
 	Offsets o;
 	o.x[0] = (wrap && x == 0) ? (X - 1) : -1;
@@ -78,10 +83,15 @@ __device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, in
 	o.y[0] = (long long) ((wrap && y == 0) ? (Y - 1) : -1) * sy;
 	o.y[1] = 0;
 	o.y[2] = (long long) ((wrap && y == Y - 1) ? -(Y - 1) : 1) * sy;
-	o.z[0] = (long long) ((wrap && z == 0) ? (Z - 1) : -1) * sz;
+	o.z[0] = (long long) ((wrap_z && z == 0) ? (Z - 1) : -1) * sz;
 	o.z[1] = 0;
-	o.z[2] = (long long) ((wrap && z == Z - 1) ? -(Z - 1) : 1) * sz;
+	o.z[2] = (long long) ((wrap_z && z == Z - 1) ? -(Z - 1) : 1) * sz;
 	return o;
+}
+
+__device__ __forceinline__ Offsets neighbour_offsets(bool wrap, int x, int y, int z, int X, int Y, int Z, int sy, int sz)
+{
+	return neighbour_offsets(wrap, wrap, x, y, z, X, Y, Z, sy, sz);
 }
 
 // A-A read of the 27 populations (streaming_AA.h:79-116)
@@ -381,7 +391,8 @@ __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typen
 			s.vx = s.vy = s.vz = R(0);
 		}
 		else {
-			o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+			const bool wrap = !GENERAL || geo == GEO_PERIODIC;
+			o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
 			if constexpr (GENERAL)
 				coll = apply_boundary(s, geo, a, z, y);
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(128, MINB)
 		const uint8_t geo = a.map[site];
 		if (geo == GEO_NOTHING)
 			return;
-		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, geo == GEO_PERIODIC && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 		aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
 		if (apply_boundary(s, geo, a, z, y))
 			collide<R, COLL, CUMF>(s, a.p);

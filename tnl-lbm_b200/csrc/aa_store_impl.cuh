@@ -139,7 +139,8 @@ struct StorageUnit
 	template <int COLL, int CUMF, bool ODD, bool GENERAL>
 	static cudaError_t launch_one(const StepLaunch& L, const StepArgs<T, R>& a)
 	{
-		if (L.kernel == KERNEL_TILE)
+		// the tile kernel's windows wrap z on periodic lattices: slabs run the direct kernel
+		if (L.kernel == KERNEL_TILE && !L.distributed_z)
 			return launch_tile<COLL, CUMF, ODD, GENERAL>(L, a);
 		// plain steps of a lattice with a map (observation steps run the direct kernel)
 		if constexpr (GENERAL)
@@ -252,6 +253,7 @@ struct StorageUnit
 		a.in_vz = (const R*) L.inflow[2];
 		a.macro = (R*) L.macro;
 		a.partials = L.partials;
+		a.zwrap = L.distributed_z ? 0 : 1;
 		a.p = make_coll_params<R>(L.p);
 		return a;
 	}

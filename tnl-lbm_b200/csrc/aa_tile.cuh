@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 		const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		const long long sidx = ((long long) z * a.Y + y) * a.X + x;
 		const bool wrap = !GENERAL || geo == GEO_PERIODIC;
-		const Offsets o = neighbour_offsets(wrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		const Offsets o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 		if constexpr (ODD) {
 			// sites on a periodic face: the wrapped neighbours are not in the window
 			bool face;

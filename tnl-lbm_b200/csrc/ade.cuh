@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(128, MINB)
 		if constexpr (GENERAL)
 			geo = a.map[site];
 		// the scalar uses the flow site's neighbour indices (kernels.h:155-156)
-		o = neighbour_offsets(!GENERAL || geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		const bool wrap = !GENERAL || geo == GEO_PERIODIC;
+		o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 #if ADE_EARLY_READ
 		// the scalar's loads go out together with the flow's, so that both are
 		// in flight at once

@@ -66,6 +66,8 @@ struct lbm_lattice
 	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
 	lbm::AdeState* ade = nullptr;			 // coupled D3Q7 scalar, or null
+	bool distributed_z = false;				 // a slab of a lattice split along z (lbm_set_distributed_z)
+	cudaEvent_t halo_ev = nullptr;			 // ordering of halo copies against this lattice's stream
 	static constexpr int GRAPH_STEPS = 16;
 
 	long long sites() const

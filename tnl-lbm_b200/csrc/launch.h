@@ -70,6 +70,7 @@ struct StepLaunch
 	long long split_n[2];
 	int split_tiles_x;
 	const struct AdeLaunch* ade;  // coupled D3Q7 scalar (ade.cuh), or null
+	bool distributed_z;			  // a slab: z neighbours through the ghost layer, no z wrap
 };
 
 // the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)

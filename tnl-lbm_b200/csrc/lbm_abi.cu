@@ -162,6 +162,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.split_n[0] = h->split_n[0];
 	L.split_n[1] = h->split_n[1];
 	L.split_tiles_x = h->split_tiles_x;
+	L.distributed_z = h->distributed_z;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
 	if (h->ade) {
 		h->ade->launch.phi = macro ? h->ade->phi_buf : nullptr;
@@ -366,6 +367,8 @@ int lbm_destroy(lbm_handle h)
 		cudaFreeHost(h->inflow_host);
 	if (h->inflow_ev)
 		cudaEventDestroy(h->inflow_ev);
+	if (h->halo_ev)
+		cudaEventDestroy(h->halo_ev);
 	cudaFree(h->partials);
 	cudaFree(h->finish_arrived);
 	cudaFree(h->status_dev);

@@ -104,6 +104,11 @@ SIGNATURES = {
                                            ctypes.c_int32, _dp, ctypes.c_double, _dp]),
     "lbm_adjoint_backward": (ctypes.c_int, [_H, ctypes.c_double, _dp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "lbm_adjoint_release": (ctypes.c_int, [_H]),
+    "lbm_set_distributed_z": (ctypes.c_int, [_H, ctypes.c_int]),
+    "lbm_halo_bytes": (ctypes.c_int64, [_H]),
+    "lbm_halo_pack": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "lbm_halo_unpack": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "lbm_halo_copy": (ctypes.c_int, [_H, ctypes.c_int, _H, ctypes.c_int, ctypes.c_int]),
     "lbm_ade_enable": (ctypes.c_int, [_H, ctypes.POINTER(lbm_ade_desc)]),
     "lbm_ade_disable": (ctypes.c_int, [_H]),
     "lbm_ade_set_map": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_uint8)]),
