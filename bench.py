@@ -36,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "tnl-lbm_b200"))
 
 METRIC = "D3Q27 cumulant A-A MLUPS, % HBM roofline; FP16-store vs FP32 at stated error"
-BYTES_PER_ELEM = {"f64": 8, "f32": 4, "f32s": 4, "f16s": 2, "bf16s": 2}
+BYTES_PER_ELEM = {"f64": 8, "f32": 4, "f32s": 4, "f16s": 2, "bf16s": 2, "f16sr": 2, "bf16sr": 2}
 
 
 def workload_spec(name):
@@ -94,7 +94,7 @@ def run_ensemble(args):
     sizes, nus = ensemble_setup(spec["count"], edges=spec["edges"])
     sites = sum(x * y * z for x, y, z in sizes)
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
-          "bf16s": pl.STORE_BF16S}[args.storage]
+          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[args.storage]
     ens = pl.Ensemble(sizes, nus, cum_flags=3, storage=st, device=local)
     ens.init_taylor_green(0.05)
     # every launch shape, timed over 256 steps, then the autotuner's choice
@@ -170,7 +170,8 @@ def run_ensemble(args):
             "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(secs_max / args.steps * 1e3, 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f64": "f64", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32"}.get(args.storage, "f32"),
+            "dtype": {"f64": "f64", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32", "f16sr": "f16-store/f32",
+                                                            "bf16sr": "bf16-store/f32"}.get(args.storage, "f32"),
             "data": "synthetic (seeded member sizes, viscosities and Taylor-Green initial states)",
             "config": {"workload": spec["workload"], "members": len(sizes), "sites": sites,
                        "storage": args.storage, "parallelism": f"replicas x{world}",
@@ -366,7 +367,7 @@ def max_over_ranks(dist, value, device):
 
 def make_lattice(pl, spec, storage, device, kernel="direct"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
-          "bf16s": pl.STORE_BF16S}[storage]
+          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
@@ -540,7 +541,7 @@ def run_ours(args):
     variants = {}
     if args.variants and args.storage == "f32" and not spec.get("ade"):
         lat.close()
-        for st in ("f16s", "bf16s"):
+        for st in ("f16s", "bf16s", "f16sr", "bf16sr"):
             vl, _ = make_lattice(pl, spec, st, local, args.kernel)
             vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
             vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
@@ -565,7 +566,7 @@ def run_ours(args):
     precision = None
     if args.precision and rank == 0:
         from pytnl_lbm import precision as prec
-        precision = prec.study(128, 5000, 100, ("f32", "f16s", "bf16s"), local)
+        precision = prec.study(128, 5000, 100, ("f32", "f16s", "bf16s", "f16sr", "bf16sr"), local)
         precision.pop("series")
 
     line = None

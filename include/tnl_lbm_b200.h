@@ -52,6 +52,8 @@ typedef struct lbm_lattice* lbm_handle;
 #define LBM_STORE_F32S 2  /* float f_q - w_q (shifted) */
 #define LBM_STORE_F16S 3  /* half (f_q - w_q) * 2^k_q, 2^k_q >= 1/w_q; FP32 arithmetic */
 #define LBM_STORE_BF16S 4 /* bfloat16 f_q - w_q; FP32 arithmetic */
+#define LBM_STORE_F16SR 5  /* as LBM_STORE_F16S, stochastic rounding on store */
+#define LBM_STORE_BF16SR 6 /* as LBM_STORE_BF16S, stochastic rounding on store */
 
 /* collision slot (COLL of LBM_CONFIG) */
 #define LBM_COLL_CUM 0 /* D3Q27_CUM, include/lbm3d/d3q27/col_cum.h */

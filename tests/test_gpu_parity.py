@@ -223,7 +223,8 @@ def test_storage_roundtrip(pl, port, storage, tol):
         assert got.shape == lat._pop_shape(layout)
 
 
-@pytest.mark.parametrize("storage,tol", [("F32S", 1e-5), ("F16S", 2e-3), ("BF16S", 2e-2)])
+@pytest.mark.parametrize("storage,tol", [("F32S", 1e-5), ("F16S", 2e-3), ("BF16S", 2e-2), ("F16SR", 2e-3),
+                                         ("BF16SR", 2e-2)])
 def test_shifted_storage_follows_fp64(pl, storage, tol):
     """Shifted low-precision storage with FP32 arithmetic against an FP64 run
     of the same Taylor-Green vortex (kinetic energy after 200 steps)."""
@@ -288,7 +289,7 @@ def test_nonfinite_density_is_reported(pl):
     assert e.value.code == 4
 
 
-@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S"])
+@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S", "F16SR", "BF16SR"])
 @pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5), (37, 9, 7), (5, 4, 3), (300, 10, 8)])
 def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
     """The step kernels are the same update: equal results, bit for bit,

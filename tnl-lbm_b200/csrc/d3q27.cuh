@@ -117,6 +117,7 @@ enum Geo : uint8_t
 //   F32S  float   f_q - w_q
 //   F16S  half    (f_q - w_q) * half_scale(q)
 //   BF16S bf16    f_q - w_q
+//   F16SR, BF16SR as F16S and BF16S, rounded stochastically on store
 // Every format is read into the compute type R and written back from it.
 // ---------------------------------------------------------------------------
 struct StoreF64
@@ -205,6 +206,35 @@ struct StoreF16S
 	}
 };
 
+// Stochastic rounding of a float to a 16-bit format that keeps the top
+// 32 - DROP bits: a pseudo-random integer below 2^DROP is added to the bit
+// pattern, then the low bits are cut (round toward zero), so that a value is
+// rounded up with probability equal to its distance from the lower neighbour.
+// The random bits come from a multiplicative hash of the value's own bit
+// pattern (Knuth's golden-ratio constant): no generator state, reproducible
+// results, and a different draw whenever the value changes from one step to
+// the next.  The thresholds are uniform over the values a site takes, so the
+// rounding error has zero mean and the storage error of a slowly varying
+// field does not drift the way round-to-nearest does.
+template <int DROP>
+__device__ __forceinline__ float stochastic_round_bits(float x)
+{
+	const unsigned b = __float_as_uint(x);
+	return __uint_as_float(b + ((b * 0x9E3779B1u) >> (32 - DROP)));
+}
+
+struct StoreF16SR : StoreF16S
+{
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		// a normal half keeps 10 of the float's 23 mantissa bits: 13 are dropped
+		const float x = stochastic_round_bits<13>((v - (float) weight(Q)) * half_scale(Q));
+		const __half h = __float2half_rz(x);
+		__stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
+	}
+};
+
 struct StoreBF16S
 {
 	using T = __nv_bfloat16;
@@ -225,6 +255,19 @@ struct StoreBF16S
 	__device__ static __forceinline__ R load_smem(const T* p)
 	{
 		return __bfloat162float(*p) + (float) weight(Q);
+	}
+};
+
+struct StoreBF16SR : StoreBF16S
+{
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		// bfloat16 keeps 7 of the float's 23 mantissa bits: 16 are dropped, and
+		// cutting them is exact truncation of the bit pattern
+		const float x = stochastic_round_bits<16>(v - (float) weight(Q));
+		const unsigned short h = (unsigned short) (__float_as_uint(x) >> 16);
+		__stcs(reinterpret_cast<unsigned short*>(p), h);
 	}
 };
 

@@ -16,7 +16,9 @@ enum Storage : int
 	ST_F32S = 2,
 	ST_F16S = 3,
 	ST_BF16S = 4,
-	ST_COUNT = 5
+	ST_F16SR = 5,
+	ST_BF16SR = 6,
+	ST_COUNT = 7
 };
 
 // collision-slot constants in double; each unit casts them to its compute type

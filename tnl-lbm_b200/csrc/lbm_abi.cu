@@ -28,6 +28,8 @@ const StorageOps& storage_ops_f32();
 const StorageOps& storage_ops_f32s();
 const StorageOps& storage_ops_f16s();
 const StorageOps& storage_ops_bf16s();
+const StorageOps& storage_ops_f16sr();
+const StorageOps& storage_ops_bf16sr();
 
 const StorageOps& storage_ops(int storage)
 {
@@ -40,6 +42,10 @@ const StorageOps& storage_ops(int storage)
 			return storage_ops_f32s();
 		case ST_F16S:
 			return storage_ops_f16s();
+		case ST_F16SR:
+			return storage_ops_f16sr();
+		case ST_BF16SR:
+			return storage_ops_bf16sr();
 		default:
 			return storage_ops_bf16s();
 	}

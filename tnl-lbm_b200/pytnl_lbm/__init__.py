@@ -20,7 +20,8 @@ from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
     COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
     ADE_CLBM, ADE_GEO, ADE_MRT, ADE_SRT, GEO, KERNEL_DIRECT, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
-    STORE_BF16S, STORE_F16S, STORE_F32, STORE_F32S, STORE_F64, LbmError, library, library_path)
+    STORE_BF16S, STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64, LbmError, library,
+    library_path)
 
 __all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute", "Actions",
            "Counter", "MAX_COUNTER", "NSE", "macro_from_populations"]
@@ -304,7 +305,7 @@ class LBM:
         """torch view of the raw population storage [27, Z+2, Y+2, pitch] (no copy)."""
         import torch
         v = self.device_view()
-        dt = {8: torch.float64, 4: torch.float32, 2: torch.float16 if self.storage == STORE_F16S else torch.bfloat16}[
+        dt = {8: torch.float64, 4: torch.float32, 2: torch.float16 if self.storage in (STORE_F16S, STORE_F16SR) else torch.bfloat16}[
             v.elem_size]
         n = 27 * v.sq
         return _wrap_device(v.populations, n, dt, self.desc.device).view(27, self.Z + 2, self.Y + 2, v.sy)

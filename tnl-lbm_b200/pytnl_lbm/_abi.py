@@ -9,7 +9,7 @@ PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LBM_OK = 0
 ERRORS = {1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "non-finite density", 5: "size limit"}
 
-STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S = 0, 1, 2, 3, 4
+STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S, STORE_F16SR, STORE_BF16SR = 0, 1, 2, 3, 4, 5, 6
 COLL_CUM, COLL_SRT, COLL_BGK, COLL_MRT = 0, 1, 2, 3
 CUM_GEIER_2017, CUM_ANTIALIAS = 1, 2
 EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
