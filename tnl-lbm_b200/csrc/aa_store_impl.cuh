@@ -206,6 +206,9 @@ struct StorageUnit
 			const StepArgs<T, R> a = step_args(L);
 			AdeArgs<R> d;
 			d.g = (R*) L.ade->g;
+			d.sq = L.ade->sq;
+			d.sy = L.ade->sy;
+			d.sz = L.ade->sz;
 			d.map = L.ade->map;
 			d.dcoef = (const R*) L.ade->dcoef;
 			d.D = (R) L.ade->D;

@@ -9,9 +9,10 @@
 // same A-A pattern and the same neighbour offsets, so a site's registers of the
 // flow update are dead before the scalar needs its own.
 //
-// Scalar populations are stored in the compute type with the flow lattice's
-// geometry (slot q at g + q * sq), which is why the coupling is offered for the
-// FP64 and FP32 storage formats (their element is the compute type's size).
+// Scalar populations are stored in the compute type, seven slot rows per
+// lattice row with the flow lattice's row pitch and x offset; the coupling is
+// offered for the FP64 and FP32 storage formats, whose element is the compute
+// type's size.
 //
 // Operators (include/lbm3d/d3q7/): equilibrium eq.h:17-54 (c_s^2 = 1/4,
 // w_0 = 1/4, w_q = 1/8), collisions col_srt.h, col_mrt.h, col_clbm.h with
@@ -65,7 +66,10 @@ enum AdeColl : int
 template <typename R>
 struct AdeArgs
 {
-	R* g;				  // [7][sq] scalar populations, flow lattice geometry
+	R* g;				  // scalar populations, slot q of site (x, y, z) at
+						  // q * sq + (z + 1) * sz + (y + 1) * sy + x0 + x
+	long long sq;
+	int sy, sz;
 	const uint8_t* map;	  // ADE site types [Z][Y][X]
 	const R* dcoef;		  // per-site diffusion coefficient [Z][Y][X], or null
 	R D;				  // diffusion coefficient when dcoef is null
@@ -288,8 +292,11 @@ __global__ void __launch_bounds__(128, MINB)
 		// the scalar's loads go out together with the flow's, so that both are
 		// in flight at once
 		ag = d.map[site];
-		if (ag != ADE_NOTHING)
-			ade_read<ODD>(d.g, a.sq, base, o, g);
+		if (ag != ADE_NOTHING) {
+			const bool w = !GENERAL || geo == GEO_PERIODIC;
+			const Offsets od = neighbour_offsets(w, w && a.zwrap, x, y, z, a.X, a.Y, a.Z, d.sy, d.sz);
+			ade_read<ODD>(d.g, d.sq, (long long) (z + 1) * d.sz + (long long) (y + 1) * d.sy + a.x0 + x, od, g);
+		}
 #endif
 		if (GENERAL && geo == GEO_NOTHING) {
 			s.rho = R(1);
@@ -319,16 +326,21 @@ __global__ void __launch_bounds__(128, MINB)
 		return;
 
 	// scalar part (kernels.h:170-195), velocity of the flow site
-#if !ADE_EARLY_READ
-	ag = d.map[site];
-	if (ag != ADE_NOTHING)
-		ade_read<ODD>(d.g, a.sq, base, o, g);
-#endif
 	R phi = 0;
-	if (ag != ADE_NOTHING) {
-		if (ade_boundary(g, phi, ag, s.vx, s.vy, s.vz, d.inflow_phi))
-			ade_collide(g, phi, s.vx, s.vy, s.vz, d.dcoef ? d.dcoef[site] : d.D, d.coll);
-		ade_write<ODD>(d.g, a.sq, base, o, g);
+	if (ag != ADE_NOTHING || !ADE_EARLY_READ) {
+		const bool w = !GENERAL || (a.map ? a.map[site] == GEO_PERIODIC : true);
+		const Offsets od = neighbour_offsets(w, w && a.zwrap, x, y, z, a.X, a.Y, a.Z, d.sy, d.sz);
+		const long long based = (long long) (z + 1) * d.sz + (long long) (y + 1) * d.sy + a.x0 + x;
+#if !ADE_EARLY_READ
+		ag = d.map[site];
+		if (ag != ADE_NOTHING)
+			ade_read<ODD>(d.g, d.sq, based, od, g);
+#endif
+		if (ag != ADE_NOTHING) {
+			if (ade_boundary(g, phi, ag, s.vx, s.vy, s.vz, d.inflow_phi))
+				ade_collide(g, phi, s.vx, s.vy, s.vz, d.dcoef ? d.dcoef[site] : d.D, d.coll);
+			ade_write<ODD>(d.g, d.sq, based, od, g);
+		}
 	}
 	if (OUT && d.phi)
 		d.phi[site] = phi;

@@ -11,19 +11,32 @@ namespace lbm {
 // front pad, ghost x = -1 at x0 - 1); a row holds the X interior sites, the
 // ghost x = X and room for the tile kernel's odd-step window, which reaches up
 // to 2 x 16 bytes beyond the last site.  f is left null.
-inline Geometry make_geometry(int X, int Y, int Z, int es)
+inline Geometry make_geometry(int X, int Y, int Z, int es, int slots = 27)
 {
+	// Rows of `row` elements (interior from x0, 128-byte aligned, with room for
+	// 16-byte windows past both ends).  The `slots` rows of one (y, z) lattice
+	// row lie side by side (slot q at q * sq within the group), so the 27
+	// streams a warp reads for one row of sites sit in one contiguous region of
+	// 27 rows instead of 27 planes a lattice-size apart: about 3 % more HBM
+	// throughput for the step kernels than separate planes per slot.
 	Geometry g{};
 	const int align = 128 / es;	 // elements per 128 bytes
 	const int a16 = 16 / es;
+	const int row = ((align + X + 2 * a16 + align - 1) / align) * align;
 	g.x0 = align;
-	g.sy = ((align + X + 2 * a16 + align - 1) / align) * align;
+	g.sq = row;
+	g.sy = slots * row;
 	g.sz = g.sy * (Y + 2);
-	g.sq = (long long) g.sz * (Z + 2);
 	g.X = X;
 	g.Y = Y;
 	g.Z = Z;
 	return g;
+}
+
+// elements of the allocation of a geometry (all slots, ghost layer included)
+inline size_t geometry_elems(const Geometry& g)
+{
+	return (size_t) g.sz * (size_t) (g.Z + 2);
 }
 
 // Geier 2017 relaxation rates for omega2 = 1 (col_cum.h:195-228), evaluated

@@ -33,8 +33,8 @@ struct CollParamsD
 struct Geometry
 {
 	void* f;		  // population storage (element 0 of the allocation)
-	long long sq;	  // direction stride in elements
-	int sy, sz, x0;	  // row stride, plane stride, interior x offset (elements)
+	long long sq;	  // slot stride in elements (one row: the slots of a lattice row lie side by side)
+	int sy, sz, x0;	  // lattice-row stride, plane stride, interior x offset (elements)
 	int X, Y, Z;
 };
 
@@ -78,7 +78,9 @@ struct StepLaunch
 // the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)
 struct AdeLaunch
 {
-	void* g;			  // compute-type [7][sq] populations, the flow lattice's geometry
+	void* g;			  // compute-type populations: 7 slot rows per lattice row
+	long long sq;		  // their geometry (rows as the flow lattice's, x0 alike)
+	int sy, sz;
 	const uint8_t* map;	  // ADE site types [Z][Y][X]
 	const void* dcoef;	  // compute-type per-site diffusion coefficient, or null
 	double D;			  // diffusion coefficient when dcoef is null

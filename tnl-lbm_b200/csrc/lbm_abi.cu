@@ -311,7 +311,7 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 	h->ops = &lbm::storage_ops(d.storage);
 	const int es = h->ops->elem_size;
 	h->g = lbm::make_geometry(d.X, d.Y, d.Z, es);
-	h->pop_bytes = (size_t) 27 * h->g.sq * es;
+	h->pop_bytes = lbm::geometry_elems(h->g) * es;
 	lbm::cumulant_rates(d.viscosity, h->p);
 	h->p.nu = d.viscosity;
 	h->p.fx = d.fx;

@@ -2,9 +2,9 @@
 // include/tnl_lbm_b200.h).  The reference couples a second LBM block set of
 // D3Q7 type to the flow (State_NSE_ADE, include/lbm3d/state_NSE_ADE.h, with
 // the coupled kernel of include/lbm3d/kernels.h:114-196); here the scalar is
-// an extension of one lattice handle: its seven population planes share the
-// flow lattice's geometry and are updated by the coupled step kernel of
-// ade.cuh inside every lbm_step.
+// an extension of one lattice handle: its seven slots, seven slot rows per
+// lattice row with the flow lattice's row pitch, are updated by the coupled
+// step kernel of ade.cuh inside every lbm_step.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -15,6 +15,7 @@
 
 #include "../../include/tnl_lbm_b200.h"
 #include "ade.cuh"
+#include "host_common.h"
 #include "lattice.h"
 
 namespace lbm {
@@ -93,12 +94,16 @@ int convert(lbm_handle h, void* dense_dev, int dtype, int layout, bool to_dense)
 	const unsigned nb = (unsigned) ((n + 127) / 128);
 	const bool f64 = h->ops->compute_size == 8;
 	void* planes = h->ade->launch.g;
+	lbm::Geometry g = h->g;	 // the scalar's geometry: the flow's rows, seven slots
+	g.sq = h->ade->launch.sq;
+	g.sy = h->ade->launch.sy;
+	g.sz = h->ade->launch.sz;
 #define ADE_CONV(R, H)                                                                                                 \
 	do {                                                                                                               \
 		if (to_dense)                                                                                                  \
-			ade_convert_kernel<R, H, true><<<nb, 128, 0, h->stream>>>(h->g, (R*) planes, (H*) dense_dev, gh);          \
+			ade_convert_kernel<R, H, true><<<nb, 128, 0, h->stream>>>(g, (R*) planes, (H*) dense_dev, gh);             \
 		else                                                                                                           \
-			ade_convert_kernel<R, H, false><<<nb, 128, 0, h->stream>>>(h->g, (R*) planes, (H*) dense_dev, gh);         \
+			ade_convert_kernel<R, H, false><<<nb, 128, 0, h->stream>>>(g, (R*) planes, (H*) dense_dev, gh);            \
 	} while (0)
 	if (f64 && dtype == 0)
 		ADE_CONV(double, double);
@@ -153,10 +158,15 @@ int lbm_ade_enable(lbm_handle h, const lbm_ade_desc* desc)
 	auto* s = new lbm::AdeState();
 	const size_t cs = (size_t) h->ops->compute_size;
 	const size_t n = (size_t) h->sites();
-	cudaError_t e = cudaMalloc(&s->launch.g, 7 * (size_t) h->g.sq * cs);
+	const lbm::Geometry ag = lbm::make_geometry(h->d.X, h->d.Y, h->d.Z, (int) cs, 7);
+	s->launch.sq = ag.sq;
+	s->launch.sy = ag.sy;
+	s->launch.sz = ag.sz;
+	const size_t gbytes = lbm::geometry_elems(ag) * cs;
+	cudaError_t e = cudaMalloc(&s->launch.g, gbytes);
 	uint8_t* map = nullptr;
 	if (e == cudaSuccess)
-		e = cudaMemsetAsync(s->launch.g, 0, 7 * (size_t) h->g.sq * cs, h->stream);
+		e = cudaMemsetAsync(s->launch.g, 0, gbytes, h->stream);
 	if (e == cudaSuccess)
 		e = cudaMalloc(&map, n);
 	if (e == cudaSuccess)

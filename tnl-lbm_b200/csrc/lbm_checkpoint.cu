@@ -28,7 +28,7 @@
 namespace {
 
 constexpr char MAGIC[8] = {'T', 'N', 'L', 'B', '2', '0', '0', 'C'};
-constexpr uint32_t VERSION = 1;
+constexpr uint32_t VERSION = 2;  // 2: slot rows interleaved per lattice row
 
 struct CheckpointHeader
 {

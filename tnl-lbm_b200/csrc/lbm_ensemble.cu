@@ -389,7 +389,7 @@ int lbm_ensemble_create(const lbm_ensemble_desc* d, lbm_ensemble* out)
 	for (int m = 0; m < e->count; m++) {
 		e->g[m] = lbm::make_geometry(d->X[m], d->Y[m], d->Z[m], es);
 		offset[m] = total;
-		total += ((size_t) 27 * e->g[m].sq * es + 255) / 256 * 256;
+		total += (lbm::geometry_elems(e->g[m]) * es + 255) / 256 * 256;
 		lbm::CollParamsD& p = e->p[m];
 		p = lbm::CollParamsD{};
 		lbm::cumulant_rates(d->viscosity[m], p);

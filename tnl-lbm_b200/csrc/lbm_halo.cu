@@ -17,7 +17,8 @@
 // (a site at the face reads those slots from the neighbour before the step and
 // writes the populations that leave the slab into its ghost layer).  The even
 // step is local.  Every plane moved is the whole (y, x) plane of a slot with
-// its ghost rows and pitch, sz elements.
+// its ghost rows: Y + 2 rows of sq elements, sy apart (the slots of a lattice
+// row lie side by side).
 //
 // lbm_halo_copy moves planes between two slabs of one process with one kernel
 // on the receiver's device; between GPUs the kernel reads the sender's memory
@@ -70,17 +71,29 @@ Slots slots_of(int cz)
 	return s;
 }
 
+// One (y, x) plane of a slot: Y + 2 rows of `row` elements, `pitch` apart.
+struct Plane
+{
+	char* base;		 // element 0 of the allocation
+	long long sq;	 // slot stride (0 for a staging buffer: planes back to back)
+	long long pitch; // row stride
+	long long off;	 // element offset of the plane's first row
+	long long sbuf;	 // staging buffer: element stride between the nine planes
+};
+
 // dst slot dq[k] plane <- src slot sq_[k] plane, k = 0..8 (blockIdx.y); W is
-// an unsigned type of the storage element's width
+// an unsigned type of the storage element's width; n = rows * row elements
 template <typename W>
-__global__ void plane_copy_kernel(W* __restrict__ dst, long long dst_sq, long long dst_off, Slots dq, const W* __restrict__ src,
-								  long long src_sq, long long src_off, Slots sq_, long long n)
+__global__ void plane_copy_kernel(Plane dst, Slots dq, Plane src, Slots sq_, long long row, long long n)
 {
 	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
 	const int k = blockIdx.y;
 	if (i >= n)
 		return;
-	dst[dq.q[k] * dst_sq + dst_off + i] = src[sq_.q[k] * src_sq + src_off + i];
+	const long long r = i / row, c = i - r * row;
+	W* d = reinterpret_cast<W*>(dst.base) + dq.q[k] * dst.sq + k * dst.sbuf + dst.off + r * dst.pitch + c;
+	const W* s = reinterpret_cast<const W*>(src.base) + sq_.q[k] * src.sq + k * src.sbuf + src.off + r * src.pitch + c;
+	*d = *s;
 }
 
 Slots dense_slots()
@@ -105,25 +118,34 @@ bool args_ok(lbm_handle h, int z, int cz)
 	return z >= -1 && z <= h->d.Z && (cz == -1 || cz == 1);
 }
 
-// element offset of plane z (ghost frame -1 .. Z) within a slot
-long long plane_offset(lbm_handle h, int z)
+// elements of one slot plane: Y + 2 rows of one row pitch
+long long plane_elems(lbm_handle h)
 {
-	return (long long) (z + 1) * h->g.sz;
+	return (long long) (h->d.Y + 2) * h->g.sq;
 }
 
-int launch_planes(cudaStream_t st, int elem, void* dst, long long dst_sq, long long dst_off, const Slots& dq, const void* src,
-				  long long src_sq, long long src_off, const Slots& sq_, long long n)
+// slot plane z (ghost frame -1 .. Z) of a lattice
+Plane lattice_plane(lbm_handle h, int z)
+{
+	return Plane{(char*) h->g.f, h->g.sq, h->g.sy, (long long) (z + 1) * h->g.sz, 0};
+}
+
+// the nine planes of a staging buffer, back to back
+Plane buffer_planes(lbm_handle h, const void* buf)
+{
+	return Plane{(char*) buf, 0, h->g.sq, 0, plane_elems(h)};
+}
+
+int launch_planes(cudaStream_t st, int elem, const Plane& dst, const Slots& dq, const Plane& src, const Slots& sq_,
+				  long long row, long long n)
 {
 	const dim3 grid((unsigned) ((n + 255) / 256), 9);
 	if (elem == 8)
-		plane_copy_kernel<unsigned long long><<<grid, 256, 0, st>>>(
-			(unsigned long long*) dst, dst_sq, dst_off, dq, (const unsigned long long*) src, src_sq, src_off, sq_, n);
+		plane_copy_kernel<unsigned long long><<<grid, 256, 0, st>>>(dst, dq, src, sq_, row, n);
 	else if (elem == 4)
-		plane_copy_kernel<unsigned>
-			<<<grid, 256, 0, st>>>((unsigned*) dst, dst_sq, dst_off, dq, (const unsigned*) src, src_sq, src_off, sq_, n);
+		plane_copy_kernel<unsigned><<<grid, 256, 0, st>>>(dst, dq, src, sq_, row, n);
 	else
-		plane_copy_kernel<unsigned short><<<grid, 256, 0, st>>>((unsigned short*) dst, dst_sq, dst_off, dq,
-																 (const unsigned short*) src, src_sq, src_off, sq_, n);
+		plane_copy_kernel<unsigned short><<<grid, 256, 0, st>>>(dst, dq, src, sq_, row, n);
 	const cudaError_t e = cudaGetLastError();
 	return e == cudaSuccess ? LBM_OK : hfail(LBM_ERR_CUDA, "halo copy launch failed: %s", cudaGetErrorString(e));
 }
@@ -149,7 +171,7 @@ int64_t lbm_halo_bytes(lbm_handle h)
 {
 	if (!h)
 		return -1;
-	return (int64_t) 9 * h->g.sz * h->ops->elem_size;
+	return (int64_t) 9 * plane_elems(h) * h->ops->elem_size;
 }
 
 int lbm_halo_pack(lbm_handle h, int z, int cz, void* dev_buf)
@@ -158,9 +180,8 @@ int lbm_halo_pack(lbm_handle h, int z, int cz, void* dev_buf)
 		return rc;
 	if (!dev_buf || !args_ok(h, z, cz))
 		return hfail(LBM_ERR_INVALID, "bad arguments (z %d, cz %d)", z, cz);
-	const long long n = h->g.sz;
-	return launch_planes(h->stream, h->ops->elem_size, dev_buf, n, 0, dense_slots(), h->g.f, h->g.sq, plane_offset(h, z),
-						 slots_of(cz), n);
+	return launch_planes(h->stream, h->ops->elem_size, buffer_planes(h, dev_buf), dense_slots(), lattice_plane(h, z),
+						 slots_of(cz), h->g.sq, plane_elems(h));
 }
 
 int lbm_halo_unpack(lbm_handle h, int z, int cz, const void* dev_buf)
@@ -169,9 +190,8 @@ int lbm_halo_unpack(lbm_handle h, int z, int cz, const void* dev_buf)
 		return rc;
 	if (!dev_buf || !args_ok(h, z, cz))
 		return hfail(LBM_ERR_INVALID, "bad arguments (z %d, cz %d)", z, cz);
-	const long long n = h->g.sz;
-	return launch_planes(h->stream, h->ops->elem_size, h->g.f, h->g.sq, plane_offset(h, z), slots_of(cz), dev_buf, n, 0,
-						 dense_slots(), n);
+	return launch_planes(h->stream, h->ops->elem_size, lattice_plane(h, z), slots_of(cz), buffer_planes(h, dev_buf),
+						 dense_slots(), h->g.sq, plane_elems(h));
 }
 
 int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, int cz)
@@ -180,7 +200,7 @@ int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, int cz)
 		return rc;
 	if (!dst || !args_ok(dst, dst_z, cz) || !args_ok(src, src_z, cz))
 		return hfail(LBM_ERR_INVALID, "bad arguments (z %d / %d, cz %d)", dst_z, src_z, cz);
-	if (dst->g.sz != src->g.sz || dst->ops != src->ops)
+	if (dst->g.sq != src->g.sq || dst->d.Y != src->d.Y || dst->ops != src->ops)
 		return hfail(LBM_ERR_INVALID, "the two slabs differ in their x-y plane or storage format");
 	// the sender's stream has finished what it wrote into the plane
 	if (!src->halo_ev)
@@ -202,8 +222,8 @@ int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, int cz)
 		HALO_CUDA(cudaEventCreateWithFlags(&dst->halo_ev, cudaEventDisableTiming));
 	HALO_CUDA(cudaStreamWaitEvent(dst->stream, src->halo_ev, 0));
 	const Slots sl = slots_of(cz);
-	if (int rc = launch_planes(dst->stream, dst->ops->elem_size, dst->g.f, dst->g.sq, plane_offset(dst, dst_z), sl, src->g.f,
-							   src->g.sq, plane_offset(src, src_z), sl, dst->g.sz))
+	if (int rc = launch_planes(dst->stream, dst->ops->elem_size, lattice_plane(dst, dst_z), sl, lattice_plane(src, src_z), sl,
+							   dst->g.sq, plane_elems(dst)))
 		return rc;
 	// the sender does not overwrite the plane before the copy has read it
 	HALO_CUDA(cudaEventRecord(dst->halo_ev, dst->stream));

@@ -302,13 +302,14 @@ class LBM:
         _abi.check(self.lib.lbm_adjoint_release(self.h))
 
     def populations_tensor(self):
-        """torch view of the raw population storage [27, Z+2, Y+2, pitch] (no copy)."""
+        """torch view of the raw population storage [27, Z+2, Y+2, pitch] (no copy;
+        strides (sq, sz, sy, 1): the 27 slot rows of a lattice row lie side by side)."""
         import torch
         v = self.device_view()
-        dt = {8: torch.float64, 4: torch.float32, 2: torch.float16 if self.storage in (STORE_F16S, STORE_F16SR) else torch.bfloat16}[
-            v.elem_size]
-        n = 27 * v.sq
-        return _wrap_device(v.populations, n, dt, self.desc.device).view(27, self.Z + 2, self.Y + 2, v.sy)
+        dt = {8: torch.float64, 4: torch.float32,
+              2: torch.float16 if self.storage in (STORE_F16S, STORE_F16SR) else torch.bfloat16}[v.elem_size]
+        flat = _wrap_device(v.populations, v.sz * (self.Z + 2), dt, self.desc.device)
+        return flat.as_strided((27, self.Z + 2, self.Y + 2, v.sq), (v.sq, v.sz, v.sy, 1))
 
 
 def _wrap_device(ptr, n, dtype, device):
