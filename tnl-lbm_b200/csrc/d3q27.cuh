@@ -193,10 +193,17 @@ struct StoreF16S
 		const unsigned short raw = __ldcs(reinterpret_cast<const unsigned short*>(p));
 		return __half2float(__ushort_as_half(raw)) * (1.0f / half_scale(Q)) + (float) weight(Q);
 	}
+	// (v - w) * s as one fused multiply-add, v * s - w * s with w * s exact
+	// (s a power of two): one rounding instead of two, one instruction less
+	template <int Q>
+	__device__ static __forceinline__ float scaled_deviation(R v)
+	{
+		return __fmaf_rn(v, half_scale(Q), -(float) weight(Q) * half_scale(Q));
+	}
 	template <int Q>
 	__device__ static __forceinline__ void store(T* p, R v)
 	{
-		const __half h = __float2half_rn((v - (float) weight(Q)) * half_scale(Q));
+		const __half h = __float2half_rn(scaled_deviation<Q>(v));
 		__stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
 	}
 	template <int Q>
@@ -229,7 +236,7 @@ struct StoreF16SR : StoreF16S
 	__device__ static __forceinline__ void store(T* p, R v)
 	{
 		// a normal half keeps 10 of the float's 23 mantissa bits: 13 are dropped
-		const float x = stochastic_round_bits<13>((v - (float) weight(Q)) * half_scale(Q));
+		const float x = stochastic_round_bits<13>(scaled_deviation<Q>(v));
 		const __half h = __float2half_rz(x);
 		__stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(h));
 	}
