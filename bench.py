@@ -492,7 +492,8 @@ def run_ours(args):
     sites = spec["X"] * spec["Y"] * spec["Z"]
     lat, prof = make_lattice(pl, spec, args.storage, local, args.kernel)
     if args.autotune:
-        lat.autotune(4)
+        lat.autotune(16)  # block shape and step kernel, 16 timed steps per candidate
+    kernel_name = {pl.KERNEL_DIRECT: "direct", pl.KERNEL_TILE: "tile", pl.KERNEL_SPLIT: "split"}.get(lat.kernel, "direct")
     stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
     if dist is not None:
         dist.barrier()
@@ -543,6 +544,8 @@ def run_ours(args):
         lat.close()
         for st in ("f16s", "bf16s", "f16sr", "bf16sr"):
             vl, _ = make_lattice(pl, spec, st, local, args.kernel)
+            if args.autotune:
+                vl.autotune(16)
             vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
             vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
             variants[st] = {"mlups": sites * args.steps / vsecs / 1e6,
@@ -582,8 +585,8 @@ def run_ours(args):
                            " Geier-2017+antialias" if spec["cum_flags"] == 3 else " default"),
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
-                       "step_kernel": args.kernel,
-                       "block": list(block) if args.kernel == "direct" else f"{args.kernel} kernel, 128 threads"},
+                       "step_kernel": kernel_name, "autotuned": bool(args.autotune),
+                       "block": list(block) if kernel_name == "direct" else f"{kernel_name} kernel, 128 threads"},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -724,7 +727,8 @@ def main():
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-precision", dest="precision", action="store_false")
-    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default block shape and kernel instead of lbm_autotune's choice")
     ap.add_argument("--kernel", default="direct", choices=["direct", "tile", "split"])
     args = ap.parse_args()
     if args.warmup < 3:
