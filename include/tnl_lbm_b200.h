@@ -160,6 +160,11 @@ LBM_API int lbm_get_macro(lbm_handle h, double* host);
  * sum rho vy, sum rho vz, sum rho |u|^2, non-finite count}.  Returns
  * LBM_ERR_NONFINITE when the count is non-zero (state.hpp:1469-1492). */
 LBM_API int lbm_get_sums(lbm_handle h, double* out);
+/* The sums of the observation step (LBM_STEP_SUMS) that ended at `iteration`;
+ * the last two observation steps are kept.  Waits for that step alone, not
+ * for work enqueued after it, so a caller can enqueue step n+1 before reading
+ * the result of step n.  LBM_ERR_INVALID when that step is no longer kept. */
+LBM_API int lbm_get_sums_of(lbm_handle h, int64_t iteration, double* out);
 
 /* sum rho |grad u|^2 over the macro field of the last LBM_STEP_MACRO step with
  * periodic central differences (sim_4.cu:21-54, :279-298). */

@@ -317,3 +317,25 @@ def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
             assert np.array_equal(out[k][0], out[1][0])
             assert np.array_equal(out[k][1], out[1][1])
             np.testing.assert_allclose(out[k][2], out[1][2], rtol=1e-12)
+
+
+def test_sums_of_earlier_observation_steps(pl, port):
+    """lbm_get_sums_of returns the sums of either of the last two observation
+    steps, equal to what lbm_get_sums returned right after each, and refuses
+    an older one."""
+    X, Y, Z = 24, 10, 8
+    rng = np.random.default_rng(11)
+    lat = pl.LBM(X, Y, Z, viscosity=0.02, storage=pl.STORE_F64, periodic=True)
+    lat.set_populations(seeded_state(port, rng, X, Y, Z))
+    got = {}
+    for _ in range(3):
+        lat.step(3, sums=True)
+        got[lat.iteration] = lat.sums()
+    its = sorted(got)
+    lat.step(2)  # plain steps queued after the observation steps
+    for it in its[-2:]:
+        np.testing.assert_array_equal(lat.sums_of(it), got[it])
+    with pytest.raises(pl.LbmError):
+        lat.sums_of(its[0])
+    lat.close()
+

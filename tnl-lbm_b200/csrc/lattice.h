@@ -42,8 +42,11 @@ struct lbm_lattice
 	bool macro_valid = false;
 	double* partials = nullptr;
 	long long partials_cap = 0;	 // in blocks
-	double* sums_host = nullptr;  // pinned [NRED]
+	double* sums_host = nullptr;  // pinned [2][NRED]: the sums of the last two observation steps
 	double* sums_mapped = nullptr;	// device address of sums_host (written by the finish kernel)
+	cudaEvent_t sums_ev[2] = {nullptr, nullptr};  // recorded after each slot's finish kernel
+	long long sums_iter[2] = {-1, -1};			  // iteration at which each slot's step ended
+	int sums_last = 1;							  // slot of the last observation step
 	unsigned* finish_arrived = nullptr;	 // arrival counter of the finish kernel, zero between launches
 	bool sums_valid = false;
 	long long iteration = 0;

@@ -336,7 +336,9 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 		&& (cudaMalloc(&h->map, (size_t) h->sites() + 64) != cudaSuccess
 			|| cudaMemsetAsync(h->map, 0, (size_t) h->sites() + 64, h->stream) != cudaSuccess))
 		return cleanup(fail(LBM_ERR_CUDA, "map allocation failed"));
-	if (cudaHostAlloc(&h->sums_host, lbm::NRED_HOST * sizeof(double), cudaHostAllocMapped) != cudaSuccess
+	if (cudaHostAlloc(&h->sums_host, 2 * lbm::NRED_HOST * sizeof(double), cudaHostAllocMapped) != cudaSuccess
+		|| cudaEventCreateWithFlags(&h->sums_ev[0], cudaEventDisableTiming) != cudaSuccess
+		|| cudaEventCreateWithFlags(&h->sums_ev[1], cudaEventDisableTiming) != cudaSuccess
 		|| cudaHostGetDevicePointer((void**) &h->sums_mapped, h->sums_host, 0) != cudaSuccess
 		|| cudaMalloc(&h->finish_arrived, sizeof(unsigned)) != cudaSuccess
 		|| cudaMemsetAsync(h->finish_arrived, 0, sizeof(unsigned), h->stream) != cudaSuccess)
@@ -380,6 +382,9 @@ int lbm_destroy(lbm_handle h)
 	cudaFree(h->status_dev);
 	if (h->sums_host)
 		cudaFreeHost(h->sums_host);
+	for (cudaEvent_t ev : h->sums_ev)
+		if (ev)
+			cudaEventDestroy(ev);
 	if (h->stream)
 		cudaStreamDestroy(h->stream);
 	delete h;
@@ -607,6 +612,23 @@ int lbm_get_populations(lbm_handle h, void* host, int layout, int dtype)
 	return LBM_OK;
 }
 
+// FP64 sums of the observation step just launched, written by the finish
+// kernel straight into the next slot of the mapped pinned ring; the slot's
+// event lets a reader wait for this step alone
+int finish_observation(lbm_handle h)
+{
+	const int slot = h->sums_last ^ 1;
+	const long long nb = h->last_blocks;
+	const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
+										   h->sums_mapped + slot * lbm::NRED_HOST, h->stream);
+	if (e != cudaSuccess)
+		return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
+	LBM_CUDA(cudaEventRecord(h->sums_ev[slot], h->stream));
+	h->sums_iter[slot] = h->iteration;
+	h->sums_last = slot;
+	return LBM_OK;
+}
+
 int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 {
 	if (int rc = check(h))
@@ -635,14 +657,8 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 				return fail(LBM_ERR_CUDA, "statistics update failed: %s", cudaGetErrorString(e));
 			h->stats_count++;
 		}
-		if (sums) {
-			const long long nb = h->last_blocks;
-			// the finish kernel writes the sums straight into the mapped pinned buffer
-			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
-												   h->sums_mapped, h->stream);
-			if (e != cudaSuccess)
-				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
-		}
+		if (sums && (rc = finish_observation(h)))
+			return rc;
 		h->macro_valid = true;
 		h->sums_valid = sums;
 		return LBM_OK;
@@ -657,14 +673,8 @@ int lbm_step(lbm_handle h, int64_t nsteps, int flags)
 			return rc;
 		if ((rc = launch_step(h, macro, sums)))
 			return rc;
-		if (sums) {
-			const long long nb = h->last_blocks;
-			// the finish kernel writes the sums straight into the mapped pinned buffer
-			const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
-												   h->sums_mapped, h->stream);
-			if (e != cudaSuccess)
-				return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
-		}
+		if (sums && (rc = finish_observation(h)))
+			return rc;
 		h->macro_valid = macro;
 		h->sums_valid = sums;
 	}
@@ -720,8 +730,25 @@ int lbm_get_sums(lbm_handle h, double* out)
 		return fail(LBM_ERR_INVALID, "null output");
 	if (!h->sums_valid)
 		return fail(LBM_ERR_INVALID, "no sums: run lbm_step with LBM_STEP_SUMS first");
-	LBM_CUDA(cudaStreamSynchronize(h->stream));
-	std::memcpy(out, h->sums_host, lbm::NRED_HOST * sizeof(double));
+	return lbm_get_sums_of(h, h->sums_iter[h->sums_last], out);
+}
+
+int lbm_get_sums_of(lbm_handle h, int64_t iteration, double* out)
+{
+	if (int rc = check(h))
+		return rc;
+	if (!out)
+		return fail(LBM_ERR_INVALID, "null output");
+	int slot = -1;
+	for (int k = 0; k < 2; k++)
+		if (h->sums_iter[k] == iteration && iteration >= 0)
+			slot = k;
+	if (slot < 0)
+		return fail(LBM_ERR_INVALID, "no sums of iteration %lld: the last two observation steps ended at %lld and %lld",
+					(long long) iteration, h->sums_iter[h->sums_last], h->sums_iter[h->sums_last ^ 1]);
+	// wait for that step's finish kernel only, not for work queued after it
+	LBM_CUDA(cudaEventSynchronize(h->sums_ev[slot]));
+	std::memcpy(out, h->sums_host + slot * lbm::NRED_HOST, lbm::NRED_HOST * sizeof(double));
 	if (out[5] != 0.0)
 		return fail(LBM_ERR_NONFINITE, "%.0f sites with a non-finite density", out[5]);
 	return LBM_OK;

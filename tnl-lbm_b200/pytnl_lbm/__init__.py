@@ -152,6 +152,13 @@ class LBM:
         _abi.check(self.lib.lbm_get_sums(self.h, _abi.dptr(out)))
         return out
 
+    def sums_of(self, iteration):
+        """Sums of the observation step that ended at `iteration` (the last two
+        are kept); waits for that step only."""
+        out = np.zeros(6, dtype=np.float64)
+        _abi.check(self.lib.lbm_get_sums_of(self.h, int(iteration), _abi.dptr(out)))
+        return out
+
     def enstrophy_sum(self):
         v = ctypes.c_double(0)
         _abi.check(self.lib.lbm_enstrophy_sum(self.h, ctypes.byref(v)))

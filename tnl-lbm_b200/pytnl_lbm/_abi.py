@@ -104,6 +104,7 @@ SIGNATURES = {
                                            ctypes.c_int32, _dp, ctypes.c_double, _dp]),
     "lbm_adjoint_backward": (ctypes.c_int, [_H, ctypes.c_double, _dp, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "lbm_adjoint_release": (ctypes.c_int, [_H]),
+    "lbm_get_sums_of": (ctypes.c_int, [_H, ctypes.c_int64, _dp]),
     "lbm_set_distributed_z": (ctypes.c_int, [_H, ctypes.c_int]),
     "lbm_halo_bytes": (ctypes.c_int64, [_H]),
     "lbm_halo_pack": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
