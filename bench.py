@@ -426,9 +426,12 @@ def run_adjoint(args):
     target[:, 1] = 0.01
     F = ac.bumps(seed=7)
     stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
-    ac.run(lat, F, min(steps, 64), samples, target)  # warm-up: kernels, allocations
-    lat.adjoint_backward()
     every = int(math.ceil(math.sqrt(steps)))
+    # warm-up with the timed run's sizes, so that the checkpoint and segment
+    # buffers are allocated before the timed region
+    lat.init_equilibrium()
+    lat.adjoint_forward(F, steps, samples, target, checkpoint_every=every)
+    lat.adjoint_backward()
     with ClockSampler(local) as clk:
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         lat.init_equilibrium()
@@ -443,7 +446,7 @@ def run_adjoint(args):
     sites = spec["X"] * spec["Y"] * spec["Z"]
     value = sites * steps * world / secs / 1e6
     v = lat.device_view()
-    pop_bytes = 27 * v.sq * v.elem_size
+    pop_bytes = v.sz * (spec["Z"] + 2) * v.elem_size  # all slots, ghost layer included
     lat.close()
     line = None
     if rank == 0:

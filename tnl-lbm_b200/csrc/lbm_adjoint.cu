@@ -46,6 +46,8 @@ struct AdjointState
 	int nsamples = 0;
 	double w_rho = 0;
 	long long it0 = 0, nsteps = 0, every = 1;
+	long long nckpt = 0;	   // checkpoints of this run (ckpt may hold more from earlier runs)
+	int nsamples_cap = 0;	   // capacity of samples / target / loss_terms
 	double loss = 0;
 	bool forward_done = false;
 };
@@ -188,7 +190,7 @@ int backward_typed(lbm_handle h, double seed)
 	ADJ_CUDA(cudaMemsetAsync(st->lam, 0, pb, h->stream));
 	ADJ_CUDA(cudaMemsetAsync(st->grad, 0, sizeof(double) * 3 * h->sites(), h->stream));
 	ADJ_CUDA(objective<S>(h, true, seed));
-	const long long nseg = (long long) st->ckpt.size();
+	const long long nseg = st->nckpt;
 	for (long long s = nseg - 1; s >= 0; s--) {
 		const long long n0 = s * st->every;
 		const long long n1 = n0 + st->every < st->nsteps ? n0 + st->every : st->nsteps;
@@ -249,9 +251,12 @@ int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64
 		every = nsteps;
 	const long long nckpt = (nsteps + every - 1) / every;
 
-	lbm::adjoint_free(h->adjoint);
-	h->adjoint = new lbm::AdjointState();
+	// the buffers of an earlier run are kept and grown only when this run
+	// needs more (an optimisation loop reruns forward and backward)
+	if (!h->adjoint)
+		h->adjoint = new lbm::AdjointState();
 	auto* st = h->adjoint;
+	st->forward_done = false;
 	st->it0 = h->iteration;
 	st->nsteps = nsteps;
 	st->every = every;
@@ -274,15 +279,29 @@ int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64
 			else
 				((float*) fh.data())[k * nsites + i] = (float) v;
 		}
-	if (cudaMalloc(&st->force, fh.size()) != cudaSuccess || cudaMalloc(&st->final_state, h->pop_bytes) != cudaSuccess
-		|| cudaMalloc(&st->samples, sizeof(long long) * nsamples) != cudaSuccess
-		|| cudaMalloc(&st->target, sizeof(double) * 4 * nsamples) != cudaSuccess
-		|| cudaMalloc(&st->loss_terms, sizeof(double) * nsamples) != cudaSuccess)
+	if ((!st->force && cudaMalloc(&st->force, fh.size()) != cudaSuccess)
+		|| (!st->final_state && cudaMalloc(&st->final_state, h->pop_bytes) != cudaSuccess))
 		return fail_free(afail(LBM_ERR_CUDA, "adjoint buffers: allocation failed"));
-	st->ckpt.assign((size_t) nckpt, nullptr);
-	for (auto& p : st->ckpt)
+	if (nsamples > st->nsamples_cap) {
+		cudaFree(st->samples);
+		cudaFree(st->target);
+		cudaFree(st->loss_terms);
+		st->samples = nullptr;
+		st->target = nullptr;
+		st->loss_terms = nullptr;
+		if (cudaMalloc(&st->samples, sizeof(long long) * nsamples) != cudaSuccess
+			|| cudaMalloc(&st->target, sizeof(double) * 4 * nsamples) != cudaSuccess
+			|| cudaMalloc(&st->loss_terms, sizeof(double) * nsamples) != cudaSuccess)
+			return fail_free(afail(LBM_ERR_CUDA, "adjoint buffers: allocation failed"));
+		st->nsamples_cap = nsamples;
+	}
+	while ((long long) st->ckpt.size() < nckpt) {
+		void* p = nullptr;
 		if (cudaMalloc(&p, h->pop_bytes) != cudaSuccess)
 			return fail_free(afail(LBM_ERR_CUDA, "adjoint checkpoints: allocation of %lld x %zu bytes failed", nckpt, h->pop_bytes));
+		st->ckpt.push_back(p);
+	}
+	st->nckpt = nckpt;
 	if (cudaMemcpyAsync(st->force, fh.data(), fh.size(), cudaMemcpyHostToDevice, h->stream) != cudaSuccess
 		|| cudaMemcpyAsync(st->samples, samples, sizeof(long long) * nsamples, cudaMemcpyHostToDevice, h->stream) != cudaSuccess
 		|| cudaMemcpyAsync(st->target, target, sizeof(double) * 4 * nsamples, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
@@ -310,13 +329,13 @@ int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, void* gr
 	if (grad_populations && ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1)))
 		return afail(LBM_ERR_INVALID, "bad layout or dtype");
 	const size_t pb = h->pop_bytes;
-	if (!st->lam) {
-		if (cudaMalloc(&st->lam, pb) != cudaSuccess || cudaMalloc(&st->grad, sizeof(double) * 3 * h->sites()) != cudaSuccess)
-			return afail(LBM_ERR_CUDA, "adjoint state allocation failed");
-		st->seg.assign((size_t) st->every, nullptr);
-		for (auto& p : st->seg)
-			if (cudaMalloc(&p, pb) != cudaSuccess)
-				return afail(LBM_ERR_CUDA, "adjoint segment buffers: allocation of %lld x %zu bytes failed", st->every, pb);
+	if (!st->lam && (cudaMalloc(&st->lam, pb) != cudaSuccess || cudaMalloc(&st->grad, sizeof(double) * 3 * h->sites()) != cudaSuccess))
+		return afail(LBM_ERR_CUDA, "adjoint state allocation failed");
+	while ((long long) st->seg.size() < st->every) {
+		void* p = nullptr;
+		if (cudaMalloc(&p, pb) != cudaSuccess)
+			return afail(LBM_ERR_CUDA, "adjoint segment buffers: allocation of %lld x %zu bytes failed", st->every, pb);
+		st->seg.push_back(p);
 	}
 	const int rc = h->ops->compute_size == 8 ? backward_typed<lbm::StoreF64>(h, seed) : backward_typed<lbm::StoreF32>(h, seed);
 	if (rc)
