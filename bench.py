@@ -373,7 +373,7 @@ def make_lattice(pl, spec, storage, device, kernel="direct"):
         m, prof, nu, fields = duct_setup(X, Y, Z)
         lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                      equilibrium=pl.EQ_INV_CUM, storage=st, device=device)
-        lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT}.get(kernel, pl.KERNEL_DIRECT))
+        lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT, "pair": pl.KERNEL_PAIR}.get(kernel, pl.KERNEL_DIRECT))
         lat.set_map(m)
         lat.set_inflow(prof, None, None)
         lat.init_equilibrium(*fields)
@@ -387,7 +387,7 @@ def make_lattice(pl, spec, storage, device, kernel="direct"):
     nu = 0.05 * (X / (2 * math.pi)) / 1600.0
     lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
                  equilibrium=pl.EQ_INV_CUM, storage=st, periodic=True, device=device)
-    lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT}.get(kernel, pl.KERNEL_DIRECT))
+    lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT, "pair": pl.KERNEL_PAIR}.get(kernel, pl.KERNEL_DIRECT))
     lat.init_taylor_green(0.05, 1.0)
     return lat, None
 
@@ -496,7 +496,7 @@ def run_ours(args):
     lat, prof = make_lattice(pl, spec, args.storage, local, args.kernel)
     if args.autotune:
         lat.autotune(16)  # block shape and step kernel, 16 timed steps per candidate
-    kernel_name = {pl.KERNEL_DIRECT: "direct", pl.KERNEL_TILE: "tile", pl.KERNEL_SPLIT: "split"}.get(lat.kernel, "direct")
+    kernel_name = {pl.KERNEL_DIRECT: "direct", pl.KERNEL_TILE: "tile", pl.KERNEL_SPLIT: "split", pl.KERNEL_PAIR: "pair"}.get(lat.kernel, "direct")
     stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
     if dist is not None:
         dist.barrier()
@@ -563,7 +563,7 @@ def run_ours(args):
                             "speedup_vs_f32": secs / vsecs,
                             "achieved_gbs": 2 * 27 * 2 * sites / (vsecs / args.steps) / 1e9}
             vl.close()
-        for other in ("direct", "tile", "split"):
+        for other in ("direct", "pair", "tile", "split"):
             if other == args.kernel or (other == "split" and spec["kind"] != "duct"):
                 continue
             vl, _ = make_lattice(pl, spec, "f32", local, other)
@@ -597,8 +597,9 @@ def run_ours(args):
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
                        "step_kernel": kernel_name, "autotuned": bool(args.autotune),
-                       "block": list(block) if kernel_name == "direct" else f"{kernel_name} kernel, 128 threads"},
-            "gpu_launches": args.steps,
+                       "block": list(block) if kernel_name in ("direct", "pair") else f"{kernel_name} kernel, 128 threads"},
+            # the pair and split steps of a lattice with a map launch two kernels per step
+            "gpu_launches": args.steps * (2 if kernel_name in ("pair", "split") and spec["kind"] == "duct" else 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
@@ -742,7 +743,7 @@ def main():
     ap.add_argument("--no-precision", dest="precision", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default block shape and kernel instead of lbm_autotune's choice")
-    ap.add_argument("--kernel", default="direct", choices=["direct", "tile", "split"])
+    ap.add_argument("--kernel", default="direct", choices=["direct", "tile", "split", "pair"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

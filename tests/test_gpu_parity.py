@@ -9,12 +9,12 @@ steps and compares populations, macro fields and sums.
 Tolerances (norm-wise relative L-infinity, ||a - b||_inf / ||b||_inf, over all
 population slots; macro fields: density and velocity vector):
   FP64 storage  1e-12   (different FMA contraction and reciprocal use only)
-  FP32 storage  1e-5 on populations for every step count (the north-star
-                bound); 1e-6 on kinetic energy and 1e-5 on the macro field up
-                to 11 steps.  Two FP32 runs that round in a different order
-                drift apart slowly: after 100 steps the kinetic energies agree
-                to ~2e-6 and the macro fields to ~1.3e-5, which the 100-step
-                cases bound by 5e-6 and 3e-5.
+  FP32 storage  1e-5 on populations for every step count; 1e-6 on kinetic
+                energy and 1e-5 on the macro field up to 11 steps.  Two FP32
+                runs that round in a different order drift apart slowly: after
+                100 steps the macro fields agree to ~1.3e-5 (bound 3e-5), and
+                the kinetic energy and mass of the 100-step runs are held to
+                an FP64 oracle run instead of the FP32 one.
 """
 import zlib
 
@@ -79,7 +79,7 @@ CASES_PERIODIC = [("CUM", 0, "INV_CUM"), ("CUM", 2, "INV_CUM"), ("CUM", 3, "INV_
                   ("SRT", 0, "INV_CUM"), ("BGK", 0, "EQ"), ("MRT", 0, "EQ")]
 
 
-KERNELS = ["TILE", "DIRECT", "SPLIT"]
+KERNELS = ["TILE", "DIRECT", "SPLIT", "PAIR"]
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
@@ -97,10 +97,28 @@ def test_periodic_taylor_green_parity(pl, port, coll, flags, eq, dtype, steps, k
     long = dtype == np.float32 and steps > 11
     assert rel_linf(fg, fo) <= TOL[dtype]
     assert rel_linf_fields(mg, mo) <= (3e-5 if long else TOL[dtype])
-    assert abs(sg[4] - ke_of(mo)) <= (5e-6 if long else KE_TOL[dtype]) * ke_of(mo)
-    mass = mo[0].astype(np.float64).sum()
-    assert abs(sg[0] - mass) <= KE_TOL[dtype] * mass
     assert sg[5] == 0
+    if not long:
+        assert abs(sg[4] - ke_of(mo)) <= KE_TOL[dtype] * ke_of(mo)
+        mass = mo[0].astype(np.float64).sum()
+        assert abs(sg[0] - mass) <= KE_TOL[dtype] * mass
+        return
+    # Over 100 steps the FP32 oracle itself drifts from the conserved mass and
+    # from the FP64 kinetic energy by about 1e-6: the long FP32 runs are held
+    # to the FP64 oracle.  The cumulant kernels write the backward chimera
+    # transform through the sum and difference of the outer values (mass and
+    # momentum of a line exact up to one rounding each): mass within 1e-7 and
+    # kinetic energy within 3e-6 of FP64 (measured 1e-8 and below 1.3e-6).  The
+    # FP32 SRT run with the factorised equilibrium drifts furthest of the other
+    # operators (kinetic energy 1.3e-5 from FP64): 3e-5 and mass 2e-6 for them.
+    f64 = np.ascontiguousarray(f0.astype(np.float64))
+    m64 = np.zeros((4, Z, Y, X), np.float64)
+    port.aa_run(f64, m.astype(np.int16), coll=coll, eq=eq, cum_flags=flags, nu=0.004, force=force, macro=m64,
+                start_iter=0, nsteps=steps)
+    ke64, mass64 = ke_of(m64), m64[0].sum()
+    cum = coll == "CUM"
+    assert abs(sg[4] - ke64) <= (3e-6 if cum else 3e-5) * ke64
+    assert abs(sg[0] - mass64) <= (1e-7 if cum else 2e-6) * mass64
 
 
 MAPS = ["duct_left", "duct_inflow", "duct_eqleft", "sym", "random", "periodic_map"]

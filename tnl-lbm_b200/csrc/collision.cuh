@@ -198,18 +198,21 @@ __device__ __forceinline__ void chim_fwd(R& m, R& z, R& p, R u, R u2)
 	p = k2;
 }
 
-// backward chimera transform (Eqs 88-96 of Geier 2015)
+// backward chimera transform (Eqs 88-96 of Geier 2015), written through the
+// sum s = v+ + v- = k0 u^2 + 2 u k1 + k2 and the difference d = v+ - v- =
+// u k0 + k1 of the outer values: v0 = k0 - s, v+- = (s +- d) / 2.  The three
+// values then add up to k0 and their first moment is d up to one rounding
+// each, the mass and momentum the line carries, where the term-by-term form
+// of the paper rounds every term separately.
 template <typename R>
 __device__ __forceinline__ void chim_bwd(R& a, R& b, R& c, R u, R u2)
 {
 	const R k0 = a, k1 = b, k2 = c;
-	const R two_u = R(2) * u;
-	const R vz = k0 * (R(1) - u2) - two_u * k1 - k2;
-	const R vm = (k0 * (u2 - u) + k1 * (two_u - R(1)) + k2) * R(0.5);
-	const R vp = (k0 * (u2 + u) + k1 * (two_u + R(1)) + k2) * R(0.5);
-	a = vm;
-	b = vz;
-	c = vp;
+	const R s = k0 * u2 + (R(2) * u * k1 + k2);
+	const R hd = R(0.5) * (u * k0 + k1);
+	a = s * R(0.5) - hd;
+	b = k0 - s;
+	c = s * R(0.5) + hd;
 }
 
 template <typename R, int FLAGS>

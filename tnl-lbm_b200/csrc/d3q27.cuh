@@ -110,6 +110,19 @@ enum Geo : uint8_t
 	GEO_SYM_FRONT = 16,
 };
 
+// Groups of the two-site step (pair.cuh): a lattice row is cut into groups of
+// PAIR_GROUP x-sites (64 bytes of a slot row in FP32, 32 in the 16-bit
+// formats: whole DRAM sectors, as the interior x = 0 of a row is 128-byte
+// aligned), and a group whose sites are all GEO_FLUID or all GEO_PERIODIC runs
+// in the two-site kernel.
+constexpr int PAIR_GROUP = 16;
+enum : uint8_t
+{
+	PAIR_GROUP_REST = 0,
+	PAIR_GROUP_FLUID = 1,
+	PAIR_GROUP_PERIODIC = 2
+};
+
 // ---------------------------------------------------------------------------
 // population storage formats
 //   F64   double  f_q

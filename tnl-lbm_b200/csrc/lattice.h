@@ -65,6 +65,11 @@ struct lbm_lattice
 	unsigned* split_tiles = nullptr;  // split step: fluid-only tiles, then the others
 	long long split_n[2] = {0, 0};
 	int split_tiles_x = 0;
+	unsigned long long* pair_rest = nullptr;  // pair step: sites outside the two-site pairs (StepLaunch)
+	long long pair_n = 0;
+	uint8_t* pair_groups = nullptr;  // pair step: PAIR_GROUP_* of every group of PAIR_GROUP sites (StepLaunch)
+	cudaStream_t side_stream = nullptr;	 // pair step: the rest sites' stream, with its fork / join events
+	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 	void* stats = nullptr;		// D3Q27_MACRO_Mean fields [9][sites], compute type
 	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward

@@ -60,7 +60,7 @@ struct StepLaunch
 	CollParamsD p;
 	int coll, cum_flags;
 	bool odd;
-	int kernel;		   // KERNEL_DIRECT, KERNEL_TILE or KERNEL_SPLIT
+	int kernel;		   // KERNEL_DIRECT, KERNEL_TILE, KERNEL_SPLIT or KERNEL_PAIR
 	dim3 grid, block;  // direct kernel launch shape
 	int* status;	   // device status word (STATUS_* bits)
 	cudaStream_t stream;
@@ -73,6 +73,15 @@ struct StepLaunch
 	int split_tiles_x;
 	const struct AdeLaunch* ade;  // coupled D3Q7 scalar (ade.cuh), or null
 	bool distributed_z;			  // a slab: z neighbours through the ghost layer, no z wrap
+	// pair step with a map: the sites outside the two-site kernel's pairs
+	// (row << 32 | x, row = z Y + y), GEO_NOTHING sites left out
+	const unsigned long long* pair_rest;
+	long long pair_n;
+	const uint8_t* pair_groups;	 // PAIR_GROUP_* per group of PAIR_GROUP sites of a row
+	// a second stream and fork / join events: the rest sites of the pair step
+	// run beside the pair kernel (null: one after the other)
+	cudaStream_t side_stream;
+	cudaEvent_t fork_ev, join_ev;
 };
 
 // the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)
@@ -95,8 +104,19 @@ enum : int
 {
 	KERNEL_DIRECT = 0,
 	KERNEL_TILE = 1,
-	KERNEL_SPLIT = 3
+	KERNEL_SPLIT = 3,
+	KERNEL_PAIR = 4
 };
+
+// two-site step kernels (pair.cuh), one per storage with FP32 arithmetic;
+// cudaErrorNotSupported for the collisions they do not cover
+using PairStepFn = cudaError_t (*)(const StepLaunch&);
+cudaError_t pair_step_f32(const StepLaunch&);
+cudaError_t pair_step_f32s(const StepLaunch&);
+cudaError_t pair_step_f16s(const StepLaunch&);
+cudaError_t pair_step_f16sr(const StepLaunch&);
+cudaError_t pair_step_bf16s(const StepLaunch&);
+cudaError_t pair_step_bf16sr(const StepLaunch&);
 // upper bound of the tile kernel's grid (blocks per SM x SMs)
 constexpr int TILE_MAX_BLOCKS_PER_SM = 8;
 

@@ -50,6 +50,27 @@ const StorageOps& storage_ops(int storage)
 			return storage_ops_bf16s();
 	}
 }
+
+// the two-site step of a storage, or null (FP64 arithmetic)
+PairStepFn pair_step_of(int storage)
+{
+	switch (storage) {
+		case ST_F32:
+			return pair_step_f32;
+		case ST_F32S:
+			return pair_step_f32s;
+		case ST_F16S:
+			return pair_step_f16s;
+		case ST_F16SR:
+			return pair_step_f16sr;
+		case ST_BF16S:
+			return pair_step_bf16s;
+		case ST_BF16SR:
+			return pair_step_bf16sr;
+		default:
+			return nullptr;
+	}
+}
 }  // namespace lbm
 
 namespace {
@@ -168,6 +189,12 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.split_n[0] = h->split_n[0];
 	L.split_n[1] = h->split_n[1];
 	L.split_tiles_x = h->split_tiles_x;
+	L.pair_rest = h->pair_rest;
+	L.pair_groups = h->pair_groups;
+	L.side_stream = h->side_stream;
+	L.fork_ev = h->fork_ev;
+	L.join_ev = h->join_ev;
+	L.pair_n = h->pair_n;
 	L.distributed_z = h->distributed_z;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
 	if (h->ade) {
@@ -176,7 +203,14 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 		if (!dry_run)
 			h->ade->phi_valid = macro;
 	}
-	const cudaError_t err = h->ade ? h->ops->ade_step(L) : (ab ? h->ops->ab_step(L) : h->ops->step(L));
+	cudaError_t err = cudaErrorNotSupported;
+	// the two-site kernel where it applies (the cumulant on FP32 arithmetic),
+	// else the direct kernel
+	if (!h->ade && !ab && h->kernel == lbm::KERNEL_PAIR)
+		if (const lbm::PairStepFn pair = lbm::pair_step_of(h->d.storage))
+			err = pair(L);
+	if (err == cudaErrorNotSupported)
+		err = h->ade ? h->ops->ade_step(L) : (ab ? h->ops->ab_step(L) : h->ops->step(L));
 	if (err != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "step kernel launch failed: %s", cudaGetErrorString(err));
 	if (dry_run)
@@ -366,6 +400,8 @@ int lbm_destroy(lbm_handle h)
 	cudaFree(h->g.f);
 	cudaFree(h->f_out);
 	cudaFree(h->split_tiles);
+	cudaFree(h->pair_rest);
+	cudaFree(h->pair_groups);
 	cudaFree(h->stats);
 	cudaFree(h->map);
 	for (auto* p : h->inflow)
@@ -377,6 +413,12 @@ int lbm_destroy(lbm_handle h)
 		cudaEventDestroy(h->inflow_ev);
 	if (h->halo_ev)
 		cudaEventDestroy(h->halo_ev);
+	if (h->fork_ev)
+		cudaEventDestroy(h->fork_ev);
+	if (h->join_ev)
+		cudaEventDestroy(h->join_ev);
+	if (h->side_stream)
+		cudaStreamDestroy(h->side_stream);
 	cudaFree(h->partials);
 	cudaFree(h->finish_arrived);
 	cudaFree(h->status_dev);
@@ -436,6 +478,44 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		h->split_n[0] = (long long) (nt - other.size());
 		h->split_n[1] = (long long) other.size();
 		h->split_tiles_x = tx;
+		// groups of the two-site step (PAIR_GROUP sites of a row: all
+		// GEO_FLUID, all GEO_PERIODIC, or the rest) and the list of the sites
+		// of the rest groups, GEO_NOTHING sites left out
+		const int X = h->d.X;
+		const int gx = (X + lbm::PAIR_GROUP - 1) / lbm::PAIR_GROUP;
+		std::vector<uint8_t> groups((size_t) gx * h->d.Y * h->d.Z);
+		std::vector<unsigned long long> rest;
+		for (long long row = 0; row < (long long) h->d.Y * h->d.Z; row++)
+			for (int k = 0; k < gx; k++) {
+				const int x0 = k * lbm::PAIR_GROUP;
+				const uint8_t first = map[row * X + x0];
+				bool same = x0 + lbm::PAIR_GROUP <= X && (first == lbm::GEO_FLUID || first == lbm::GEO_PERIODIC);
+				for (int x = x0 + 1; same && x < x0 + lbm::PAIR_GROUP; x++)
+					same = map[row * X + x] == first;
+				groups[row * gx + k] = !same ? lbm::PAIR_GROUP_REST
+										: (first == lbm::GEO_PERIODIC ? lbm::PAIR_GROUP_PERIODIC : lbm::PAIR_GROUP_FLUID);
+				if (!same)
+					for (int x = x0; x < x0 + lbm::PAIR_GROUP && x < X; x++)
+						if (map[row * X + x] != lbm::GEO_NOTHING)
+							rest.push_back((unsigned long long) row << 32 | (unsigned) x);
+			}
+		if (!h->side_stream) {
+			LBM_CUDA(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+			LBM_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+			LBM_CUDA(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
+		}
+		cudaFree(h->pair_groups);
+		h->pair_groups = nullptr;
+		LBM_CUDA(cudaMalloc(&h->pair_groups, groups.size()));
+		LBM_CUDA(cudaMemcpyAsync(h->pair_groups, groups.data(), groups.size(), cudaMemcpyHostToDevice, h->stream));
+		cudaFree(h->pair_rest);
+		h->pair_rest = nullptr;
+		h->pair_n = (long long) rest.size();
+		LBM_CUDA(cudaMalloc(&h->pair_rest, (rest.empty() ? 1 : rest.size()) * sizeof(unsigned long long)));
+		if (!rest.empty())
+			LBM_CUDA(cudaMemcpyAsync(h->pair_rest, rest.data(), rest.size() * sizeof(unsigned long long),
+									 cudaMemcpyHostToDevice, h->stream));
+		LBM_CUDA(cudaStreamSynchronize(h->stream));
 		h->drop_graph();
 	}
 	return LBM_OK;
@@ -838,34 +918,42 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	cudaEventCreate(&e1);
 	float best = 1e30f;
 	int bbx = 0, bby = 0;
+	int best_kernel = lbm::KERNEL_DIRECT;
 	const int obx = h->bx, oby = h->by;
+	// the direct and the two-site kernel take the block shape
+	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->d.collision == LBM_COLL_CUM && !h->ade
+					  && h->streaming == LBM_STREAMING_AA;
 	for (auto& c : cands) {
 		if (c[0] > 32 && c[0] / 2 >= h->d.X)
 			continue;  // far wider than the lattice
 		h->bx = c[0];
 		h->by = c[1];
-		h->kernel = lbm::KERNEL_DIRECT;
 		if (ensure_partials(h, h->max_step_blocks()))
 			break;
-		// warm-up pair, then timed steps
-		launch_step(h, false, false);
-		launch_step(h, false, false);
-		cudaEventRecord(e0, h->stream);
-		for (int s = 0; s < ntrials; s++)
+		for (int k : {(int) lbm::KERNEL_DIRECT, (int) lbm::KERNEL_PAIR}) {
+			if (k == lbm::KERNEL_PAIR && !pair_ok)
+				continue;
+			h->kernel = k;
+			// warm-up pair, then timed steps
 			launch_step(h, false, false);
-		cudaEventRecord(e1, h->stream);
-		cudaEventSynchronize(e1);
-		float ms = 0;
-		cudaEventElapsedTime(&ms, e0, e1);
-		if (ms < best) {
-			best = ms;
-			bbx = c[0];
-			bby = c[1];
+			launch_step(h, false, false);
+			cudaEventRecord(e0, h->stream);
+			for (int s = 0; s < ntrials; s++)
+				launch_step(h, false, false);
+			cudaEventRecord(e1, h->stream);
+			cudaEventSynchronize(e1);
+			float ms = 0;
+			cudaEventElapsedTime(&ms, e0, e1);
+			if (ms < best) {
+				best = ms;
+				bbx = c[0];
+				bby = c[1];
+				best_kernel = k;
+			}
 		}
 	}
 	// the tile kernel and, with a map, the split step (the block shape does
 	// not apply to them)
-	int best_kernel = lbm::KERNEL_DIRECT;
 	for (int k : {(int) lbm::KERNEL_TILE, (int) lbm::KERNEL_SPLIT}) {
 		if (k == lbm::KERNEL_SPLIT && !h->split_tiles)
 			continue;
@@ -986,7 +1074,7 @@ int lbm_set_kernel(lbm_handle h, int kernel)
 {
 	if (int rc = check(h))
 		return rc;
-	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE && kernel != LBM_KERNEL_SPLIT)
+	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE && kernel != LBM_KERNEL_SPLIT && kernel != LBM_KERNEL_PAIR)
 		return fail(LBM_ERR_INVALID, "unknown kernel %d", kernel);
 	h->kernel = kernel;
 	h->drop_graph();

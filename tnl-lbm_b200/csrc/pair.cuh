@@ -1,0 +1,530 @@
+// Two-site A-A step for sm_100a: every thread updates the x-adjacent sites
+// (x, x + 1) of one lattice row, and the cumulant collision of both runs on
+// the packed FP32 instructions of sm_100 (add/mul/fma on .f32x2 operands,
+// __fadd2_rn / __fmul2_rn / __ffma2_rn), which issue one instruction for two
+// values.  The two sites share their y and z neighbour offsets, and the
+// directions without an x component (and every direction of the even step)
+// move both sites' populations with one 8-byte (FP32) or 4-byte (16-bit)
+// access.
+//
+// The per-site algorithm is that of aa_step_kernel (aa_kernels.cuh): A-A
+// read and write of streaming_AA.h, D3Q27_BC_All (bc.h) through
+// apply_boundary, and the cumulant collision of col_cum.h.  On a lattice with
+// a map, the pair kernel updates the pairs whose sites are both GEO_FLUID or
+// both GEO_PERIODIC, and a second launch updates every other site one thread
+// per site over the tiles that hold such sites (the inlet and outlet columns,
+// the walls); A-A sites are independent within a step, so the two launches
+// together are the same step.
+#pragma once
+
+#include "aa_kernels.cuh"
+#include "coll_params.cuh"
+#include "launch.h"
+
+namespace lbm {
+
+// two FP32 lanes
+struct F2
+{
+	float2 v;
+	F2() = default;
+	__host__ __device__ __forceinline__ F2(double a) : v{(float) a, (float) a} {}
+	__host__ __device__ __forceinline__ F2(float a, float b) : v{a, b} {}
+	__host__ __device__ __forceinline__ explicit F2(float2 a) : v(a) {}
+};
+
+__device__ __forceinline__ F2 operator+(F2 a, F2 b)
+{
+	return F2(__fadd2_rn(a.v, b.v));
+}
+__device__ __forceinline__ F2 operator-(F2 a)
+{
+	return F2(make_float2(-a.v.x, -a.v.y));
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b)
+{
+	return F2(__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y)));
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b)
+{
+	return F2(__fmul2_rn(a.v, b.v));
+}
+__device__ __forceinline__ F2& operator+=(F2& a, F2 b)
+{
+	a = a + b;
+	return a;
+}
+__device__ __forceinline__ F2& operator-=(F2& a, F2 b)
+{
+	a = a - b;
+	return a;
+}
+// a * b + c, one rounding per lane
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c)
+{
+	return F2(__ffma2_rn(a.v, b.v, c.v));
+}
+__device__ __forceinline__ F2 fabs(F2 a)
+{
+	return F2(fabsf(a.v.x), fabsf(a.v.y));
+}
+template <>
+__device__ __forceinline__ F2 rcp<F2>(F2 x)
+{
+	return F2(__frcp_rn(x.v.x), __frcp_rn(x.v.y));
+}
+template <>
+__device__ __forceinline__ F2 div_approx<F2>(F2 a, F2 b)
+{
+	return F2(__fdividef(a.v.x, b.v.x), __fdividef(a.v.y, b.v.y));
+}
+
+// Chimera transforms of collide_cumulant with the multiply-adds written out
+// (the compiler fuses a * b + c only for scalar operands), in the order of the
+// scalar forms.
+__device__ __forceinline__ void chim_fwd(F2& m, F2& z, F2& p, F2 u, F2 u2)
+{
+	const F2 s = p + m, d = p - m;
+	const F2 k0 = s + z;
+	m = k0;
+	z = fma2(-u, k0, d);
+	p = fma2(u2, k0, fma2(-(u + u), d, s));
+}
+__device__ __forceinline__ void chim_bwd(F2& a, F2& b, F2& c, F2 u, F2 u2)
+{
+	const F2 k0 = a, k1 = b, k2 = c;
+	const F2 s = fma2(k0, u2, fma2(u + u, k1, k2));
+	const F2 hd = F2(0.5) * fma2(u, k0, k1);
+	a = fma2(s, F2(0.5), -hd);
+	b = k0 - s;
+	c = fma2(s, F2(0.5), hd);
+}
+
+// ---------------------------------------------------------------------------
+// two-site accesses per storage format: load2 / store2 move the populations
+// of sites (x, x + 1) at p, p + 1 (p 8-byte aligned for FP32, 4-byte for the
+// 16-bit formats); Q is the slot, as for the scalar S::load / S::store
+// ---------------------------------------------------------------------------
+template <typename S>
+struct PairIO;
+
+template <>
+struct PairIO<StoreF32>
+{
+	template <int Q>
+	__device__ static __forceinline__ F2 load2(const float* p)
+	{
+		return F2(__ldcs(reinterpret_cast<const float2*>(p)));
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store2(float* p, F2 v)
+	{
+		__stcs(reinterpret_cast<float2*>(p), v.v);
+	}
+};
+
+template <>
+struct PairIO<StoreF32S>
+{
+	template <int Q>
+	__device__ static __forceinline__ F2 load2(const float* p)
+	{
+		return F2(__ldcs(reinterpret_cast<const float2*>(p))) + F2(weight(Q));
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store2(float* p, F2 v)
+	{
+		__stcs(reinterpret_cast<float2*>(p), (v - F2(weight(Q))).v);
+	}
+};
+
+template <>
+struct PairIO<StoreF16S>
+{
+	template <int Q>
+	__device__ static __forceinline__ F2 load2(const __half* p)
+	{
+		const F2 h(__half22float2(__ldcs(reinterpret_cast<const __half2*>(p))));
+		return fma2(h, F2(1.0 / half_scale(Q)), F2(weight(Q)));
+	}
+	// (v - w) * s as v * s - w * s, as StoreF16S::scaled_deviation
+	template <int Q>
+	__device__ static __forceinline__ F2 scaled_deviation(F2 v)
+	{
+		return fma2(v, F2(half_scale(Q)), F2(-(float) weight(Q) * half_scale(Q)));
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store2(__half* p, F2 v)
+	{
+		__stcs(reinterpret_cast<__half2*>(p), __float22half2_rn(scaled_deviation<Q>(v).v));
+	}
+};
+
+template <>
+struct PairIO<StoreF16SR> : PairIO<StoreF16S>
+{
+	template <int Q>
+	__device__ static __forceinline__ void store2(__half* p, F2 v)
+	{
+		const F2 d = scaled_deviation<Q>(v);
+		const __half lo = __float2half_rz(stochastic_round_bits<13>(d.v.x));
+		const __half hi = __float2half_rz(stochastic_round_bits<13>(d.v.y));
+		__stcs(reinterpret_cast<__half2*>(p), __halves2half2(lo, hi));
+	}
+};
+
+template <>
+struct PairIO<StoreBF16S>
+{
+	template <int Q>
+	__device__ static __forceinline__ F2 load2(const __nv_bfloat16* p)
+	{
+		return F2(__bfloat1622float2(__ldcs(reinterpret_cast<const __nv_bfloat162*>(p)))) + F2(weight(Q));
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store2(__nv_bfloat16* p, F2 v)
+	{
+		__stcs(reinterpret_cast<__nv_bfloat162*>(p), __float22bfloat162_rn((v - F2(weight(Q))).v));
+	}
+};
+
+template <>
+struct PairIO<StoreBF16SR> : PairIO<StoreBF16S>
+{
+	template <int Q>
+	__device__ static __forceinline__ void store2(__nv_bfloat16* p, F2 v)
+	{
+		const F2 d = v - F2(weight(Q));
+		const unsigned lo = __float_as_uint(stochastic_round_bits<16>(d.v.x)) >> 16;
+		const unsigned hi = __float_as_uint(stochastic_round_bits<16>(d.v.y)) & 0xffff0000u;
+		__stcs(reinterpret_cast<unsigned*>(p), lo | hi);
+	}
+};
+
+// x offsets of a pair: the left neighbour of site x and the right neighbour
+// of site x + 1 (the other two are the pair's own sites); periodic sites wrap
+struct PairX
+{
+	int left;	// -1, or X - 1 for a periodic site at x = 0
+	int right;	// +1, or -(X - 1) for a periodic site at x + 1 = X - 1
+};
+
+// A-A read of both sites with shared y and z offsets (o.y, o.z of either site)
+template <typename S, bool ODD>
+__device__ __forceinline__ void pair_read(const typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o,
+										  PairX px, Site<F2>& s)
+{
+	using IO = PairIO<S>;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (!ODD)
+				s.f[q] = IO::template load2<q>(f + q * sq + base);
+			else {
+				// direction q of site x comes from slot opp(q) of site x - c_q
+				const typename S::T* c = f + opp(q) * sq + base + o.y[1 - cy(q)] + o.z[1 - cz(q)];
+				if constexpr (cx(q) == 0)
+					s.f[q] = IO::template load2<opp(q)>(c);
+				else if constexpr (cx(q) > 0)
+					s.f[q] = F2(S::template load<opp(q)>(c + px.left), S::template load<opp(q)>(c));
+				else
+					s.f[q] = F2(S::template load<opp(q)>(c + 1), S::template load<opp(q)>(c + 1 + px.right));
+			}
+		}
+	);
+}
+
+// A-A write of both sites, the mirror of pair_read
+template <typename S, bool ODD>
+__device__ __forceinline__ void pair_write(typename S::T* __restrict__ f, long long sq, long long base, const Offsets& o, PairX px,
+										   const Site<F2>& s)
+{
+	using IO = PairIO<S>;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (!ODD)
+				IO::template store2<opp(q)>(f + opp(q) * sq + base, s.f[q]);
+			else {
+				// direction q of site x goes to slot q of site x + c_q
+				typename S::T* c = f + q * sq + base + o.y[1 + cy(q)] + o.z[1 + cz(q)];
+				if constexpr (cx(q) == 0)
+					IO::template store2<q>(c, s.f[q]);
+				else if constexpr (cx(q) > 0) {
+					S::template store<q>(c + 1, s.f[q].v.x);
+					S::template store<q>(c + 1 + px.right, s.f[q].v.y);
+				}
+				else {
+					S::template store<q>(c + px.left, s.f[q].v.x);
+					S::template store<q>(c, s.f[q].v.y);
+				}
+			}
+		}
+	);
+}
+
+// outputs of an observation step for both sites (step_outputs of the scalar
+// kernel); in = site inside the lattice
+template <typename T>
+__device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool inA, bool inB, long long site, const Site<F2>& s)
+{
+	if (a.macro) {
+		const long long n = (long long) a.X * a.Y * a.Z;
+		const F2 m[4] = {s.rho, s.vx, s.vy, s.vz};
+#pragma unroll
+		for (int k = 0; k < 4; k++) {
+			if (inA)
+				a.macro[k * n + site] = m[k].v.x;
+			if (inB)
+				a.macro[k * n + site + 1] = m[k].v.y;
+		}
+	}
+	if (a.partials) {
+		double red[NRED] = {0, 0, 0, 0, 0, 0};
+		if (inA) {
+			const double rho = s.rho.v.x, vx = s.vx.v.x, vy = s.vy.v.x, vz = s.vz.v.x;
+			red[0] = rho;
+			red[1] = rho * vx;
+			red[2] = rho * vy;
+			red[3] = rho * vz;
+			red[4] = rho * (vx * vx + vy * vy + vz * vz);
+			red[5] = isfinite(rho) ? 0.0 : 1.0;
+		}
+		if (inB) {
+			const double rho = s.rho.v.y, vx = s.vx.v.y, vy = s.vy.v.y, vz = s.vz.v.y;
+			red[0] += rho;
+			red[1] += rho * vx;
+			red[2] += rho * vy;
+			red[3] += rho * vz;
+			red[4] += rho * (vx * vx + vy * vy + vz * vz);
+			red[5] += isfinite(rho) ? 0.0 : 1.0;
+		}
+		warp_reduce_store(red, a.partials);
+	}
+}
+
+// One A-A step, two sites per thread (cumulant collision).  Thread (t, y) of
+// the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).  Without
+// a map (GENERAL = false) every site is periodic and X is even.  With a map,
+// the lattice rows are cut into groups of PAIR_GROUP sites (32 bytes of every
+// slot row in FP32, the DRAM sector); groups[row * ceil(X / PAIR_GROUP) + x /
+// PAIR_GROUP] is PAIR_GROUP_FLUID or PAIR_GROUP_PERIODIC when every site of
+// the group has that type, and the pair kernel updates those groups only;
+// the sites of all other groups (boundaries, obstacles, the lattice ends) run
+// in aa_pair_rest_kernel, which then reads whole sectors too.  OUT (macro
+// field and partial sums) only without a map, where every thread of the grid
+// inside the lattice updates its pair.
+template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const uint8_t* __restrict__ groups)
+{
+	static_assert(!(GENERAL && OUT), "observation steps with a map run the direct kernel");
+	const int x = 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x);
+	const int y = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	bool act = x < a.X && y < a.Y;
+	long long site = 0, base = 0;
+	Site<F2> s;
+	Offsets o;
+	PairX px{-1, 1};
+	if (act) {
+		site = ((long long) z * a.Y + y) * a.X + x;
+		base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+		if constexpr (GENERAL) {
+			// a pair away from every lattice face has the same neighbours
+			// whether it wraps or not: its loads are issued together with the
+			// group flag's (and are discarded if the group is not a pair group)
+			const bool inner = x > 0 && x + 2 < a.X && y > 0 && y < a.Y - 1 && z > 0 && z < a.Z - 1;
+			if (inner) {
+				o = neighbour_offsets(false, false, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+				pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+			}
+			const int gx = (a.X + PAIR_GROUP - 1) / PAIR_GROUP;
+			const uint8_t g = groups[((long long) z * a.Y + y) * gx + x / PAIR_GROUP];
+			act = g != PAIR_GROUP_REST;
+			if (act && !inner) {
+				const bool wrap = g == PAIR_GROUP_PERIODIC;
+				o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+				px.left = (wrap && x == 0) ? a.X - 1 : -1;
+				px.right = (wrap && x + 1 == a.X - 1) ? -(a.X - 1) : 1;
+				pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+			}
+		}
+		else {
+			o = neighbour_offsets(true, a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+			px.left = x == 0 ? a.X - 1 : -1;
+			px.right = x + 1 == a.X - 1 ? -(a.X - 1) : 1;
+			pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+		}
+		if (act)
+			density_velocity(s, p2);
+	}
+	if constexpr (OUT)
+		pair_outputs(a, act, act, site, s);
+	else
+		__syncwarp();  // keeps the collision after the loads (fewer live registers)
+	if (!act)
+		return;
+	collide_cumulant<F2, CUMF>(s, p2);
+	pair_write<S, ODD>(a.f, a.sq, base, o, px, s);
+}
+
+// The sites of a lattice with a map that aa_pair_kernel leaves out (except
+// GEO_NOTHING sites), one thread per site of the host-built list
+// rest[i] = row << 32 | x with row = z Y + y (the per-site update of
+// aa_step_kernel).
+template <typename S, int CUMF, bool ODD, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	aa_pair_rest_kernel(const StepArgs<typename S::T, float> a, const unsigned long long* __restrict__ rest, long long n)
+{
+	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const unsigned long long e = rest[i];
+	const unsigned row = (unsigned) (e >> 32);
+	const int x = (int) (e & 0xffffffffu);
+	const int y = (int) (row % (unsigned) a.Y);
+	const int z = (int) (row / (unsigned) a.Y);
+	const uint8_t geo = a.map[(long long) row * a.X + x];
+	const bool wrap = geo == GEO_PERIODIC;
+	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+	const Offsets o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+	Site<float> s;
+	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+	if (apply_boundary(s, geo, a, z, y))
+		collide_cumulant<float, CUMF>(s, a.p);
+	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+}
+
+// Resident 128-thread blocks per SM requested for the pair kernel (register
+// cap 65536 / (128 n)): the largest counts that compile without spills
+// (-Xptxas -v on sm_100a).
+template <int CUMF, bool ODD>
+constexpr int pair_minb()
+{
+	// 118-128 registers; the odd step of the 2017 variant needs 140-144
+	return (CUMF & CUM_2017) && ODD ? 3 : 4;
+}
+// the rest kernel is the scalar general step: the caps of the direct kernel
+template <bool ODD>
+constexpr int pair_rest_minb()
+{
+	return ODD ? 5 : 6;
+}
+
+// One A-A step through aa_pair_kernel (and aa_pair_rest_kernel with a map);
+// cudaErrorNotSupported for what they do not cover: collisions other than the
+// cumulant, periodic lattices of odd width, observation steps of lattices with
+// a map.
+template <typename S>
+cudaError_t pair_step(const StepLaunch& L)
+{
+	using T = typename S::T;
+	static_assert(sizeof(typename S::R) == 4, "the pair kernel computes in FP32");
+	const bool general = L.map != nullptr;
+	const bool out = L.macro || L.partials;
+	if (L.coll != COLL_CUM)
+		return cudaErrorNotSupported;
+	if (L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS && L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
+		return cudaErrorInvalidValue;
+	if (general ? (out || !L.pair_rest || !L.pair_groups || L.pair_n > 0xffffffffLL * 128) : (L.g.X % 2 != 0))
+		return cudaErrorNotSupported;
+	// 8- and 4-byte alignment of every pair's first site
+	if ((L.g.x0 | L.g.sq | L.g.sy | L.g.sz) & 1)
+		return cudaErrorNotSupported;
+	StepArgs<T, float> a;
+	a.f = (T*) L.g.f;
+	a.sq = L.g.sq;
+	a.sy = L.g.sy;
+	a.sz = L.g.sz;
+	a.x0 = L.g.x0;
+	a.X = L.g.X;
+	a.Y = L.g.Y;
+	a.Z = L.g.Z;
+	a.map = L.map;
+	a.in_vx = (const float*) L.inflow[0];
+	a.in_vy = (const float*) L.inflow[1];
+	a.in_vz = (const float*) L.inflow[2];
+	a.macro = (float*) L.macro;
+	a.partials = L.partials;
+	a.zwrap = L.distributed_z ? 0 : 1;
+	a.p = make_coll_params<float>(L.p);
+	const CollParams<F2> p2 = make_coll_params<F2>(L.p);
+	const dim3 block = L.block;
+	const int pairs = (L.g.X + 1) / 2;
+	const dim3 grid((pairs + block.x - 1) / block.x, (L.g.Y + block.y - 1) / block.y, L.g.Z);
+	if (L.blocks_out)  // one partial-sum slot per warp
+		*L.blocks_out = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
+	if (L.dry_run)
+		return cudaSuccess;
+	const unsigned nrest = (unsigned) ((L.pair_n + 127) / 128);
+	// the rest sites run on the side stream, beside the pair kernel (they
+	// touch other sites), joined back before the next step
+	const bool side = general && L.pair_n > 0 && L.side_stream && L.fork_ev && L.join_ev;
+	const cudaStream_t rest_stream = side ? L.side_stream : L.stream;
+	if (side) {
+		cudaError_t e = cudaEventRecord(L.fork_ev, L.stream);
+		if (e == cudaSuccess)
+			e = cudaStreamWaitEvent(L.side_stream, L.fork_ev, 0);
+		if (e != cudaSuccess)
+			return e;
+	}
+#define LBM_PAIR_LAUNCH(CUMF, ODD)                                                                                       \
+	do {                                                                                                                 \
+		if (general) {                                                                                                   \
+			if (L.pair_n > 0)                                                                                            \
+				aa_pair_rest_kernel<S, CUMF, ODD, pair_rest_minb<ODD>()>                                                   \
+					<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, L.pair_n);                                          \
+			aa_pair_kernel<S, CUMF, ODD, true, false, pair_minb<CUMF, ODD>()>                                            \
+				<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups);                                                    \
+		}                                                                                                                \
+		else if (out)                                                                                                    \
+			aa_pair_kernel<S, CUMF, ODD, false, true, pair_minb<CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, nullptr); \
+		else                                                                                                             \
+			aa_pair_kernel<S, CUMF, ODD, false, false, pair_minb<CUMF, ODD>()>                                   \
+				<<<grid, block, 0, L.stream>>>(a, p2, nullptr);                                                                   \
+	} while (0)
+#define LBM_PAIR_PARITY(CUMF)           \
+	do {                                \
+		if (L.odd)                      \
+			LBM_PAIR_LAUNCH(CUMF, true);  \
+		else                            \
+			LBM_PAIR_LAUNCH(CUMF, false); \
+	} while (0)
+	switch (L.cum_flags) {
+		case 0:
+			LBM_PAIR_PARITY(0);
+			break;
+		case CUM_ANTIALIAS:
+			LBM_PAIR_PARITY(CUM_ANTIALIAS);
+			break;
+		case CUM_2017 | CUM_ANTIALIAS:
+			LBM_PAIR_PARITY(CUM_2017 | CUM_ANTIALIAS);
+			break;
+		default:
+			return cudaErrorInvalidValue;
+	}
+#undef LBM_PAIR_PARITY
+#undef LBM_PAIR_LAUNCH
+	if (side) {
+		cudaError_t e = cudaEventRecord(L.join_ev, L.side_stream);
+		if (e == cudaSuccess)
+			e = cudaStreamWaitEvent(L.stream, L.join_ev, 0);
+		if (e != cudaSuccess)
+			return e;
+	}
+	return cudaGetLastError();
+}
+
+}  // namespace lbm
+
+// defines cudaError_t lbm::FN(const StepLaunch&) for storage S
+#define LBM_DEFINE_PAIR_STEP(FN, S)     \
+	namespace lbm {                     \
+	cudaError_t FN(const StepLaunch& L) \
+	{                                   \
+		return pair_step<S>(L);         \
+	}                                   \
+	}

@@ -15,7 +15,7 @@ CUM_GEIER_2017, CUM_ANTIALIAS = 1, 2
 EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
 LAYOUT_INTERIOR, LAYOUT_GHOST = 0, 1
 STEP_MACRO, STEP_SUMS = 1, 2
-KERNEL_DIRECT, KERNEL_TILE, KERNEL_SPLIT = 0, 1, 3
+KERNEL_DIRECT, KERNEL_TILE, KERNEL_SPLIT, KERNEL_PAIR = 0, 1, 3, 4
 STREAMING_AA, STREAMING_AB = 0, 1
 STATUS_TIMEOUT = 1
 ADE_SRT, ADE_MRT, ADE_CLBM = 0, 1, 2
