@@ -519,7 +519,7 @@ def run_ours(args):
     alg_bytes = bytes_per_site * sites
     achieved = alg_bytes / (secs / args.steps) / 1e9
     peak, peak_kind = read_peaks()
-    traffic = read_traffic(f"{args.workload}_{args.storage}")
+    traffic = read_traffic(f"{args.workload}_{args.storage}_{kernel_name}")
 
     # e2e through the C-ABI with host buffers: per step an inlet-profile upload
     # from pinned host memory, one step with the FP64 sums, and the sums read
