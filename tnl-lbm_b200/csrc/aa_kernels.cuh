@@ -270,8 +270,9 @@ __device__ __forceinline__ bool apply_boundary(Site<R>& s, uint8_t geo, const St
 // plain levels, 9 64-bit shuffles in all instead of 5 per quantity; lane 4q
 // ends with the warp sum of quantity q.  The order of the additions is fixed.
 // Requires blockDim.x to be a multiple of 32, so that a warp is one row of
-// the block.
-__device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], double* partials)
+// the block.  The warp's slot is `slot` of `nslots` (partials[k * nslots +
+// slot]); the two-argument form numbers the warps of the launch from 0.
+__device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], double* partials, long long slot, long long nslots)
 {
 	constexpr unsigned FULL = 0xffffffffu;
 	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
@@ -292,12 +293,16 @@ __device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], doubl
 	c += __shfl_xor_sync(FULL, c, 2);
 	c += __shfl_xor_sync(FULL, c, 1);
 	const int q = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
-	if ((lane & 3) == 0 && q < NRED) {
-		const int wpb = (blockDim.x * blockDim.y) >> 5;
-		const long long nslots = (long long) gridDim.x * gridDim.y * gridDim.z * wpb;
-		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
-		partials[q * nslots + block * wpb + (tid >> 5)] = c;
-	}
+	if ((lane & 3) == 0 && q < NRED)
+		partials[q * nslots + slot] = c;
+}
+__device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], double* partials)
+{
+	const int wpb = (blockDim.x * blockDim.y) >> 5;
+	const long long nslots = (long long) gridDim.x * gridDim.y * gridDim.z * wpb;
+	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
+	const int warp = (threadIdx.x + blockDim.x * threadIdx.y) >> 5;
+	warp_reduce_store(v, partials, block * wpb + warp, nslots);
 }
 
 // Outputs of an observation step for one site: the macro field and the

@@ -66,7 +66,7 @@ struct lbm_lattice
 	long long split_n[2] = {0, 0};
 	int split_tiles_x = 0;
 	unsigned long long* pair_rest = nullptr;  // pair step: sites outside the two-site pairs (StepLaunch)
-	long long pair_n = 0;
+	long long pair_n = 0, pair_n_active = 0;  // listed sites, and those that are not GEO_NOTHING (first)
 	uint8_t* pair_groups = nullptr;  // pair step: PAIR_GROUP_* of every group of PAIR_GROUP sites (StepLaunch)
 	cudaStream_t side_stream = nullptr;	 // pair step: the rest sites' stream, with its fork / join events
 	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
@@ -106,7 +106,11 @@ struct lbm_lattice
 		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
 		const dim3 b = block();
 		const long long direct = grid_blocks() * ((b.x * b.y) / 32);
-		return tile > direct ? tile : direct;
+		// pair step: the two-site grid's warps and the rest list's
+		const long long pairs = (long long) (((d.X + 1) / 2 + b.x - 1) / b.x) * ((d.Y + b.y - 1) / b.y) * d.Z * ((b.x * b.y) / 32)
+							  + 4 * ((pair_n + 127) / 128);
+		const long long m = tile > direct ? tile : direct;
+		return m > pairs ? m : pairs;
 	}
 	void drop_graph()
 	{

@@ -76,7 +76,8 @@ struct StepLaunch
 	// pair step with a map: the sites outside the two-site kernel's pairs
 	// (row << 32 | x, row = z Y + y), GEO_NOTHING sites left out
 	const unsigned long long* pair_rest;
-	long long pair_n;
+	long long pair_n;		  // listed sites
+	long long pair_n_active;  // the first pair_n_active are not GEO_NOTHING
 	const uint8_t* pair_groups;	 // PAIR_GROUP_* per group of PAIR_GROUP sites of a row
 	// a second stream and fork / join events: the rest sites of the pair step
 	// run beside the pair kernel (null: one after the other)

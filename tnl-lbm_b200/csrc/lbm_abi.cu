@@ -195,6 +195,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.fork_ev = h->fork_ev;
 	L.join_ev = h->join_ev;
 	L.pair_n = h->pair_n;
+	L.pair_n_active = h->pair_n_active;
 	L.distributed_z = h->distributed_z;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
 	if (h->ade) {
@@ -480,11 +481,12 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		h->split_tiles_x = tx;
 		// groups of the two-site step (PAIR_GROUP sites of a row: all
 		// GEO_FLUID, all GEO_PERIODIC, or the rest) and the list of the sites
-		// of the rest groups, GEO_NOTHING sites left out
+		// of the rest groups, their GEO_NOTHING sites at the end (they only
+		// give outputs on observation steps)
 		const int X = h->d.X;
 		const int gx = (X + lbm::PAIR_GROUP - 1) / lbm::PAIR_GROUP;
 		std::vector<uint8_t> groups((size_t) gx * h->d.Y * h->d.Z);
-		std::vector<unsigned long long> rest;
+		std::vector<unsigned long long> rest, nothing;
 		for (long long row = 0; row < (long long) h->d.Y * h->d.Z; row++)
 			for (int k = 0; k < gx; k++) {
 				const int x0 = k * lbm::PAIR_GROUP;
@@ -496,8 +498,8 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 										: (first == lbm::GEO_PERIODIC ? lbm::PAIR_GROUP_PERIODIC : lbm::PAIR_GROUP_FLUID);
 				if (!same)
 					for (int x = x0; x < x0 + lbm::PAIR_GROUP && x < X; x++)
-						if (map[row * X + x] != lbm::GEO_NOTHING)
-							rest.push_back((unsigned long long) row << 32 | (unsigned) x);
+						(map[row * X + x] != lbm::GEO_NOTHING ? rest : nothing)
+							.push_back((unsigned long long) row << 32 | (unsigned) x);
 			}
 		if (!h->side_stream) {
 			LBM_CUDA(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
@@ -510,6 +512,8 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		LBM_CUDA(cudaMemcpyAsync(h->pair_groups, groups.data(), groups.size(), cudaMemcpyHostToDevice, h->stream));
 		cudaFree(h->pair_rest);
 		h->pair_rest = nullptr;
+		h->pair_n_active = (long long) rest.size();
+		rest.insert(rest.end(), nothing.begin(), nothing.end());
 		h->pair_n = (long long) rest.size();
 		LBM_CUDA(cudaMalloc(&h->pair_rest, (rest.empty() ? 1 : rest.size()) * sizeof(unsigned long long)));
 		if (!rest.empty())

@@ -266,9 +266,11 @@ __device__ __forceinline__ void pair_write(typename S::T* __restrict__ f, long l
 }
 
 // outputs of an observation step for both sites (step_outputs of the scalar
-// kernel); in = site inside the lattice
+// kernel); in = site inside the lattice; the warp's partial-sum slot is its
+// index in the launch, of nslots in all
 template <typename T>
-__device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool inA, bool inB, long long site, const Site<F2>& s)
+__device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool inA, bool inB, long long site, const Site<F2>& s,
+											 long long nslots)
 {
 	if (a.macro) {
 		const long long n = (long long) a.X * a.Y * a.Z;
@@ -301,26 +303,27 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 			red[4] += rho * (vx * vx + vy * vy + vz * vz);
 			red[5] += isfinite(rho) ? 0.0 : 1.0;
 		}
-		warp_reduce_store(red, a.partials);
+		const int wpb = (blockDim.x * blockDim.y) >> 5;
+		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
+		warp_reduce_store(red, a.partials, block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5), nslots);
 	}
 }
 
 // One A-A step, two sites per thread (cumulant collision).  Thread (t, y) of
 // the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).  Without
 // a map (GENERAL = false) every site is periodic and X is even.  With a map,
-// the lattice rows are cut into groups of PAIR_GROUP sites (32 bytes of every
-// slot row in FP32, the DRAM sector); groups[row * ceil(X / PAIR_GROUP) + x /
-// PAIR_GROUP] is PAIR_GROUP_FLUID or PAIR_GROUP_PERIODIC when every site of
-// the group has that type, and the pair kernel updates those groups only;
-// the sites of all other groups (boundaries, obstacles, the lattice ends) run
-// in aa_pair_rest_kernel, which then reads whole sectors too.  OUT (macro
-// field and partial sums) only without a map, where every thread of the grid
-// inside the lattice updates its pair.
+// the lattice rows are cut into groups of PAIR_GROUP sites (whole DRAM sectors
+// of every slot row); groups[row * ceil(X / PAIR_GROUP) + x / PAIR_GROUP] is
+// PAIR_GROUP_FLUID or PAIR_GROUP_PERIODIC when every site of the group has
+// that type, and the pair kernel updates those groups only; the sites of all
+// other groups (boundaries, obstacles, the lattice ends) run in
+// aa_pair_rest_kernel, which then reads whole sectors too.  OUT: the macro
+// field and the partial sums of the pairs it updates, in the partial-sum slots
+// of its warps (0 .. of red_slots in all; the rest kernel's follow).
 template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
-__global__ void __launch_bounds__(128, MINB)
-	aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const uint8_t* __restrict__ groups)
+__global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
+															 const uint8_t* __restrict__ groups, long long red_slots)
 {
-	static_assert(!(GENERAL && OUT), "observation steps with a map run the direct kernel");
 	const int x = 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x);
 	const int y = blockIdx.y * blockDim.y + threadIdx.y;
 	const int z = blockIdx.z;
@@ -362,7 +365,7 @@ __global__ void __launch_bounds__(128, MINB)
 			density_velocity(s, p2);
 	}
 	if constexpr (OUT)
-		pair_outputs(a, act, act, site, s);
+		pair_outputs(a, act, act, site, s, red_slots);
 	else
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
 	if (!act)
@@ -371,29 +374,69 @@ __global__ void __launch_bounds__(128, MINB)
 	pair_write<S, ODD>(a.f, a.sq, base, o, px, s);
 }
 
-// The sites of a lattice with a map that aa_pair_kernel leaves out (except
-// GEO_NOTHING sites), one thread per site of the host-built list
-// rest[i] = row << 32 | x with row = z Y + y (the per-site update of
-// aa_step_kernel).
-template <typename S, int CUMF, bool ODD, int MINB>
+// The sites of a lattice with a map that aa_pair_kernel leaves out, one
+// thread per site of the host-built list rest[i] = row << 32 | x with row =
+// z Y + y (the per-site update of aa_step_kernel; GEO_NOTHING sites only
+// give their outputs).  OUT: macro field and partial sums of the listed sites,
+// the warps' partial-sum slots from red_base on, of red_slots in all.
+template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
-	aa_pair_rest_kernel(const StepArgs<typename S::T, float> a, const unsigned long long* __restrict__ rest, long long n)
+	aa_pair_rest_kernel(const StepArgs<typename S::T, float> a, const unsigned long long* __restrict__ rest, long long n,
+						long long red_base, long long red_slots)
 {
 	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
-	if (i >= n)
+	const bool in = i < n;
+	if (!OUT && !in)
 		return;
-	const unsigned long long e = rest[i];
-	const unsigned row = (unsigned) (e >> 32);
-	const int x = (int) (e & 0xffffffffu);
-	const int y = (int) (row % (unsigned) a.Y);
-	const int z = (int) (row / (unsigned) a.Y);
-	const uint8_t geo = a.map[(long long) row * a.X + x];
-	const bool wrap = geo == GEO_PERIODIC;
-	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-	const Offsets o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
 	Site<float> s;
-	aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
-	if (apply_boundary(s, geo, a, z, y))
+	s.rho = 1.0f;
+	s.vx = s.vy = s.vz = 0.0f;
+	Offsets o;
+	long long base = 0, site = 0;
+	bool rw = false, coll = false;
+	if (in) {
+		const unsigned long long e = rest[i];
+		const unsigned row = (unsigned) (e >> 32);
+		const int x = (int) (e & 0xffffffffu);
+		const int y = (int) (row % (unsigned) a.Y);
+		const int z = (int) (row / (unsigned) a.Y);
+		site = (long long) row * a.X + x;
+		const uint8_t geo = a.map[site];
+		if (geo != GEO_NOTHING) {
+			const bool wrap = geo == GEO_PERIODIC;
+			base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
+			o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+			coll = apply_boundary(s, geo, a, z, y);
+			rw = true;
+		}
+	}
+	if constexpr (OUT) {
+		if (in && a.macro) {
+			const long long nsites = (long long) a.X * a.Y * a.Z;
+			a.macro[site] = s.rho;
+			a.macro[nsites + site] = s.vx;
+			a.macro[2 * nsites + site] = s.vy;
+			a.macro[3 * nsites + site] = s.vz;
+		}
+		if (a.partials) {
+			double red[NRED] = {0, 0, 0, 0, 0, 0};
+			if (in) {
+				const double rho = s.rho, vx = s.vx, vy = s.vy, vz = s.vz;
+				red[0] = rho;
+				red[1] = rho * vx;
+				red[2] = rho * vy;
+				red[3] = rho * vz;
+				red[4] = rho * (vx * vx + vy * vy + vz * vz);
+				red[5] = isfinite(rho) ? 0.0 : 1.0;
+			}
+			warp_reduce_store(red, a.partials, red_base + blockIdx.x * (long long) (blockDim.x >> 5) + (threadIdx.x >> 5),
+							  red_slots);
+		}
+	}
+	if (!rw)
+		return;
+	if (coll)
 		collide_cumulant<float, CUMF>(s, a.p);
 	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
 }
@@ -401,11 +444,12 @@ __global__ void __launch_bounds__(128, MINB)
 // Resident 128-thread blocks per SM requested for the pair kernel (register
 // cap 65536 / (128 n)): the largest counts that compile without spills
 // (-Xptxas -v on sm_100a).
-template <int CUMF, bool ODD>
+template <typename T, int CUMF, bool ODD>
 constexpr int pair_minb()
 {
-	// 118-128 registers; the odd step of the 2017 variant needs 140-144
-	return (CUMF & CUM_2017) && ODD ? 3 : 4;
+	// even steps fit 96 registers (5 blocks), odd steps 116-128 (4 blocks;
+	// at 5 they spill 8-32 bytes)
+	return ODD ? 4 : 5;
 }
 // the rest kernel is the scalar general step: the caps of the direct kernel
 template <bool ODD>
@@ -416,8 +460,7 @@ constexpr int pair_rest_minb()
 
 // One A-A step through aa_pair_kernel (and aa_pair_rest_kernel with a map);
 // cudaErrorNotSupported for what they do not cover: collisions other than the
-// cumulant, periodic lattices of odd width, observation steps of lattices with
-// a map.
+// cumulant, periodic lattices of odd width.
 template <typename S>
 cudaError_t pair_step(const StepLaunch& L)
 {
@@ -429,7 +472,7 @@ cudaError_t pair_step(const StepLaunch& L)
 		return cudaErrorNotSupported;
 	if (L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS && L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
 		return cudaErrorInvalidValue;
-	if (general ? (out || !L.pair_rest || !L.pair_groups || L.pair_n > 0xffffffffLL * 128) : (L.g.X % 2 != 0))
+	if (general ? (!L.pair_rest || !L.pair_groups || L.pair_n > 0xffffffffLL * 128) : (L.g.X % 2 != 0))
 		return cudaErrorNotSupported;
 	// 8- and 4-byte alignment of every pair's first site
 	if ((L.g.x0 | L.g.sq | L.g.sy | L.g.sz) & 1)
@@ -455,14 +498,19 @@ cudaError_t pair_step(const StepLaunch& L)
 	const dim3 block = L.block;
 	const int pairs = (L.g.X + 1) / 2;
 	const dim3 grid((pairs + block.x - 1) / block.x, (L.g.Y + block.y - 1) / block.y, L.g.Z);
-	if (L.blocks_out)  // one partial-sum slot per warp
-		*L.blocks_out = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
+	// the GEO_NOTHING sites at the end of the list give outputs only
+	const long long nlist = out ? L.pair_n : L.pair_n_active;
+	const unsigned nrest = general ? (unsigned) ((nlist + 127) / 128) : 0u;
+	// one partial-sum slot per warp: the pair kernel's, then the rest kernel's
+	const long long pair_slots = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
+	const long long red_slots = pair_slots + 4LL * nrest;
+	if (L.blocks_out)
+		*L.blocks_out = red_slots;
 	if (L.dry_run)
 		return cudaSuccess;
-	const unsigned nrest = (unsigned) ((L.pair_n + 127) / 128);
 	// the rest sites run on the side stream, beside the pair kernel (they
 	// touch other sites), joined back before the next step
-	const bool side = general && L.pair_n > 0 && L.side_stream && L.fork_ev && L.join_ev;
+	const bool side = nrest > 0 && L.side_stream && L.fork_ev && L.join_ev;
 	const cudaStream_t rest_stream = side ? L.side_stream : L.stream;
 	if (side) {
 		cudaError_t e = cudaEventRecord(L.fork_ev, L.stream);
@@ -471,20 +519,30 @@ cudaError_t pair_step(const StepLaunch& L)
 		if (e != cudaSuccess)
 			return e;
 	}
-#define LBM_PAIR_LAUNCH(CUMF, ODD)                                                                                       \
-	do {                                                                                                                 \
-		if (general) {                                                                                                   \
-			if (L.pair_n > 0)                                                                                            \
-				aa_pair_rest_kernel<S, CUMF, ODD, pair_rest_minb<ODD>()>                                                   \
-					<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, L.pair_n);                                          \
-			aa_pair_kernel<S, CUMF, ODD, true, false, pair_minb<CUMF, ODD>()>                                            \
-				<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups);                                                    \
-		}                                                                                                                \
-		else if (out)                                                                                                    \
-			aa_pair_kernel<S, CUMF, ODD, false, true, pair_minb<CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, nullptr); \
-		else                                                                                                             \
-			aa_pair_kernel<S, CUMF, ODD, false, false, pair_minb<CUMF, ODD>()>                                   \
-				<<<grid, block, 0, L.stream>>>(a, p2, nullptr);                                                                   \
+#define LBM_PAIR_LAUNCH(CUMF, ODD)                                                                                        \
+	do {                                                                                                                  \
+		if (general) {                                                                                                    \
+			if (nrest > 0) {                                                                                              \
+				if (out)                                                                                                  \
+					aa_pair_rest_kernel<S, CUMF, ODD, true, pair_rest_minb<ODD>()>                                        \
+						<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, nlist, pair_slots, red_slots);                \
+				else                                                                                                      \
+					aa_pair_rest_kernel<S, CUMF, ODD, false, pair_rest_minb<ODD>()>                                       \
+						<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, nlist, pair_slots, red_slots);                \
+			}                                                                                                             \
+			if (out)                                                                                                      \
+				aa_pair_kernel<S, CUMF, ODD, true, true, pair_minb<T, CUMF, ODD>()>                                          \
+					<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups, red_slots);                                      \
+			else                                                                                                          \
+				aa_pair_kernel<S, CUMF, ODD, true, false, pair_minb<T, CUMF, ODD>()>                                         \
+					<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups, red_slots);                                      \
+		}                                                                                                                 \
+		else if (out)                                                                                                     \
+			aa_pair_kernel<S, CUMF, ODD, false, true, pair_minb<T, CUMF, ODD>()>                                             \
+				<<<grid, block, 0, L.stream>>>(a, p2, nullptr, red_slots);                                                \
+		else                                                                                                              \
+			aa_pair_kernel<S, CUMF, ODD, false, false, pair_minb<T, CUMF, ODD>()>                                            \
+				<<<grid, block, 0, L.stream>>>(a, p2, nullptr, red_slots);                                                \
 	} while (0)
 #define LBM_PAIR_PARITY(CUMF)           \
 	do {                                \
