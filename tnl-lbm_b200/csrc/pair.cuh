@@ -447,9 +447,10 @@ __global__ void __launch_bounds__(128, MINB)
 template <typename T, int CUMF, bool ODD>
 constexpr int pair_minb()
 {
-	// even steps fit 96 registers (5 blocks), odd steps 116-128 (4 blocks;
-	// at 5 they spill 8-32 bytes)
-	return ODD ? 4 : 5;
+	// even steps fit 96 registers without spills; odd steps spill 8-32 bytes
+	// at 96 and still run faster than at 4 blocks (116-128 registers): duct
+	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks
+	return 5;
 }
 // the rest kernel is the scalar general step: the caps of the direct kernel
 template <bool ODD>
