@@ -99,7 +99,8 @@ def run_ensemble(args):
     ens.init_taylor_green(0.05)
     # every launch shape, timed over 256 steps, then the autotuner's choice
     shapes = {}
-    for tile, gp in ((128, 0), (256, 0), (128, 1), (128, 2)):
+    cands = ((128, 0), (256, 0), (128, 1), (128, 2)) + (((256, 3),) if args.storage != "f64" else ())
+    for tile, gp in cands:
         ens.set_shape(tile, gp)
         ens.step(16)
         ens.synchronize()
@@ -177,7 +178,8 @@ def run_ensemble(args):
                        "storage": args.storage, "parallelism": f"replicas x{world}",
                        "launch": {"tile_sites": shape[0],
                                   "grid": ["persistent", "one block per tile",
-                                           "per-member launches in concurrent graph branches"][shape[1]],
+                                           "per-member launches in concurrent graph branches",
+                                           "persistent, two sites per thread (packed FP32)"][shape[1]],
                                   "autotuned": True},
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (27 * bpe * sites / 1e9)},
             "gpu_launches": args.steps,

@@ -55,6 +55,11 @@ constexpr int ab_minb()
 #define ENS_MINB128 5
 #endif
 
+// resident 128-thread blocks per SM of the persistent two-site ensemble kernel
+#ifndef ENS_PAIR_MINB
+#define ENS_PAIR_MINB 4
+#endif
+
 // Resident blocks per SM for the fluid-only launch of the split step (no map,
 // no boundary branch): the largest counts without register spills.
 template <typename R, int COLL, bool ODD>
@@ -347,6 +352,7 @@ struct StorageUnit
 		e.dx = make_fast_div(g.X);
 		e.dy = make_fast_div(g.Y);
 		e.p = make_coll_params<R>(pd);
+		e.p2 = make_coll_params<F2>(pd);
 		memcpy(dst, &e, sizeof(e));
 	}
 
@@ -390,10 +396,59 @@ struct StorageUnit
 		return cudaGetLastError();
 	}
 
+	// grid policy 3: the persistent two-site kernel over tiles of 256 sites
+	template <int CUMF, bool ODD, bool OUT>
+	static cudaError_t ens_pair_launch(const EnsLaunch& L)
+	{
+		if constexpr (sizeof(R) != 4) {
+			(void) L;
+			return cudaErrorNotSupported;
+		}
+		else {
+			auto kern = ens_pair_kernel<S, CUMF, ODD, OUT, ENS_PAIR_MINB>;
+			static int per_sm_cache[64] = {0};
+			static int sms_cache[64] = {0};
+			int dev = 0;
+			cudaGetDevice(&dev);
+			if (dev < 0 || dev >= 64)
+				return cudaErrorInvalidDevice;
+			if (per_sm_cache[dev] == 0) {
+				int per_sm = 0, sms = 0;
+				cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0);
+				if (e != cudaSuccess)
+					return e;
+				e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+				if (e != cudaSuccess)
+					return e;
+				if (per_sm < 1)
+					return cudaErrorInvalidConfiguration;
+				per_sm_cache[dev] = per_sm;
+				sms_cache[dev] = sms;
+			}
+			long long grid = (long long) per_sm_cache[dev] * sms_cache[dev];
+			if (grid > L.ntiles)
+				grid = L.ntiles;
+			if (L.blocks_out)
+				*L.blocks_out = grid;
+			if (L.dry_run || grid < 1)
+				return cudaSuccess;
+			kern<<<(unsigned) grid, 128, 0, L.stream>>>((const EnsMember<T, float>*) L.members, L.tile_member, L.ntiles,
+														L.partials);
+			return cudaGetLastError();
+		}
+	}
+
 	template <int COLL, int CUMF>
 	static cudaError_t ens_dispatch(const EnsLaunch& L)
 	{
 		const bool out = L.partials != nullptr;
+		if (L.pair) {
+			if (COLL != COLL_CUM || L.tpb != 256)
+				return cudaErrorNotSupported;
+			if (L.odd)
+				return out ? ens_pair_launch<CUMF, true, true>(L) : ens_pair_launch<CUMF, true, false>(L);
+			return out ? ens_pair_launch<CUMF, false, true>(L) : ens_pair_launch<CUMF, false, false>(L);
+		}
 		if (L.tpb == 256) {
 			if (L.odd)
 				return out ? ens_launch<COLL, CUMF, true, true, 256>(L) : ens_launch<COLL, CUMF, true, false, 256>(L);

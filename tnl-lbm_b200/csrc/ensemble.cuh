@@ -19,6 +19,7 @@
 #pragma once
 
 #include "aa_kernels.cuh"
+#include "pair.cuh"
 
 namespace lbm {
 
@@ -58,6 +59,7 @@ struct EnsMember
 	long long tile0;   // first tile of the member in the ensemble's tile list
 	FastDiv dx, dy;	   // division by X and by Y
 	CollParams<R> p;
+	CollParams<F2> p2;	// the same constants in both lanes (two-site kernel)
 };
 
 // One A-A step of every member.  OUT: per-tile FP64 partial sums
@@ -132,6 +134,88 @@ __global__ void __launch_bounds__(TPB, MINB)
 					acc += wsum[w][threadIdx.x];
 				partials[threadIdx.x * ntiles + t] = acc;
 			}
+			__syncthreads();
+		}
+	}
+}
+
+// One A-A step of every member, two x-adjacent sites per thread (grid policy
+// 3): tiles of 256 sites, 128 threads, the per-pair code of aa_pair_kernel
+// with the member's constants.  Every member's X is even, so a tile's pairs
+// never straddle two rows.  OUT: per-tile FP64 partial sums as
+// ens_step_kernel's.
+template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	ens_pair_kernel(const EnsMember<typename S::T, float>* __restrict__ members, const int* __restrict__ tile_member,
+					long long ntiles, double* __restrict__ partials)
+{
+	using T = typename S::T;
+	__shared__ EnsMember<T, float> M;
+	constexpr int WORDS = (int) (sizeof(EnsMember<T, float>) / 4);
+	static_assert(sizeof(EnsMember<T, float>) % 4 == 0 && WORDS <= 128, "member entry size");
+	int cur = -1;
+	for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+		const int m = tile_member[t];
+		if (m != cur) {
+			__syncthreads();
+			if ((int) threadIdx.x < WORDS)
+				reinterpret_cast<unsigned*>(&M)[threadIdx.x] = reinterpret_cast<const unsigned*>(members + m)[threadIdx.x];
+			__syncthreads();
+			cur = m;
+		}
+		const unsigned i = (unsigned) ((t - M.tile0) * 256) + 2 * threadIdx.x;
+		const bool act = i < (unsigned) M.n;
+		Site<F2> s;
+		Offsets o;
+		PairX px{-1, 1};
+		long long base = 0;
+		if (act) {
+			const unsigned row = fast_div(i, M.dx);
+			const int x = (int) (i - row * (unsigned) M.X);
+			const unsigned z = fast_div(row, M.dy);
+			const int y = (int) (row - z * (unsigned) M.Y);
+			base = (long long) (z + 1) * M.sz + (long long) (y + 1) * M.sy + M.x0 + x;
+			o = neighbour_offsets(true, x, y, (int) z, M.X, M.Y, M.Z, M.sy, M.sz);
+			px.left = x == 0 ? M.X - 1 : -1;
+			px.right = x + 1 == M.X - 1 ? -(M.X - 1) : 1;
+			pair_read<S, ODD>(M.f, M.sq, base, o, px, s);
+			density_velocity(s, M.p2);
+		}
+		__syncwarp();  // keeps the collision after the loads (fewer live registers)
+		double red[NRED] = {0, 0, 0, 0, 0, 0};
+		if (act) {
+			if constexpr (OUT) {
+#pragma unroll
+				for (int l = 0; l < 2; l++) {
+					const double rho = l ? s.rho.v.y : s.rho.v.x, vx = l ? s.vx.v.y : s.vx.v.x;
+					const double vy = l ? s.vy.v.y : s.vy.v.x, vz = l ? s.vz.v.y : s.vz.v.x;
+					red[0] += rho;
+					red[1] += rho * vx;
+					red[2] += rho * vy;
+					red[3] += rho * vz;
+					red[4] += rho * (vx * vx + vy * vy + vz * vz);
+					red[5] += isfinite(rho) ? 0.0 : 1.0;
+				}
+			}
+			collide_cumulant<F2, CUMF>(s, M.p2);
+			pair_write<S, ODD>(M.f, M.sq, base, o, px, s);
+		}
+		if constexpr (OUT) {
+#pragma unroll
+			for (int k = 0; k < NRED; k++)
+#pragma unroll
+				for (int off = 16; off > 0; off >>= 1)
+					red[k] += __shfl_down_sync(0xffffffffu, red[k], off);
+			__shared__ double wsum[4][NRED];
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+			if (lane == 0)
+#pragma unroll
+				for (int k = 0; k < NRED; k++)
+					wsum[warp][k] = red[k];
+			__syncthreads();
+			if (threadIdx.x < NRED)
+				partials[threadIdx.x * ntiles + t] = ((wsum[0][threadIdx.x] + wsum[1][threadIdx.x]) + wsum[2][threadIdx.x])
+												   + wsum[3][threadIdx.x];
 			__syncthreads();
 		}
 	}

@@ -128,6 +128,7 @@ struct EnsLaunch
 	const int* tile_member;	 // member of each tile
 	long long ntiles;
 	int tpb;		   // sites per tile = threads per block: 128 or 256
+	bool pair;		   // two sites per thread (tpb = 256 sites on 128 threads, cumulant, FP32 arithmetic)
 	long long grid;	   // blocks; 0 = resident blocks per SM x SMs (persistent)
 	double* partials;  // [NRED][ntiles] or null
 	int coll, cum_flags;

@@ -129,6 +129,18 @@ struct lbm_ensemble_t
 
 namespace {
 
+// grid policy 3 (persistent two-site kernel): the cumulant on FP32
+// arithmetic, every member of even width
+bool ens_pair_ok(lbm_ensemble e)
+{
+	if (e->collision != LBM_COLL_CUM || e->ops->compute_size != 4)
+		return false;
+	for (int m = 0; m < e->count; m++)
+		if (e->g[m].X % 2 != 0)
+			return false;
+	return true;
+}
+
 int echeck(lbm_ensemble e)
 {
 	if (!e)
@@ -238,6 +250,7 @@ int ens_launch(lbm_ensemble e, bool sums, bool dry_run = false)
 	L.tile_member = e->tile_member_dev;
 	L.ntiles = e->ntiles;
 	L.tpb = e->tile_sites;
+	L.pair = e->grid_policy == 3;
 	L.grid = e->grid_policy == 1 ? e->ntiles : 0;
 	L.partials = sums ? e->partials : nullptr;
 	L.coll = e->collision;
@@ -575,8 +588,11 @@ int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy)
 {
 	if (int rc = echeck(e))
 		return rc;
-	if ((tile_sites != 128 && tile_sites != 256) || grid_policy < 0 || grid_policy > 2)
-		return efail(LBM_ERR_INVALID, "launch shape: tile_sites 128 or 256, grid_policy 0, 1 or 2");
+	if ((tile_sites != 128 && tile_sites != 256) || grid_policy < 0 || grid_policy > 3)
+		return efail(LBM_ERR_INVALID, "launch shape: tile_sites 128 or 256, grid_policy 0, 1, 2 or 3");
+	if (grid_policy == 3 && (tile_sites != 256 || !ens_pair_ok(e)))
+		return efail(LBM_ERR_UNSUPPORTED,
+					 "grid policy 3 (two-site kernel) needs tile_sites 256, the cumulant, FP32 arithmetic and members of even width");
 	if (tile_sites != e->tile_sites) {
 		ENS_CUDA(cudaStreamSynchronize(e->stream));
 		e->tile_sites = tile_sites;
@@ -618,9 +634,11 @@ int lbm_ensemble_autotune(lbm_ensemble e, int ntrials)
 	// are on (the first replay builds and warms the graph)
 	const long long chunk = e->use_graphs ? lbm_ensemble_t::GRAPH_STEPS : 2;
 	for (int tile : {128, 256}) {
-		for (int gp : {0, 1, 2}) {
+		for (int gp : {0, 1, 2, 3}) {
 			if (gp == 2 && tile != 128)
 				continue;  // the tile size does not apply to per-member launches
+			if (gp == 3 && (tile != 256 || !ens_pair_ok(e)))
+				continue;
 			if ((rc = lbm_ensemble_set_shape(e, tile, gp)))
 				break;
 			e->iteration = it0 + (it0 % 2);	 // timed steps start at an even step
