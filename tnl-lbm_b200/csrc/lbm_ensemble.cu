@@ -24,6 +24,7 @@
 
 namespace lbm {
 int record_error(int code, const char* msg);
+PairStepFn pair_step_of(int storage);  // lbm_abi.cu
 }
 
 namespace {
@@ -200,8 +201,8 @@ int ensure_lanes(lbm_ensemble e)
 	return LBM_OK;
 }
 
-// grid policy 2: every member runs the single-lattice direct kernel on its
-// lane; the lanes fork from and join into the ensemble's stream, so under
+// grid policy 2: every member runs the single-lattice step (the two-site
+// kernel where it applies, else the direct kernel) on its lane; the lanes fork from and join into the ensemble's stream, so under
 // graph capture the members become independent branches
 int ens_launch_members(lbm_ensemble e)
 {
@@ -224,7 +225,12 @@ int ens_launch_members(lbm_ensemble e)
 		L.grid = dim3((g.X + bx - 1) / bx, (g.Y + L.block.y - 1) / L.block.y, g.Z);
 		L.stream = e->lanes[m % nl];
 		L.kernel = lbm::KERNEL_DIRECT;
-		const cudaError_t err = e->ops->step(L);
+		// the two-site kernel where it applies (cumulant, FP32 arithmetic, even X)
+		cudaError_t err = cudaErrorNotSupported;
+		if (const lbm::PairStepFn pair = lbm::pair_step_of(e->storage))
+			err = pair(L);
+		if (err == cudaErrorNotSupported)
+			err = e->ops->step(L);
 		if (err != cudaSuccess)
 			return efail(LBM_ERR_CUDA, "member %d step launch failed: %s", m, cudaGetErrorString(err));
 	}
