@@ -252,10 +252,10 @@ typedef struct lbm_device_view {
 LBM_API int lbm_device_view_get(lbm_handle h, lbm_device_view* out);
 
 /* Allocation-free FP64 sums of a macro field, for callers that cannot
- * allocate device memory where they need the result: code being captured
- * into a CUDA graph, an application whose own pool allocator owns the device
- * memory, a real-time loop that must not take an allocation's implicit
- * synchronisation.  No counterpart in the reference.
+ * allocate device memory where they need the result: an application whose
+ * own pool allocator owns the device memory and forbids libraries to
+ * allocate beside it, or a real-time loop that must not take an
+ * allocation's implicit synchronisation.  No counterpart in the reference.
  *   macro   device pointer to a field [4][nsites] (rho, vx, vy, vz) of
  *           LBM_DTYPE_F64 or LBM_DTYPE_F32 values, e.g. a lattice's macro
  *           field from lbm_device_view_get

@@ -1,9 +1,8 @@
 """The allocation-free sums entry point against the regular sums, through the C-ABI.
 
 Some callers of this library cannot allocate device memory at the point where
-they want a reduction: code under CUDA-graph capture, an application whose
-own pool allocator owns the device, a real-time loop that must not stall on an
-allocation.  lbm_macro_sums_noalloc serves them: it reduces a macro field with
+they want a reduction: an application whose own pool allocator owns the
+device, or a real-time loop that must not stall on an allocation.  lbm_macro_sums_noalloc serves them: it reduces a macro field with
 partial sums kept in a fixed file-scope device array, and the caller passes
 the already-allocated input and output.  This test checks it against the
 regular path (lbm_step with LBM_STEP_SUMS, then lbm_get_sums) on two calls in

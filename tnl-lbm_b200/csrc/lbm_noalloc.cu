@@ -2,10 +2,10 @@
 // lbm_macro_sums_noalloc).
 //
 // Why it exists: some callers cannot allocate device memory at the point where
-// they want the sums.  Code that is being captured into a CUDA graph may not
-// call cudaMalloc; a host application that has handed the whole device to its
-// own pool allocator forbids stray allocations from libraries; and a real-time
-// loop cannot afford the implicit synchronisation an allocation can bring.  The
+// they want the sums.  A host application that has handed the whole device to
+// its own pool allocator forbids stray allocations from libraries, and a
+// real-time loop cannot afford the implicit synchronisation an allocation can
+// bring.  The
 // regular path (lbm_step with LBM_STEP_SUMS) keeps its per-block partial sums
 // in a buffer the handle allocates.  This entry point does the same reduction
 // with its scratch in a file-scope device array instead, so a call allocates
