@@ -600,8 +600,8 @@ def run_ours(args):
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
                        "step_kernel": kernel_name, "autotuned": bool(args.autotune),
                        "block": list(block) if kernel_name in ("direct", "pair") else f"{kernel_name} kernel, 128 threads"},
-            # the pair and split steps of a lattice with a map launch two kernels per step
-            "gpu_launches": args.steps * (2 if kernel_name in ("pair", "split") and spec["kind"] == "duct" else 1),
+            # the split step of a lattice with a map launches two kernels per step
+            "gpu_launches": args.steps * (2 if kernel_name == "split" and spec["kind"] == "duct" else 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"

@@ -122,6 +122,9 @@ enum : uint8_t
 	PAIR_GROUP_FLUID = 1,
 	PAIR_GROUP_PERIODIC = 2
 };
+// work item of the pair step with a map: a chunk of the rest-site list when
+// this bit is set, else a tile of a row
+constexpr unsigned PAIR_WORK_REST = 0x80000000u;
 
 // ---------------------------------------------------------------------------
 // population storage formats

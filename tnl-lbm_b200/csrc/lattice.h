@@ -65,11 +65,13 @@ struct lbm_lattice
 	unsigned* split_tiles = nullptr;  // split step: fluid-only tiles, then the others
 	long long split_n[2] = {0, 0};
 	int split_tiles_x = 0;
-	unsigned long long* pair_rest = nullptr;  // pair step: sites outside the two-site pairs (StepLaunch)
-	long long pair_n = 0, pair_n_active = 0;  // listed sites, and those that are not GEO_NOTHING (first)
-	uint8_t* pair_groups = nullptr;  // pair step: PAIR_GROUP_* of every group of PAIR_GROUP sites (StepLaunch)
-	cudaStream_t side_stream = nullptr;	 // pair step: the rest sites' stream, with its fork / join events
-	cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+	// pair step with a map ([0] plain steps, [1] observation steps): rest-site
+	// lists, work lists (pair.cuh aa_pair_work_kernel) and the group flags
+	unsigned long long* pair_rest[2] = {nullptr, nullptr};
+	long long pair_nrest[2] = {0, 0};
+	unsigned* pair_work[2] = {nullptr, nullptr};
+	long long pair_nwork[2] = {0, 0};
+	uint8_t* pair_groups = nullptr;  // PAIR_GROUP_* of every group of PAIR_GROUP sites
 	void* stats = nullptr;		// D3Q27_MACRO_Mean fields [9][sites], compute type
 	long long stats_count = 0;	// steps accumulated in stats
 	lbm::AdjointState* adjoint = nullptr;	 // checkpoints of lbm_adjoint_forward
@@ -106,9 +108,10 @@ struct lbm_lattice
 		const long long tile = (long long) lbm::TILE_MAX_BLOCKS_PER_SM * sms;
 		const dim3 b = block();
 		const long long direct = grid_blocks() * ((b.x * b.y) / 32);
-		// pair step: the two-site grid's warps and the rest list's
-		const long long pairs = (long long) (((d.X + 1) / 2 + b.x - 1) / b.x) * ((d.Y + b.y - 1) / b.y) * d.Z * ((b.x * b.y) / 32)
-							  + 4 * ((pair_n + 127) / 128);
+		// pair step: the two-site grid's warps, or the work list's (4 per item)
+		long long pairs = (long long) (((d.X + 1) / 2 + b.x - 1) / b.x) * ((d.Y + b.y - 1) / b.y) * d.Z * ((b.x * b.y) / 32);
+		for (long long nw : pair_nwork)
+			pairs = pairs > 4 * nw ? pairs : 4 * nw;
 		const long long m = tile > direct ? tile : direct;
 		return m > pairs ? m : pairs;
 	}

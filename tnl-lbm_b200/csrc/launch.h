@@ -50,6 +50,16 @@ struct InitSpec
 	double u0;
 };
 
+// work list of the pair step on a lattice with a map: items (pair tiles and
+// rest chunks, pair.cuh) and the rest-site list the chunks index
+struct PairWork
+{
+	const unsigned* work;
+	long long nwork;
+	const unsigned long long* rest;	 // row << 32 | x, row = z Y + y
+	long long nrest;
+};
+
 struct StepLaunch
 {
 	Geometry g;
@@ -73,16 +83,10 @@ struct StepLaunch
 	int split_tiles_x;
 	const struct AdeLaunch* ade;  // coupled D3Q7 scalar (ade.cuh), or null
 	bool distributed_z;			  // a slab: z neighbours through the ghost layer, no z wrap
-	// pair step with a map: the sites outside the two-site kernel's pairs
-	// (row << 32 | x, row = z Y + y), GEO_NOTHING sites left out
-	const unsigned long long* pair_rest;
-	long long pair_n;		  // listed sites
-	long long pair_n_active;  // the first pair_n_active are not GEO_NOTHING
+	// pair step with a map: group flags, and the work lists of plain and of
+	// observation steps (pair.cuh aa_pair_work_kernel)
 	const uint8_t* pair_groups;	 // PAIR_GROUP_* per group of PAIR_GROUP sites of a row
-	// a second stream and fork / join events: the rest sites of the pair step
-	// run beside the pair kernel (null: one after the other)
-	cudaStream_t side_stream;
-	cudaEvent_t fork_ev, join_ev;
+	PairWork pair_work, pair_work_out;
 };
 
 // the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)

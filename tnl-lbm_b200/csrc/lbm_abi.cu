@@ -189,13 +189,9 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.split_n[0] = h->split_n[0];
 	L.split_n[1] = h->split_n[1];
 	L.split_tiles_x = h->split_tiles_x;
-	L.pair_rest = h->pair_rest;
 	L.pair_groups = h->pair_groups;
-	L.side_stream = h->side_stream;
-	L.fork_ev = h->fork_ev;
-	L.join_ev = h->join_ev;
-	L.pair_n = h->pair_n;
-	L.pair_n_active = h->pair_n_active;
+	L.pair_work = lbm::PairWork{h->pair_work[0], h->pair_nwork[0], h->pair_rest[0], h->pair_nrest[0]};
+	L.pair_work_out = lbm::PairWork{h->pair_work[1], h->pair_nwork[1], h->pair_rest[1], h->pair_nrest[1]};
 	L.distributed_z = h->distributed_z;
 	const bool ab = h->streaming == LBM_STREAMING_AB;
 	if (h->ade) {
@@ -401,7 +397,10 @@ int lbm_destroy(lbm_handle h)
 	cudaFree(h->g.f);
 	cudaFree(h->f_out);
 	cudaFree(h->split_tiles);
-	cudaFree(h->pair_rest);
+	for (int k = 0; k < 2; k++) {
+		cudaFree(h->pair_rest[k]);
+		cudaFree(h->pair_work[k]);
+	}
 	cudaFree(h->pair_groups);
 	cudaFree(h->stats);
 	cudaFree(h->map);
@@ -414,12 +413,6 @@ int lbm_destroy(lbm_handle h)
 		cudaEventDestroy(h->inflow_ev);
 	if (h->halo_ev)
 		cudaEventDestroy(h->halo_ev);
-	if (h->fork_ev)
-		cudaEventDestroy(h->fork_ev);
-	if (h->join_ev)
-		cudaEventDestroy(h->join_ev);
-	if (h->side_stream)
-		cudaStreamDestroy(h->side_stream);
 	cudaFree(h->partials);
 	cudaFree(h->finish_arrived);
 	cudaFree(h->status_dev);
@@ -480,14 +473,17 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		h->split_n[1] = (long long) other.size();
 		h->split_tiles_x = tx;
 		// groups of the two-site step (PAIR_GROUP sites of a row: all
-		// GEO_FLUID, all GEO_PERIODIC, or the rest) and the list of the sites
-		// of the rest groups, their GEO_NOTHING sites at the end (they only
-		// give outputs on observation steps)
-		const int X = h->d.X;
+		// GEO_FLUID, all GEO_PERIODIC, or the rest), the sites of the rest
+		// groups in row order (without GEO_NOTHING sites for plain steps, with
+		// them for observation steps, where they give their outputs), and the
+		// work lists: per z plane the plane's tiles of 256 x-sites that hold a
+		// pair group, then the chunks of 128 rest sites that start in it
+		const int X = h->d.X, Y = h->d.Y, Z = h->d.Z;
 		const int gx = (X + lbm::PAIR_GROUP - 1) / lbm::PAIR_GROUP;
-		std::vector<uint8_t> groups((size_t) gx * h->d.Y * h->d.Z);
-		std::vector<unsigned long long> rest, nothing;
-		for (long long row = 0; row < (long long) h->d.Y * h->d.Z; row++)
+		const int tiles_x = ((X + 1) / 2 + 127) / 128;
+		std::vector<uint8_t> groups((size_t) gx * Y * Z);
+		std::vector<unsigned long long> rest[2];
+		for (long long row = 0; row < (long long) Y * Z; row++)
 			for (int k = 0; k < gx; k++) {
 				const int x0 = k * lbm::PAIR_GROUP;
 				const uint8_t first = map[row * X + x0];
@@ -497,28 +493,55 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 				groups[row * gx + k] = !same ? lbm::PAIR_GROUP_REST
 										: (first == lbm::GEO_PERIODIC ? lbm::PAIR_GROUP_PERIODIC : lbm::PAIR_GROUP_FLUID);
 				if (!same)
-					for (int x = x0; x < x0 + lbm::PAIR_GROUP && x < X; x++)
-						(map[row * X + x] != lbm::GEO_NOTHING ? rest : nothing)
-							.push_back((unsigned long long) row << 32 | (unsigned) x);
+					for (int x = x0; x < x0 + lbm::PAIR_GROUP && x < X; x++) {
+						const unsigned long long e = (unsigned long long) row << 32 | (unsigned) x;
+						if (map[row * X + x] != lbm::GEO_NOTHING)
+							rest[0].push_back(e);
+						rest[1].push_back(e);
+					}
 			}
-		if (!h->side_stream) {
-			LBM_CUDA(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
-			LBM_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
-			LBM_CUDA(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
+		std::vector<unsigned> work[2];
+		for (int k = 0; k < 2; k++) {
+			const long long nchunks = ((long long) rest[k].size() + 127) / 128;
+			if (nchunks > (long long) (lbm::PAIR_WORK_REST - 1) || (long long) Y * Z * tiles_x >= (long long) lbm::PAIR_WORK_REST)
+				return fail(LBM_ERR_SIZE, "lattice too large for the pair step's work list");
+			long long c = 0;
+			for (int z = 0; z < Z; z++) {
+				for (int y = 0; y < Y; y++) {
+					const long long row = (long long) z * Y + y;
+					for (int t = 0; t < tiles_x; t++) {
+						bool any = false;
+						for (int g = t * 256 / lbm::PAIR_GROUP; !any && g < gx && g < (t + 1) * 256 / lbm::PAIR_GROUP; g++)
+							any = groups[row * gx + g] != lbm::PAIR_GROUP_REST;
+						if (any)
+							work[k].push_back((unsigned) (row * tiles_x + t));
+					}
+				}
+				// chunks whose first site lies in plane z
+				while (c < nchunks && (long long) (rest[k][(size_t) c * 128] >> 32) / Y <= z)
+					work[k].push_back(lbm::PAIR_WORK_REST | (unsigned) c++);
+			}
 		}
 		cudaFree(h->pair_groups);
 		h->pair_groups = nullptr;
 		LBM_CUDA(cudaMalloc(&h->pair_groups, groups.size()));
 		LBM_CUDA(cudaMemcpyAsync(h->pair_groups, groups.data(), groups.size(), cudaMemcpyHostToDevice, h->stream));
-		cudaFree(h->pair_rest);
-		h->pair_rest = nullptr;
-		h->pair_n_active = (long long) rest.size();
-		rest.insert(rest.end(), nothing.begin(), nothing.end());
-		h->pair_n = (long long) rest.size();
-		LBM_CUDA(cudaMalloc(&h->pair_rest, (rest.empty() ? 1 : rest.size()) * sizeof(unsigned long long)));
-		if (!rest.empty())
-			LBM_CUDA(cudaMemcpyAsync(h->pair_rest, rest.data(), rest.size() * sizeof(unsigned long long),
-									 cudaMemcpyHostToDevice, h->stream));
+		for (int k = 0; k < 2; k++) {
+			cudaFree(h->pair_rest[k]);
+			cudaFree(h->pair_work[k]);
+			h->pair_rest[k] = nullptr;
+			h->pair_work[k] = nullptr;
+			h->pair_nrest[k] = (long long) rest[k].size();
+			h->pair_nwork[k] = (long long) work[k].size();
+			LBM_CUDA(cudaMalloc(&h->pair_rest[k], (rest[k].empty() ? 1 : rest[k].size()) * sizeof(unsigned long long)));
+			LBM_CUDA(cudaMalloc(&h->pair_work[k], (work[k].empty() ? 1 : work[k].size()) * sizeof(unsigned)));
+			if (!rest[k].empty())
+				LBM_CUDA(cudaMemcpyAsync(h->pair_rest[k], rest[k].data(), rest[k].size() * sizeof(unsigned long long),
+										 cudaMemcpyHostToDevice, h->stream));
+			if (!work[k].empty())
+				LBM_CUDA(cudaMemcpyAsync(h->pair_work[k], work[k].data(), work[k].size() * sizeof(unsigned),
+										 cudaMemcpyHostToDevice, h->stream));
+		}
 		LBM_CUDA(cudaStreamSynchronize(h->stream));
 		h->drop_graph();
 	}

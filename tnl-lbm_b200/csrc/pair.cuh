@@ -10,11 +10,10 @@
 // The per-site algorithm is that of aa_step_kernel (aa_kernels.cuh): A-A
 // read and write of streaming_AA.h, D3Q27_BC_All (bc.h) through
 // apply_boundary, and the cumulant collision of col_cum.h.  On a lattice with
-// a map, the pair kernel updates the pairs whose sites are both GEO_FLUID or
-// both GEO_PERIODIC, and a second launch updates every other site one thread
-// per site over the tiles that hold such sites (the inlet and outlet columns,
-// the walls); A-A sites are independent within a step, so the two launches
-// together are the same step.
+// a map, the groups of sites that are all GEO_FLUID (or all GEO_PERIODIC) take
+// the two-site update and every other site the per-site update, both in one
+// launch over a host-built work list; A-A sites are independent within a
+// step, so the order of the work items does not change the result.
 #pragma once
 
 #include "aa_kernels.cuh"
@@ -266,11 +265,11 @@ __device__ __forceinline__ void pair_write(typename S::T* __restrict__ f, long l
 }
 
 // outputs of an observation step for both sites (step_outputs of the scalar
-// kernel); in = site inside the lattice; the warp's partial-sum slot is its
-// index in the launch, of nslots in all
+// kernel); in = site inside the lattice; the warp's partial sums go to slot
+// `slot` of nslots
 template <typename T>
 __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool inA, bool inB, long long site, const Site<F2>& s,
-											 long long nslots)
+											 long long slot, long long nslots)
 {
 	if (a.macro) {
 		const long long n = (long long) a.X * a.Y * a.Z;
@@ -303,30 +302,25 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 			red[4] += rho * (vx * vx + vy * vy + vz * vz);
 			red[5] += isfinite(rho) ? 0.0 : 1.0;
 		}
-		const int wpb = (blockDim.x * blockDim.y) >> 5;
-		const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
-		warp_reduce_store(red, a.partials, block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5), nslots);
+		warp_reduce_store(red, a.partials, slot, nslots);
 	}
 }
 
-// One A-A step, two sites per thread (cumulant collision).  Thread (t, y) of
-// the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).  Without
-// a map (GENERAL = false) every site is periodic and X is even.  With a map,
-// the lattice rows are cut into groups of PAIR_GROUP sites (whole DRAM sectors
-// of every slot row); groups[row * ceil(X / PAIR_GROUP) + x / PAIR_GROUP] is
-// PAIR_GROUP_FLUID or PAIR_GROUP_PERIODIC when every site of the group has
-// that type, and the pair kernel updates those groups only; the sites of all
-// other groups (boundaries, obstacles, the lattice ends) run in
-// aa_pair_rest_kernel, which then reads whole sectors too.  OUT: the macro
-// field and the partial sums of the pairs it updates, in the partial-sum slots
-// of its warps (0 .. of red_slots in all; the rest kernel's follow).
-template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
-__global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
-															 const uint8_t* __restrict__ groups, long long red_slots)
+// The update of the pair (x, x + 1) of row (y, z), cumulant collision on two
+// lanes.  Without a map (GENERAL = false) every site is periodic and X is
+// even.  With a map, the lattice rows are cut into groups of PAIR_GROUP sites
+// (whole DRAM sectors of every slot row); groups[row * ceil(X / PAIR_GROUP) +
+// x / PAIR_GROUP] is PAIR_GROUP_FLUID or PAIR_GROUP_PERIODIC when every site
+// of the group has that type, and only those groups are updated here; the
+// sites of the other groups (boundaries, obstacles, the lattice ends) take
+// rest_update, one thread per site.  OUT: the macro field and the partial sums
+// of the pair, the warp's sums in slot `slot` of nslots.  Every thread of the
+// warp calls it (threads past the lattice with x >= X).
+template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT>
+__device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
+											const uint8_t* __restrict__ groups, int x, int y, int z, long long slot,
+											long long nslots)
 {
-	const int x = 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x);
-	const int y = blockIdx.y * blockDim.y + threadIdx.y;
-	const int z = blockIdx.z;
 	bool act = x < a.X && y < a.Y;
 	long long site = 0, base = 0;
 	Site<F2> s;
@@ -365,7 +359,7 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 			density_velocity(s, p2);
 	}
 	if constexpr (OUT)
-		pair_outputs(a, act, act, site, s, red_slots);
+		pair_outputs(a, act, act, site, s, slot, nslots);
 	else
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
 	if (!act)
@@ -374,17 +368,14 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 	pair_write<S, ODD>(a.f, a.sq, base, o, px, s);
 }
 
-// The sites of a lattice with a map that aa_pair_kernel leaves out, one
-// thread per site of the host-built list rest[i] = row << 32 | x with row =
-// z Y + y (the per-site update of aa_step_kernel; GEO_NOTHING sites only
-// give their outputs).  OUT: macro field and partial sums of the listed sites,
-// the warps' partial-sum slots from red_base on, of red_slots in all.
-template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
-__global__ void __launch_bounds__(128, MINB)
-	aa_pair_rest_kernel(const StepArgs<typename S::T, float> a, const unsigned long long* __restrict__ rest, long long n,
-						long long red_base, long long red_slots)
+// The per-site update of aa_step_kernel for entry i of a host-built site list
+// rest[i] = row << 32 | x with row = z Y + y (entries i >= n: no site);
+// GEO_NOTHING sites only give their outputs.  OUT: macro field and partial
+// sums, the warp's in slot `slot` of nslots.  Every thread of the warp calls it.
+template <typename S, int CUMF, bool ODD, bool OUT>
+__device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>& a, const unsigned long long* __restrict__ rest,
+											long long n, long long i, long long slot, long long nslots)
 {
-	const long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x;
 	const bool in = i < n;
 	if (!OUT && !in)
 		return;
@@ -430,8 +421,7 @@ __global__ void __launch_bounds__(128, MINB)
 				red[4] = rho * (vx * vx + vy * vy + vz * vz);
 				red[5] = isfinite(rho) ? 0.0 : 1.0;
 			}
-			warp_reduce_store(red, a.partials, red_base + blockIdx.x * (long long) (blockDim.x >> 5) + (threadIdx.x >> 5),
-							  red_slots);
+			warp_reduce_store(red, a.partials, slot, nslots);
 		}
 	}
 	if (!rw)
@@ -439,6 +429,46 @@ __global__ void __launch_bounds__(128, MINB)
 	if (coll)
 		collide_cumulant<float, CUMF>(s, a.p);
 	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
+}
+
+// One A-A step of a lattice without a map, two sites per thread: thread
+// (t, y) of the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).
+template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
+															 long long red_slots)
+{
+	const int wpb = (blockDim.x * blockDim.y) >> 5;
+	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
+	const long long slot = block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5);
+	pair_update<S, CUMF, ODD, false, OUT>(a, p2, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
+										  blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, slot, red_slots);
+}
+
+// One A-A step of a lattice with a map in one launch of 128-thread blocks, each
+// taking one item of a host-built work list, in z-plane order: a tile of 256
+// x-sites of one row through pair_update (item = row * tiles_x + tile), or 128
+// entries of the rest-site list through rest_update (item = PAIR_WORK_REST |
+// chunk).  A plane's rest chunks follow its pair tiles, so the rest sites
+// run while the pair tiles around them are in flight and share their DRAM
+// sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
+template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const uint8_t* __restrict__ groups,
+						const unsigned* __restrict__ work, const unsigned long long* __restrict__ rest, long long nrest,
+						int tiles_x)
+{
+	const unsigned w = work[blockIdx.x];
+	const long long slot = (long long) blockIdx.x * 4 + (threadIdx.x >> 5);
+	const long long nslots = (long long) gridDim.x * 4;
+	if (w & PAIR_WORK_REST) {
+		rest_update<S, CUMF, ODD, OUT>(a, rest, nrest, (long long) (w & ~PAIR_WORK_REST) * 128 + threadIdx.x, slot, nslots);
+	}
+	else {
+		const unsigned row = w / (unsigned) tiles_x;
+		const int x = (int) (w - row * (unsigned) tiles_x) * 256 + 2 * (int) threadIdx.x;
+		pair_update<S, CUMF, ODD, true, OUT>(a, p2, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
+											 slot, nslots);
+	}
 }
 
 // Resident 128-thread blocks per SM requested for the pair kernel (register
@@ -452,14 +482,7 @@ constexpr int pair_minb()
 	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks
 	return 5;
 }
-// the rest kernel is the scalar general step: the caps of the direct kernel
-template <bool ODD>
-constexpr int pair_rest_minb()
-{
-	return ODD ? 5 : 6;
-}
-
-// One A-A step through aa_pair_kernel (and aa_pair_rest_kernel with a map);
+// One A-A step through aa_pair_kernel (no map) or aa_pair_work_kernel (a map);
 // cudaErrorNotSupported for what they do not cover: collisions other than the
 // cumulant, periodic lattices of odd width.
 template <typename S>
@@ -473,7 +496,8 @@ cudaError_t pair_step(const StepLaunch& L)
 		return cudaErrorNotSupported;
 	if (L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS && L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
 		return cudaErrorInvalidValue;
-	if (general ? (!L.pair_rest || !L.pair_groups || L.pair_n > 0xffffffffLL * 128) : (L.g.X % 2 != 0))
+	const PairWork& W = out ? L.pair_work_out : L.pair_work;
+	if (general ? (!W.work || !L.pair_groups || W.nwork < 1) : (L.g.X % 2 != 0))
 		return cudaErrorNotSupported;
 	// 8- and 4-byte alignment of every pair's first site
 	if ((L.g.x0 | L.g.sq | L.g.sy | L.g.sz) & 1)
@@ -496,54 +520,31 @@ cudaError_t pair_step(const StepLaunch& L)
 	a.zwrap = L.distributed_z ? 0 : 1;
 	a.p = make_coll_params<float>(L.p);
 	const CollParams<F2> p2 = make_coll_params<F2>(L.p);
-	const dim3 block = L.block;
+	const dim3 block = general ? dim3(128, 1, 1) : L.block;
 	const int pairs = (L.g.X + 1) / 2;
-	const dim3 grid((pairs + block.x - 1) / block.x, (L.g.Y + block.y - 1) / block.y, L.g.Z);
-	// the GEO_NOTHING sites at the end of the list give outputs only
-	const long long nlist = out ? L.pair_n : L.pair_n_active;
-	const unsigned nrest = general ? (unsigned) ((nlist + 127) / 128) : 0u;
-	// one partial-sum slot per warp: the pair kernel's, then the rest kernel's
-	const long long pair_slots = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
-	const long long red_slots = pair_slots + 4LL * nrest;
+	const dim3 grid = general ? dim3((unsigned) W.nwork, 1, 1)
+							  : dim3((pairs + block.x - 1) / block.x, (L.g.Y + block.y - 1) / block.y, L.g.Z);
+	// one partial-sum slot per warp
+	const long long red_slots = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
 	if (L.blocks_out)
 		*L.blocks_out = red_slots;
 	if (L.dry_run)
 		return cudaSuccess;
-	// the rest sites run on the side stream, beside the pair kernel (they
-	// touch other sites), joined back before the next step
-	const bool side = nrest > 0 && L.side_stream && L.fork_ev && L.join_ev;
-	const cudaStream_t rest_stream = side ? L.side_stream : L.stream;
-	if (side) {
-		cudaError_t e = cudaEventRecord(L.fork_ev, L.stream);
-		if (e == cudaSuccess)
-			e = cudaStreamWaitEvent(L.side_stream, L.fork_ev, 0);
-		if (e != cudaSuccess)
-			return e;
-	}
+	const int tiles_x = (pairs + 127) / 128;
 #define LBM_PAIR_LAUNCH(CUMF, ODD)                                                                                        \
 	do {                                                                                                                  \
 		if (general) {                                                                                                    \
-			if (nrest > 0) {                                                                                              \
-				if (out)                                                                                                  \
-					aa_pair_rest_kernel<S, CUMF, ODD, true, pair_rest_minb<ODD>()>                                        \
-						<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, nlist, pair_slots, red_slots);                \
-				else                                                                                                      \
-					aa_pair_rest_kernel<S, CUMF, ODD, false, pair_rest_minb<ODD>()>                                       \
-						<<<nrest, 128, 0, rest_stream>>>(a, L.pair_rest, nlist, pair_slots, red_slots);                \
-			}                                                                                                             \
 			if (out)                                                                                                      \
-				aa_pair_kernel<S, CUMF, ODD, true, true, pair_minb<T, CUMF, ODD>()>                                          \
-					<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups, red_slots);                                      \
+				aa_pair_work_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(        \
+					a, p2, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 			else                                                                                                          \
-				aa_pair_kernel<S, CUMF, ODD, true, false, pair_minb<T, CUMF, ODD>()>                                         \
-					<<<grid, block, 0, L.stream>>>(a, p2, L.pair_groups, red_slots);                                      \
+				aa_pair_work_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(       \
+					a, p2, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 		}                                                                                                                 \
 		else if (out)                                                                                                     \
-			aa_pair_kernel<S, CUMF, ODD, false, true, pair_minb<T, CUMF, ODD>()>                                             \
-				<<<grid, block, 0, L.stream>>>(a, p2, nullptr, red_slots);                                                \
+			aa_pair_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, red_slots);  \
 		else                                                                                                              \
-			aa_pair_kernel<S, CUMF, ODD, false, false, pair_minb<T, CUMF, ODD>()>                                            \
-				<<<grid, block, 0, L.stream>>>(a, p2, nullptr, red_slots);                                                \
+			aa_pair_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, red_slots); \
 	} while (0)
 #define LBM_PAIR_PARITY(CUMF)           \
 	do {                                \
@@ -559,21 +560,12 @@ cudaError_t pair_step(const StepLaunch& L)
 		case CUM_ANTIALIAS:
 			LBM_PAIR_PARITY(CUM_ANTIALIAS);
 			break;
-		case CUM_2017 | CUM_ANTIALIAS:
+		default:
 			LBM_PAIR_PARITY(CUM_2017 | CUM_ANTIALIAS);
 			break;
-		default:
-			return cudaErrorInvalidValue;
 	}
 #undef LBM_PAIR_PARITY
 #undef LBM_PAIR_LAUNCH
-	if (side) {
-		cudaError_t e = cudaEventRecord(L.join_ev, L.side_stream);
-		if (e == cudaSuccess)
-			e = cudaStreamWaitEvent(L.stream, L.join_ev, 0);
-		if (e != cudaSuccess)
-			return e;
-	}
 	return cudaGetLastError();
 }
 
