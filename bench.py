@@ -599,7 +599,8 @@ def run_ours(args):
                        "streaming": "A-A in place", "parallelism": f"replicas x{world}",
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
                        "step_kernel": kernel_name, "autotuned": bool(args.autotune),
-                       "block": list(block) if kernel_name in ("direct", "pair") else f"{kernel_name} kernel, 128 threads"},
+                       "block": (list(block) if kernel_name == "direct" or (kernel_name == "pair" and spec["kind"] != "duct")
+                                 else f"{kernel_name} kernel, 128 threads")},
             # the split step of a lattice with a map launches two kernels per step
             "gpu_launches": args.steps * (2 if kernel_name == "split" and spec["kind"] == "duct" else 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
