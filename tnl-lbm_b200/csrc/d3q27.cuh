@@ -111,11 +111,12 @@ enum Geo : uint8_t
 };
 
 // Groups of the two-site step (pair.cuh): a lattice row is cut into groups of
-// PAIR_GROUP x-sites (64 bytes of a slot row in FP32, 32 in the 16-bit
-// formats: whole DRAM sectors, as the interior x = 0 of a row is 128-byte
-// aligned), and a group whose sites are all GEO_FLUID or all GEO_PERIODIC runs
-// in the two-site kernel.
-constexpr int PAIR_GROUP = 16;
+// PAIR_GROUP x-sites (32 bytes of a slot row in FP32, one DRAM sector, as the
+// interior x = 0 of a row is 128-byte aligned; 16 bytes in the 16-bit
+// formats), and a group whose sites are all GEO_FLUID or all GEO_PERIODIC
+// runs in the two-site update.  Groups of 8 took the duct 1-3 % above groups
+// of 16: half as many sites on the per-site path.
+constexpr int PAIR_GROUP = 8;
 enum : uint8_t
 {
 	PAIR_GROUP_REST = 0,
