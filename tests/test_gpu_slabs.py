@@ -1,5 +1,7 @@
 """z-slab decomposition on the GPU: slabs with halo exchange must reproduce the
-single lattice bit for bit (same per-site code, same inputs to every site).
+single lattice bit for bit (same per-site code, same inputs to every site), with
+the direct kernel and with the two-site kernel (whose slabs leave the z wrap to
+the halo exchange).
 
 All slabs run on device 0 here; across GPUs the exchange kernel reads the
 sender's memory with peer loads, the same copies over NVLink.
@@ -25,7 +27,8 @@ def pl():
 @pytest.mark.parametrize("nslabs", [1, 2, 3])
 @pytest.mark.parametrize("start", [0, 1])
 @pytest.mark.parametrize("kind", ["periodic", "duct"])
-def test_slabs_match_the_single_lattice(pl, port, storage, nslabs, start, kind):
+@pytest.mark.parametrize("kernel", ["DIRECT", "PAIR"])
+def test_slabs_match_the_single_lattice(pl, port, storage, nslabs, start, kind, kernel):
     from pytnl_lbm.slabs import SlabLattice
     X, Y, Z = 40, 10, 21
     rng = np.random.default_rng(nslabs + 10 * start)
@@ -43,6 +46,7 @@ def test_slabs_match_the_single_lattice(pl, port, storage, nslabs, start, kind):
     single = pl.LBM(X, Y, Z, periodic=periodic, **kw)
     slabs = SlabLattice(X, Y, Z, nslabs, periodic=periodic, periodic_z=periodic, **kw)
     for lat in (single, slabs):
+        lat.set_kernel(getattr(pl, "KERNEL_" + kernel))
         if not periodic:
             lat.set_map(m)
             lat.set_inflow(*inflow)

@@ -88,6 +88,11 @@ class SlabLattice:
             s.close()
         self.slabs = []
 
+    def set_kernel(self, kernel):
+        """Step kernel of every slab (lbm_set_kernel)."""
+        for lat in self.slabs:
+            lat.set_kernel(kernel)
+
     # -- distribution of global arrays ------------------------------------
     def _zslices(self, arr, axis, ghost):
         """Per-slab views of a global array along its z axis (ghost: the array
