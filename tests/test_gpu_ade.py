@@ -185,3 +185,48 @@ def test_refusals(pl):
     lat.ade_disable()
     lat.set_streaming(pl.STREAMING_AB)
     lat.close()
+
+
+@pytest.mark.parametrize("X", [37, 40])
+@pytest.mark.parametrize("flags", [0, 3])
+@pytest.mark.parametrize("ade_coll", ["SRT", "MRT", "CLBM"])
+@pytest.mark.parametrize("start,field", [(0, False), (1, True)])
+def test_two_site_coupled_step_matches_reference(pl, port, X, flags, ade_coll, start, field):
+    """The two-site coupled step (LBM_KERNEL_PAIR on FP32 storage): its plain
+    steps against the reference's coupled update, at the FP32 tolerance of the
+    one-site kernel.  The duct's inlet, outlet, wall and rim sites and the
+    scalar's boundary sites take the one-site update inside the same launch."""
+    from oracle import Reference, reference_available
+    if not reference_available(flags):
+        pytest.skip("reference harness not built")
+    ref = Reference(flags)
+    Y, Z = 11, 9
+    rng = np.random.default_rng(X + 100 * start + flags)
+    f0 = seeded_state(port, rng, X, Y, Z, eq="INV_CUM")
+    g0 = scalar_state(rng, X, Y, Z, np.float64)
+    nu, D, phi_in = 0.02, 0.013, 1.7
+    dfield = (0.005 + 0.02 * rng.random((Z, Y, X))) if field else None
+    m = duct_map(X, Y, Z, GEO["INFLOW_LEFT"], GEO["OUTFLOW_EQ"])
+    am = scalar_duct_map(X, Y, Z)
+    inflow = (0.03 * np.ones((Z, Y)), 0.002 * np.ones((Z, Y)), None)
+    steps = 7
+    lat = pl.LBM(X, Y, Z, viscosity=nu, cum_flags=flags, equilibrium=pl.EQ_INV_CUM, storage=pl.STORE_F32)
+    lat.set_map(m)
+    lat.set_inflow(*inflow)
+    lat.ade_enable(D, collision=getattr(pl, "ADE_" + ade_coll), inflow_phi=phi_in)
+    lat.ade_set_map(am)
+    if field:
+        lat.ade_set_diffusion(dfield)
+    lat.set_kernel(pl.KERNEL_PAIR)
+    lat.set_populations(f0.astype(np.float32))
+    lat.ade_set_populations(g0.astype(np.float32))
+    lat.iteration = start
+    lat.step(steps)
+    fg, gg = lat.get_populations(), lat.ade_get_populations()
+    assert lat.status() == 0
+    lat.close()
+    fo, go = np.ascontiguousarray(f0.astype(np.float32)), np.ascontiguousarray(g0.astype(np.float32))
+    ref.aa_ade_run(fo, m, go, am, coll="CUM", eq="INV_CUM", ade_coll=ade_coll, nu=nu, D=D, inflow=inflow, dfield=dfield,
+                   inflow_phi=phi_in, start_iter=start, nsteps=steps)
+    assert rel_linf(fg, fo) < 1e-5
+    assert rel_linf(gg, go) < 1e-5

@@ -82,7 +82,7 @@ struct AdeArgs
 template <int Q, typename R>
 __device__ __forceinline__ R ade_feq(R phi, R vx, R vy, R vz)
 {
-	constexpr R w = Q == 0 ? R(0.25) : R(0.125);
+	const R w = Q == 0 ? R(0.25) : R(0.125);
 	const R cu = R(cx(Q)) * vx + R(cy(Q)) * vy + R(cz(Q)) * vz;
 	return w * phi * (R(1) - R(2) * (vx * vx + vy * vy + vz * vz) + R(4) * cu + R(8) * cu * cu);
 }
@@ -262,15 +262,13 @@ __device__ __forceinline__ void ade_write(R* __restrict__ g, long long sq, long 
 #define ADE_EARLY_READ 1
 #endif
 
-// Coupled step: the direct kernel's flow update of a site, then the scalar's.
-template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
-__global__ void __launch_bounds__(128, MINB)
-	ade_step_kernel(const StepArgs<typename S::T, typename S::R> a, const AdeArgs<typename S::R> d)
+// Coupled update of site (x, y, z): the direct kernel's flow update, then the
+// scalar's.  OUT: every thread of the warp calls it (outputs are warp-wide).
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
+__device__ __forceinline__ void ade_site_update(const StepArgs<typename S::T, typename S::R>& a, const AdeArgs<typename S::R>& d,
+												int x, int y, int z)
 {
 	using R = typename S::R;
-	const int x = blockIdx.x * blockDim.x + threadIdx.x;
-	const int y = blockIdx.y * blockDim.y + threadIdx.y;
-	const int z = blockIdx.z;
 	const bool active = x < a.X && y < a.Y;
 
 	Site<R> s;
@@ -344,6 +342,15 @@ __global__ void __launch_bounds__(128, MINB)
 	}
 	if (OUT && d.phi)
 		d.phi[site] = phi;
+}
+
+// Coupled step: one thread per site.
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+	ade_step_kernel(const StepArgs<typename S::T, typename S::R> a, const AdeArgs<typename S::R> d)
+{
+	ade_site_update<S, COLL, CUMF, ODD, GENERAL, OUT>(a, d, blockIdx.x * blockDim.x + threadIdx.x,
+													  blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z);
 }
 
 }  // namespace lbm

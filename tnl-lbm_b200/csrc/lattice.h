@@ -22,7 +22,14 @@ struct AdeState
 	std::vector<uint8_t> map_host;	// host copy of the accepted ADE map
 	void* phi_buf = nullptr;		// phi of the last observation step
 	bool phi_valid = false;
+	// two-site coupled step: group flags, rest-site list and work list,
+	// rebuilt before the next pair step after either map changes
+	uint8_t* pair_groups = nullptr;
+	unsigned long long* pair_rest = nullptr;
+	unsigned* pair_work = nullptr;
+	bool pair_dirty = true;
 };
+int ade_build_pair(lbm_lattice* h);  // lbm_ade.cu
 void ade_free(AdeState*);
 }  // namespace lbm
 

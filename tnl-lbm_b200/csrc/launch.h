@@ -101,7 +101,14 @@ struct AdeLaunch
 	double inflow_phi;
 	void* phi;			  // compute-type [Z][Y][X] output of observation steps, or null
 	int coll;			  // 0 SRT, 1 MRT, 2 central-moment (CLBM)
+	// two-site coupled step (ade_pair.cuh): group flags and work list, or null
+	const uint8_t* pair_groups;
+	PairWork pair_work;
 };
+
+// two-site coupled flow + scalar step for FP32 storage (ade_pair.cuh);
+// cudaErrorNotSupported where it does not apply
+cudaError_t ade_pair_step_f32(const StepLaunch&);
 
 // step kernel variants: one thread per site with direct loads, or the
 // persistent bulk-copy pipeline of aa_tile.cuh

@@ -201,6 +201,13 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 			h->ade->phi_valid = macro;
 	}
 	cudaError_t err = cudaErrorNotSupported;
+	// the two-site coupled step (FP32 storage, plain steps of a lattice with a map)
+	if (h->ade && h->kernel == lbm::KERNEL_PAIR && h->d.storage == lbm::ST_F32 && !macro && !sums) {
+		if (h->ade->pair_dirty)
+			if (int rc = lbm::ade_build_pair(h))
+				return rc;
+		err = lbm::ade_pair_step_f32(L);
+	}
 	// the two-site kernel where it applies (the cumulant on FP32 arithmetic),
 	// else the direct kernel
 	if (!h->ade && !ab && h->kernel == lbm::KERNEL_PAIR)
@@ -449,6 +456,8 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	h->map_host.assign(map, map + n);
 	h->map_set = true;
+	if (h->ade)
+		h->ade->pair_dirty = true;  // the coupled pair step's lists follow the flow map
 	// tiles of 128 x-sites for the split step: fluid-only ones first
 	{
 		const int tx = (h->d.X + 127) / 128;
@@ -948,7 +957,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	int best_kernel = lbm::KERNEL_DIRECT;
 	const int obx = h->bx, oby = h->by;
 	// the direct and the two-site kernel take the block shape
-	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->d.collision == LBM_COLL_CUM && !h->ade
+	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->d.collision == LBM_COLL_CUM
 					  && h->streaming == LBM_STREAMING_AA;
 	for (auto& c : cands) {
 		if (c[0] > 32 && c[0] / 2 >= h->d.X)

@@ -19,6 +19,7 @@
 #include "lattice.h"
 
 namespace lbm {
+int record_error(int code, const char* msg);
 
 void ade_free(AdeState* s)
 {
@@ -28,7 +29,97 @@ void ade_free(AdeState* s)
 	cudaFree((void*) s->launch.map);
 	cudaFree((void*) s->launch.dcoef);
 	cudaFree(s->phi_buf);
+	cudaFree(s->pair_groups);
+	cudaFree(s->pair_rest);
+	cudaFree(s->pair_work);
 	delete s;
+}
+
+// Group flags, rest-site list and work list of the two-site coupled step
+// (ade_pair.cuh) from the host copies of both maps: a group of PAIR_GROUP
+// sites is a pair group when its flow sites are all GEO_FLUID (or all
+// GEO_PERIODIC) and its scalar sites all collide without a boundary rewrite
+// (ADE_FLUID, ADE_SOLID, ADE_PERIODIC); the other groups' sites are listed
+// unless both their flow and scalar types are NOTHING.  Periodic lattices
+// (no flow map) get no lists; their coupled step runs one site per thread.
+int ade_build_pair(lbm_lattice* h)
+{
+	AdeState* s = h->ade;
+	cudaFree(s->pair_groups);
+	cudaFree(s->pair_rest);
+	cudaFree(s->pair_work);
+	s->pair_groups = nullptr;
+	s->pair_rest = nullptr;
+	s->pair_work = nullptr;
+	s->launch.pair_groups = nullptr;
+	s->launch.pair_work = PairWork{nullptr, 0, nullptr, 0};
+	s->pair_dirty = false;
+	if (h->d.periodic || !h->map_set)
+		return 0;
+	const int X = h->d.X, Y = h->d.Y, Z = h->d.Z;
+	const uint8_t* fm = h->map_host.data();
+	const uint8_t* am = s->map_host.data();
+	const int gx = (X + PAIR_GROUP - 1) / PAIR_GROUP;
+	const int tiles_x = ((X + 1) / 2 + 127) / 128;
+	if ((long long) Y * Z * tiles_x >= (long long) PAIR_WORK_REST)
+		return 0;
+	std::vector<uint8_t> groups((size_t) gx * Y * Z);
+	std::vector<unsigned long long> rest;
+	for (long long row = 0; row < (long long) Y * Z; row++)
+		for (int k = 0; k < gx; k++) {
+			const int x0 = k * PAIR_GROUP;
+			const uint8_t first = fm[row * X + x0];
+			bool same = x0 + PAIR_GROUP <= X && (first == GEO_FLUID || first == GEO_PERIODIC);
+			for (int x = x0; same && x < x0 + PAIR_GROUP; x++) {
+				const uint8_t ag = am[row * X + x];
+				same = fm[row * X + x] == first && (ag == ADE_FLUID || ag == ADE_SOLID || ag == ADE_PERIODIC);
+			}
+			groups[row * gx + k] = !same ? PAIR_GROUP_REST : (first == GEO_PERIODIC ? PAIR_GROUP_PERIODIC : PAIR_GROUP_FLUID);
+			if (!same)
+				for (int x = x0; x < x0 + PAIR_GROUP && x < X; x++)
+					if (fm[row * X + x] != GEO_NOTHING || am[row * X + x] != ADE_NOTHING)
+						rest.push_back((unsigned long long) row << 32 | (unsigned) x);
+		}
+	const long long nchunks = ((long long) rest.size() + 127) / 128;
+	if (nchunks >= (long long) PAIR_WORK_REST)
+		return 0;
+	std::vector<unsigned> work;
+	long long c = 0;
+	for (int z = 0; z < Z; z++) {
+		for (int y = 0; y < Y; y++) {
+			const long long row = (long long) z * Y + y;
+			for (int t = 0; t < tiles_x; t++) {
+				bool any = false;
+				for (int g = t * 256 / PAIR_GROUP; !any && g < gx && g < (t + 1) * 256 / PAIR_GROUP; g++)
+					any = groups[row * gx + g] != PAIR_GROUP_REST;
+				if (any)
+					work.push_back((unsigned) (row * tiles_x + t));
+			}
+		}
+		while (c < nchunks && (long long) (rest[(size_t) c * 128] >> 32) / Y <= z)
+			work.push_back(PAIR_WORK_REST | (unsigned) c++);
+	}
+	if (work.empty())
+		return 0;
+	cudaError_t e = cudaMalloc(&s->pair_groups, groups.size());
+	if (e == cudaSuccess)
+		e = cudaMalloc(&s->pair_rest, (rest.empty() ? 1 : rest.size()) * sizeof(unsigned long long));
+	if (e == cudaSuccess)
+		e = cudaMalloc(&s->pair_work, work.size() * sizeof(unsigned));
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(s->pair_groups, groups.data(), groups.size(), cudaMemcpyHostToDevice, h->stream);
+	if (e == cudaSuccess && !rest.empty())
+		e = cudaMemcpyAsync(s->pair_rest, rest.data(), rest.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+							h->stream);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(s->pair_work, work.data(), work.size() * sizeof(unsigned), cudaMemcpyHostToDevice, h->stream);
+	if (e == cudaSuccess)
+		e = cudaStreamSynchronize(h->stream);
+	if (e != cudaSuccess)
+		return record_error(LBM_ERR_CUDA, cudaGetErrorString(e));
+	s->launch.pair_groups = s->pair_groups;
+	s->launch.pair_work = PairWork{s->pair_work, (long long) work.size(), s->pair_rest, (long long) rest.size()};
+	return 0;
 }
 
 }  // namespace lbm
@@ -215,6 +306,8 @@ int lbm_ade_set_map(lbm_handle h, const uint8_t* map)
 	ADE_CUDA(cudaMemcpyAsync((void*) h->ade->launch.map, h->ade->map_host.data(), (size_t) n, cudaMemcpyHostToDevice,
 							 h->stream));
 	ADE_CUDA(cudaStreamSynchronize(h->stream));
+	h->ade->pair_dirty = true;
+	h->drop_graph();
 	return LBM_OK;
 }
 

@@ -48,6 +48,16 @@ __device__ __forceinline__ F2 operator*(F2 a, F2 b)
 {
 	return F2(__fmul2_rn(a.v, b.v));
 }
+// per lane, IEEE division as the scalar form
+__device__ __forceinline__ F2 operator/(F2 a, F2 b)
+{
+	return F2(a.v.x / b.v.x, a.v.y / b.v.y);
+}
+__device__ __forceinline__ F2& operator*=(F2& a, F2 b)
+{
+	a = a * b;
+	return a;
+}
 __device__ __forceinline__ F2& operator+=(F2& a, F2 b)
 {
 	a = a + b;
