@@ -54,13 +54,13 @@ __global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __
 	const long long chunk = (nslots + gridDim.x - 1) / gridDim.x;
 	const long long b0 = blockIdx.x * chunk;
 	const long long b1 = b0 + chunk < nslots ? b0 + chunk : nslots;
-	double v[NRED];
+	// the quantities innermost: the NRED loads of a slot go out together (the
+	// order of each quantity's additions is unchanged)
+	double v[NRED] = {0, 0, 0, 0, 0, 0};
+	for (long long b = b0 + threadIdx.x; b < b1; b += FINISH_THREADS)
 #pragma unroll
-	for (int k = 0; k < NRED; k++) {
-		v[k] = 0;
-		for (long long b = b0 + threadIdx.x; b < b1; b += FINISH_THREADS)
-			v[k] += partials[k * nslots + b];
-	}
+		for (int k = 0; k < NRED; k++)
+			v[k] += __ldcs(partials + k * nslots + b);
 	block_sums(v, sh);
 	if (threadIdx.x == 0) {
 #pragma unroll
@@ -75,11 +75,12 @@ __global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __
 	__threadfence();
 	__syncthreads();  // sh is reused
 #pragma unroll
-	for (int k = 0; k < NRED; k++) {
+	for (int k = 0; k < NRED; k++)
 		v[k] = 0;
-		for (int b = threadIdx.x; b < (int) gridDim.x; b += FINISH_THREADS)
+	for (int b = threadIdx.x; b < (int) gridDim.x; b += FINISH_THREADS)
+#pragma unroll
+		for (int k = 0; k < NRED; k++)
 			v[k] += __ldcg(stage + k * FINISH_BLOCKS + b);
-	}
 	block_sums(v, sh);
 	if (threadIdx.x == 0) {
 #pragma unroll
