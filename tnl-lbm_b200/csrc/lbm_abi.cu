@@ -485,8 +485,8 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 		// GEO_FLUID, all GEO_PERIODIC, or the rest), the sites of the rest
 		// groups in row order (without GEO_NOTHING sites for plain steps, with
 		// them for observation steps, where they give their outputs), and the
-		// work lists: per z plane the plane's tiles of 256 x-sites that hold a
-		// pair group, then the chunks of 128 rest sites that start in it
+		// work lists: per z plane the chunks of 128 rest sites that start in it,
+		// then the plane's tiles of 256 x-sites that hold a pair group
 		const int X = h->d.X, Y = h->d.Y, Z = h->d.Z;
 		const int gx = (X + lbm::PAIR_GROUP - 1) / lbm::PAIR_GROUP;
 		const int tiles_x = ((X + 1) / 2 + 127) / 128;
@@ -516,6 +516,11 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 				return fail(LBM_ERR_SIZE, "lattice too large for the pair step's work list");
 			long long c = 0;
 			for (int z = 0; z < Z; z++) {
+				// the chunks whose first site lies in plane z, ahead of the plane's
+				// tiles: the slower per-site work starts first and the tiles fill in
+				// around it (duct 26.7 -> 28.3 GLUPS against chunks after the tiles)
+				while (c < nchunks && (long long) (rest[k][(size_t) c * 128] >> 32) / Y <= z)
+					work[k].push_back(lbm::PAIR_WORK_REST | (unsigned) c++);
 				for (int y = 0; y < Y; y++) {
 					const long long row = (long long) z * Y + y;
 					for (int t = 0; t < tiles_x; t++) {
@@ -526,9 +531,6 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 							work[k].push_back((unsigned) (row * tiles_x + t));
 					}
 				}
-				// chunks whose first site lies in plane z
-				while (c < nchunks && (long long) (rest[k][(size_t) c * 128] >> 32) / Y <= z)
-					work[k].push_back(lbm::PAIR_WORK_REST | (unsigned) c++);
 			}
 		}
 		cudaFree(h->pair_groups);

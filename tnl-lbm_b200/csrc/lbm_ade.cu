@@ -86,6 +86,9 @@ int ade_build_pair(lbm_lattice* h)
 	std::vector<unsigned> work;
 	long long c = 0;
 	for (int z = 0; z < Z; z++) {
+		// the plane's rest chunks first, as the flow step's work list
+		while (c < nchunks && (long long) (rest[(size_t) c * 128] >> 32) / Y <= z)
+			work.push_back(PAIR_WORK_REST | (unsigned) c++);
 		for (int y = 0; y < Y; y++) {
 			const long long row = (long long) z * Y + y;
 			for (int t = 0; t < tiles_x; t++) {
@@ -96,8 +99,6 @@ int ade_build_pair(lbm_lattice* h)
 					work.push_back((unsigned) (row * tiles_x + t));
 			}
 		}
-		while (c < nchunks && (long long) (rest[(size_t) c * 128] >> 32) / Y <= z)
-			work.push_back(PAIR_WORK_REST | (unsigned) c++);
 	}
 	if (work.empty())
 		return 0;

@@ -458,9 +458,9 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 // taking one item of a host-built work list, in z-plane order: a tile of 256
 // x-sites of one row through pair_update (item = row * tiles_x + tile), or 128
 // entries of the rest-site list through rest_update (item = PAIR_WORK_REST |
-// chunk).  A plane's rest chunks follow its pair tiles, so the rest sites
-// run while the pair tiles around them are in flight and share their DRAM
-// sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
+// chunk).  A plane's rest chunks come first and its pair tiles after them, so
+// the rest sites run while the pair tiles around them are in flight and share
+// their DRAM sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
 template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
 	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const uint8_t* __restrict__ groups,
