@@ -489,8 +489,10 @@ constexpr int pair_minb()
 {
 	// even steps fit 96 registers without spills; odd steps spill 8-32 bytes
 	// at 96 and still run faster than at 4 blocks (116-128 registers): duct
-	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks
-	return 5;
+	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks.  The
+	// even step of the 16-bit formats runs 6 blocks (80 registers, 8-32 bytes
+	// of spills): duct F16S 35.2 against 34.4 GLUPS at 5
+	return sizeof(T) == 2 && !ODD ? 6 : 5;
 }
 // One A-A step through aa_pair_kernel (no map) or aa_pair_work_kernel (a map);
 // cudaErrorNotSupported for what they do not cover: collisions other than the
