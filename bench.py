@@ -37,6 +37,9 @@ sys.path.insert(0, os.path.join(ROOT, "tnl-lbm_b200"))
 
 METRIC = "D3Q27 cumulant A-A MLUPS, % HBM roofline; FP16-store vs FP32 at stated error"
 BYTES_PER_ELEM = {"f64": 8, "f32": 4, "f32s": 4, "f16s": 2, "bf16s": 2, "f16sr": 2, "bf16sr": 2}
+# the type the populations are stored in / the type the update computes in
+DTYPE_LABEL = {"f64": "f64", "f32": "f32", "f32s": "f32", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32",
+               "f16sr": "f16-store/f32", "bf16sr": "bf16-store/f32"}
 
 
 def workload_spec(name):
@@ -171,8 +174,7 @@ def run_ensemble(args):
             "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(secs_max / args.steps * 1e3, 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f64": "f64", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32", "f16sr": "f16-store/f32",
-                                                            "bf16sr": "bf16-store/f32"}.get(args.storage, "f32"),
+            "dtype": DTYPE_LABEL[args.storage],
             "data": "synthetic (seeded member sizes, viscosities and Taylor-Green initial states)",
             "config": {"workload": spec["workload"], "members": len(sizes), "sites": sites,
                        "storage": args.storage, "parallelism": f"replicas x{world}",
@@ -277,6 +279,33 @@ def duct_setup(X, Y, Z, seed=1234):
     return m, prof, nu, (rho, vx, vy, vz)
 
 
+def workload_config(spec, storage, world):
+    """The workload description both arms print as `config` (same keys and
+    values for the same workload, so that the arms compare like for like)."""
+    X, Y, Z = spec["X"], spec["Y"], spec["Z"]
+    bpe = BYTES_PER_ELEM[storage]
+    return {"workload": spec["workload"], "lattice": [X, Y, Z], "storage": storage,
+            "collision": "cumulant" + (" Geier-2017+antialias" if spec["cum_flags"] == 3 else " default"),
+            "streaming": "A-A in place", "parallelism": f"replicas x{world}",
+            "l2": "populations (%.2f GB) larger than L2; no flush" % (27 * bpe * X * Y * Z / 1e9)}
+
+
+def cpu_description():
+    """Model name, logical CPUs and the vector ISA level of the timed CPU build."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    sys.path.insert(0, ROOT)
+    import oracle
+    return {"model": model, "logical_cpus": os.cpu_count(), "isa": oracle.host_isa_level()}
+
+
 def read_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -297,26 +326,79 @@ def read_traffic(key):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clocks and clock-event reasons sampled in-process through NVML
+    during a region: one sample on entry, one every `period_s` from a
+    background thread, one on exit, so that a region of a few milliseconds
+    still carries samples.  Without NVML it falls back to `nvidia-smi -lms`."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device_index):
+    def __init__(self, device_index, period_s=0.001):
         self.dev = device_index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.samples = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        power = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+        self.samples.append((float(sm), float(mx), int(reasons), power))
+
+    def _loop(self):
+        while not self._stop.wait(self.period):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        import threading
+        try:
+            self.nvml = self._nvml_handle()
+            self._nvml_sample()
+            self.source = "nvml"
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.samples = []
+        if self.nvml is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+            return
         if self.proc is None:
             return
         self.proc.terminate()
@@ -327,18 +409,23 @@ class ClockSampler:
             out, _ = self.proc.communicate()
         for line in out.strip().splitlines():
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.samples.append(parts)
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                bits = 0
+                for (name, bit), field in zip(self.REASONS, parts[5:9]):
+                    bits |= bit if field.lower() == "active" else 0
+                self.samples.append((float(parts[1]), float(parts[2]), bits, None))
 
     def summary(self):
-        if not getattr(self, "samples", None):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({name for s in self.samples for name, bit in self.REASONS if s[2] & bit})
+        out = {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm), "sm_max_mhz": max(s[1] for s in self.samples),
+               "reasons": reasons, "samples": len(self.samples), "source": self.source}
+        power = [s[3] for s in self.samples if s[3] is not None]
+        if power:
+            out["power_w_max"] = round(max(power), 1)
+        return out
 
 
 def dist_env():
@@ -590,15 +677,10 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": {"f64": "f64", "f16s": "f16-store/f32",
-                                                            "bf16s": "bf16-store/f32"}.get(args.storage, "f32"),
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE_LABEL[args.storage],
             "data": "synthetic (seeded initial state of the named configuration)",
-            "config": {"workload": spec["workload"], "lattice": [spec["X"], spec["Y"], spec["Z"]],
-                       "storage": args.storage, "collision": "cumulant" + (
-                           " Geier-2017+antialias" if spec["cum_flags"] == 3 else " default"),
-                       "streaming": "A-A in place", "parallelism": f"replicas x{world}",
-                       "l2": "populations (%.2f GB) larger than L2; no flush" % (alg_bytes / 2 / 1e9),
-                       "step_kernel": kernel_name, "autotuned": bool(args.autotune),
+            "config": workload_config(spec, args.storage, world),
+            "launch": {"step_kernel": kernel_name, "autotuned": bool(args.autotune),
                        "block": (list(block) if kernel_name == "direct" or (kernel_name == "pair" and spec["kind"] != "duct")
                                  else f"{kernel_name} kernel, 128 threads")},
             # the split step of a lattice with a map launches two kernels per step
@@ -670,16 +752,21 @@ def cpu_baseline(spec, args):
 
     # calibrate on two steps, then time about 10 s of stepping
     per_step = run(2, 0) / 2
-    steps = int(min(200, max(2, 10.0 / max(per_step, 1e-6))))
+    steps = int(min(400, max(2, 10.0 / max(per_step, 1e-6))))
     steps += steps % 2
     el = run(steps, 2)
     return {"value": round(X * Y * Z * steps / el / 1e6, 3), "unit": "MLUPS", "cores": cores, "kind": kind,
-            "sample": f"{steps} A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), OpenMP on {cores} "
-                      f"threads, loop order of state.hpp:1388-1397"}
+            "sample": f"{steps} A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), {el:.1f} s, OpenMP on "
+                      f"{cores} threads, loop order of state.hpp:1388-1397",
+            "cpu": cpu_description()}
 
 
 def run_reference(args):
-    """The reference arm: TNL-LBM's per-site code on the host cores."""
+    """The reference arm: TNL-LBM's per-site code on the host cores.
+
+    Every timed step is one A-A update of the whole workload, as in our arm.
+    Samples of `steps` steps (at most ~60 s each) repeat until at least 10 s
+    have been timed, so that the figure does not rest on a short run."""
     rank, world, local = dist_env()
     if rank != 0:
         return
@@ -710,25 +797,32 @@ def run_reference(args):
     f = impl.allocate(X, Y, Z, prec)
     impl.init_equilibrium(f, X, Y, Z, eq="INV_CUM", fields=fields)
     m16 = m.astype(np.int16)
-    # warm-up steps, then timed steps in one harness call (bounded to ~60 s)
-    _, el_w = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, nsteps=max(1, min(args.warmup, 2)), nthreads=cores,
-                          return_time=True)
-    per_step = el_w / max(1, min(args.warmup, 2))
+    warm = max(1, min(args.warmup, 2))
+    _, el_w = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, nsteps=warm, nthreads=cores, return_time=True)
+    per_step = el_w / warm
     steps = int(max(2, min(args.steps, 60.0 / max(per_step, 1e-6))))
     steps += steps % 2
-    _, el = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, start_iter=0, nsteps=steps, nthreads=cores,
-                        return_time=True)
-    value = X * Y * Z * steps / el / 1e6
-    sample = f"{steps} timed A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), OpenMP on {cores} threads"
+    it, el, reps = warm, 0.0, 0
+    while reps == 0 or el < 10.0:
+        _, e = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, start_iter=it, nsteps=steps, nthreads=cores,
+                           return_time=True)
+        el += e
+        it += steps
+        reps += 1
+    value = X * Y * Z * steps * reps / el / 1e6
+    sample = (f"{reps} samples of {steps} timed A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), "
+              f"{el:.1f} s in all, OpenMP on {cores} threads, loop order of state.hpp:1388-1397")
+    cpu = cpu_description()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "MLUPS", "n_gpus": world,
-        "steps": steps, "warmup": args.warmup, "ms_per_step": round(el / steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == np.float64 else "f32",
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(el / (steps * reps) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == np.float64 else "f32",
         "data": "synthetic (seeded initial state of the named configuration)",
-        "config": {"workload": spec["workload"], "lattice": [X, Y, Z], "storage": args.storage,
-                   "implementation": "TNL-LBM per-site headers (oracle/_ref) + reference OpenMP loop"},
+        "config": workload_config(spec, args.storage, world),
+        "implementation": "TNL-LBM per-site headers (oracle/_ref, %s build) + the reference's OpenMP loop" % cpu["isa"],
+        "repetitions": reps,
         "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "cpu": cpu},
         "e2e": {"value": round(value, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

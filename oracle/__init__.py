@@ -40,9 +40,13 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
 
 
-def build(quiet: bool = True) -> None:
-    """Compile the restatement (and the reference harness when its sources exist)."""
-    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+def build(quiet: bool = True, reference: str | None = None) -> None:
+    """Compile the restatement, and the reference harness when a reference
+    checkout is given (``reference`` or the TNL_LBM_REFERENCE environment
+    variable) and holds the sources."""
+    ref = reference or os.environ.get("TNL_LBM_REFERENCE", "")
+    cmd = ["make", "-C", HERE, "all"] + ([f"REF={ref}"] if ref else [])
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
@@ -151,6 +155,24 @@ class Port(_Base):
         return out
 
 
+_V4_FLAGS = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
+def host_isa_level() -> str:
+    """x86-64 micro-architecture level of this host that the timed reference
+    builds target: "x86-64-v4" with AVX-512 (F, BW, CD, DQ, VL), else
+    "x86-64-v3"."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return "x86-64-v4" if all(f in flags for f in _V4_FLAGS) else "x86-64-v3"
+    except OSError:
+        pass
+    return "x86-64-v3"
+
+
 _REF_VARIANTS = {0: "libref_cum_default", CUM_ANTIALIAS: "libref_cum_aa",
                  CUM_2017 | CUM_ANTIALIAS: "libref_cum_2017aa"}
 
@@ -166,6 +188,11 @@ class Reference(_Base):
     def __init__(self, cum_flags: int = 0, fast: bool = False):
         name = _REF_VARIANTS[cum_flags] + ("_fast" if fast else "")
         path = os.path.join(REFDIR, name + ".so")
+        # the timed build: the AVX-512 one where the host has AVX-512
+        v4 = os.path.join(REFDIR, name + "_v4.so")
+        if fast and host_isa_level() == "x86-64-v4" and os.path.exists(v4):
+            path = v4
+        self.path = path
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.cum_flags = cum_flags

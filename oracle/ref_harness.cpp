@@ -32,6 +32,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #ifdef _OPENMP
@@ -279,6 +280,22 @@ void canonical_to_ref(const DREAL* src, DREAL* dst, long X, long Y, long Z)
 					dst[q * XYZ + (x * (Z + 2) + z) * (Y + 2) + y] = src[q * XYZ + (z * (Y + 2) + y) * (X + 2) + x];
 }
 
+// The same conversion into a freshly allocated, untouched buffer, with the
+// (x, z) rows split over the threads as the time loop splits them (static
+// schedule), so that each thread's pages are first touched, and therefore
+// placed, on its own NUMA node as in the reference's OpenMP host path.
+template <typename DREAL, int Q = 27>
+void canonical_to_ref_first_touch(const DREAL* src, DREAL* dst, long X, long Y, long Z, int threads)
+{
+	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
+#pragma omp parallel for schedule(static) collapse(2) num_threads(threads)
+	for (long x = 0; x < X + 2; x++)
+		for (long z = 0; z < Z + 2; z++)
+			for (int q = 0; q < Q; q++)
+				for (long y = 0; y < Y + 2; y++)
+					dst[q * XYZ + (x * (Z + 2) + z) * (Y + 2) + y] = src[q * XYZ + (z * (Y + 2) + y) * (X + 2) + x];
+}
+
 template <typename DREAL, int Q = 27>
 void ref_to_canonical(const DREAL* src, DREAL* dst, long X, long Y, long Z)
 {
@@ -316,8 +333,19 @@ int run_aa(
 	if (! map_is_supported(map, n))
 		return -2;
 	const long XYZ = (X + 2) * (Y + 2) * (Z + 2);
-	std::vector<dreal> df(27 * XYZ);
-	canonical_to_ref(f_canonical, df.data(), X, Y, Z);
+	const bool sequential = map_is_order_dependent(map, n);
+#ifdef _OPENMP
+	const int threads = sequential ? 1 : (nthreads > 0 ? nthreads : omp_get_max_threads());
+#else
+	const int threads = 1;
+	(void) nthreads;
+	(void) sequential;
+#endif
+	// populations in the reference's order, first touched by the threads that
+	// update them (new[] leaves the buffer untouched)
+	std::unique_ptr<dreal[]> df_owner(new dreal[27 * XYZ]);
+	dreal* const df = df_owner.get();
+	canonical_to_ref_first_touch(f_canonical, df, X, Y, Z, threads);
 
 	std::vector<dreal> pvx, pvy, pvz;
 	auto convert_profile = [&](const double* src, std::vector<dreal>& dst) -> const dreal*
@@ -339,11 +367,11 @@ int run_aa(
 	SD.fx = (dreal) fx;
 	SD.fy = (dreal) fy;
 	SD.fz = (dreal) fz;
-	SD.dfs[df_cur] = df.data();
+	SD.dfs[df_cur] = df;
 #ifdef AB_PATTERN
 	// the write buffer starts as a copy: ghost and GEO_NOTHING entries are
 	// never written and must hold the same values in both buffers
-	std::vector<dreal> df2(df);
+	std::vector<dreal> df2(df, df + 27 * XYZ);
 	SD.dfs[df_out] = df2.data();
 #endif
 	SD.dmacro = macro;
@@ -352,13 +380,6 @@ int run_aa(
 	SD.inflow_vy = convert_profile(in_vy, pvy);
 	SD.inflow_vz = convert_profile(in_vz, pvz);
 
-	const bool sequential = map_is_order_dependent(map, n);
-#ifdef _OPENMP
-	const int threads = sequential ? 1 : (nthreads > 0 ? nthreads : omp_get_max_threads());
-#else
-	(void) nthreads;
-	(void) sequential;
-#endif
 	g_unsupported_hit = 0;
 	const auto t0 = std::chrono::steady_clock::now();
 	for (int s = 0; s < nsteps; s++) {

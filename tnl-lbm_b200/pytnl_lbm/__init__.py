@@ -270,6 +270,31 @@ class LBM:
         _abi.check(self.lib.lbm_autotune(self.h, int(ntrials)))
         return self.block()
 
+    # -- slabs of a lattice split along z (lbm_halo_*) -----------------------
+    def set_distributed_z(self, distributed=True):
+        _abi.check(self.lib.lbm_set_distributed_z(self.h, 1 if distributed else 0))
+
+    def halo_bytes(self):
+        """Bytes of one staged exchange: the nine slot planes that cross a z face."""
+        return int(self.lib.lbm_halo_bytes(self.h))
+
+    def halo_buffer(self):
+        """A device buffer of halo_bytes() bytes on this lattice's device."""
+        import torch
+        return torch.empty(self.halo_bytes(), dtype=torch.uint8, device=torch.device("cuda", self.desc.device))
+
+    def halo_pack(self, z, cz, buf):
+        """Stage the slots with c_z = cz of plane z (ghost frame) into the device
+        tensor ``buf``, on this lattice's stream."""
+        _abi.check(self.lib.lbm_halo_pack(self.h, int(z), int(cz), ctypes.c_void_p(buf.data_ptr())))
+
+    def halo_unpack(self, z, cz, buf):
+        _abi.check(self.lib.lbm_halo_unpack(self.h, int(z), int(cz), ctypes.c_void_p(buf.data_ptr())))
+
+    def halo_copy(self, z, src, src_z, cz):
+        """Plane z of this lattice <- plane src_z of ``src`` (slots with c_z = cz)."""
+        _abi.check(self.lib.lbm_halo_copy(self.h, int(z), src.h, int(src_z), int(cz)))
+
     def device_view(self):
         v = _abi.lbm_device_view()
         _abi.check(self.lib.lbm_device_view_get(self.h, ctypes.byref(v)))

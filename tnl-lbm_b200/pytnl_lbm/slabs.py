@@ -13,7 +13,8 @@ populations that left each slab into the neighbour's boundary plane
 planes with one kernel on the receiver's device (peer loads over NVLink when
 the slabs sit on different GPUs).  ``exchange_plan`` lists the copies of one
 phase; ``DistributedSlab`` runs one slab per process and carries the same
-plan over torch.distributed point-to-point operations (NCCL on GPUs).
+plan over torch.distributed point-to-point operations (NCCL on GPUs, or gloo
+with the planes staged through host memory).
 """
 from __future__ import annotations
 
@@ -166,48 +167,77 @@ class SlabLattice:
 class DistributedSlab:
     """One slab per process of a torch.distributed group (rank r owns slab r):
     the plan of ``exchange_plan`` carried by point-to-point sends and receives
-    of staged planes (NCCL between GPUs).  ``lattice`` is this rank's ``LBM``
-    slab; ``sizes`` the z extent of every rank's slab."""
+    of staged planes.  ``lattice`` is this rank's slab (an ``LBM``, or any
+    object with the same halo methods); ``sizes`` the z extent of every
+    rank's slab.
 
-    def __init__(self, lattice, sizes, periodic_z, group=None):
+    ``staging`` picks the transport buffers: ``"device"`` sends the staged
+    device buffers themselves (NCCL between GPUs), ``"host"`` copies them
+    through host memory first (gloo, or any backend without device tensors).
+    A lattice whose halo buffers already live in host memory is sent as is."""
+
+    def __init__(self, lattice, sizes, periodic_z, group=None, staging="device"):
         import torch
+        if staging not in ("device", "host"):
+            raise ValueError("staging must be 'device' or 'host'")
         self.lat = lattice
         self.sizes = list(sizes)
         self.periodic_z = bool(periodic_z)
         self.group = group
+        self.staging = staging
         self.rank = torch.distributed.get_rank(group)
-        _abi.check(lattice.lib.lbm_set_distributed_z(lattice.h, 1))
-        nbytes = int(lattice.lib.lbm_halo_bytes(lattice.h))
-        dev = torch.device("cuda", lattice.desc.device)
-        # one staging buffer per copy this rank takes part in
-        self._bufs = {}
+        if len(self.sizes) != torch.distributed.get_world_size(group):
+            raise ValueError("one slab size per rank")
+        lattice.set_distributed_z(True)
+        self._plans = {ph: exchange_plan(self.sizes, self.periodic_z, ph) for ph in (PRE, POST)}
+        # one staging buffer per copy of a phase this rank sends or receives
+        # (keys (phase, k): k the copy's position in the plan), plus its host
+        # mirror when staging through host memory
+        self._bufs, self._host = {}, {}
         for ph in (PRE, POST):
-            for k, (dst, _, src, _, _) in enumerate(exchange_plan(self.sizes, self.periodic_z, ph)):
-                if self.rank in (dst, src):
-                    self._bufs[(ph, k)] = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-        self.stream = torch.cuda.ExternalStream(lattice.device_view().stream, device=dev)
+            for k, (dst, _, src, _, _) in enumerate(self._plans[ph]):
+                if self.rank in (dst, src) and dst != src:
+                    buf = lattice.halo_buffer()
+                    self._bufs[(ph, k)] = buf
+                    if staging == "host" and buf.is_cuda:
+                        self._host[(ph, k)] = torch.empty(buf.numel(), dtype=buf.dtype, pin_memory=True)
+        self.stream = None
+        if any(b.is_cuda for b in self._bufs.values()) or hasattr(lattice, "device_view"):
+            dev = torch.device("cuda", lattice.desc.device)
+            self.stream = torch.cuda.ExternalStream(lattice.device_view().stream, device=dev)
+
+    def _wire(self, key):
+        """The tensor that travels for copy `key`."""
+        return self._host.get(key, self._bufs[key])
 
     def exchange(self, phase):
+        import contextlib
+
         import torch
         import torch.distributed as dist
-        plan = exchange_plan(self.sizes, self.periodic_z, phase)
+        ctx = torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
         ops, unpack = [], []
-        with torch.cuda.stream(self.stream):
-            for k, (dst, dz, src, sz, cz) in enumerate(plan):
-                buf = self._bufs.get((phase, k))
+        with ctx:
+            for k, (dst, dz, src, sz, cz) in enumerate(self._plans[phase]):
                 if src == self.rank and dst == self.rank:
-                    _abi.check(self.lat.lib.lbm_halo_copy(self.lat.h, dz, self.lat.h, sz, cz))
+                    self.lat.halo_copy(dz, self.lat, sz, cz)  # a slab facing itself
                 elif src == self.rank:
-                    _abi.check(self.lat.lib.lbm_halo_pack(self.lat.h, sz, cz, ctypes.c_void_p(buf.data_ptr())))
-                    ops.append(dist.P2POp(dist.isend, buf, dst, self.group))
+                    self.lat.halo_pack(sz, cz, self._bufs[(phase, k)])
+                    if (phase, k) in self._host:
+                        self._host[(phase, k)].copy_(self._bufs[(phase, k)], non_blocking=True)
+                    ops.append(dist.P2POp(dist.isend, self._wire((phase, k)), dst, self.group))
                 elif dst == self.rank:
-                    ops.append(dist.P2POp(dist.irecv, buf, src, self.group))
-                    unpack.append((dz, cz, buf))
+                    ops.append(dist.P2POp(dist.irecv, self._wire((phase, k)), src, self.group))
+                    unpack.append((dz, cz, (phase, k)))
+            if self._host and ops:
+                self.stream.synchronize()  # staged planes in host memory before they are sent
             if ops:
                 for w in dist.batch_isend_irecv(ops):
                     w.wait()
-            for dz, cz, buf in unpack:
-                _abi.check(self.lat.lib.lbm_halo_unpack(self.lat.h, dz, cz, ctypes.c_void_p(buf.data_ptr())))
+            for dz, cz, key in unpack:
+                if key in self._host:
+                    self._bufs[key].copy_(self._host[key], non_blocking=True)
+                self.lat.halo_unpack(dz, cz, self._bufs[key])
 
     def step(self, nsteps=1, macro=False, sums=False):
         for i in range(int(nsteps)):
