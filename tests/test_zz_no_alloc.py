@@ -41,11 +41,14 @@ def noalloc_fn(pl):
     return fn
 
 
+# 2048 blocks of 256 threads cover 524,288 sites in one pass; the larger
+# lattice makes every block walk its grid-stride loop more than once
+@pytest.mark.parametrize("shape", [(150, 40, 30), (128, 96, 72)], ids=["one_pass", "grid_stride"])
 @pytest.mark.parametrize("storage,dtype_code", [("F32", 1), ("F64", 0)])
-def test_noalloc_sums_match_regular_sums_on_two_calls(pl, storage, dtype_code):
+def test_noalloc_sums_match_regular_sums_on_two_calls(pl, storage, dtype_code, shape):
     import torch
     fn = noalloc_fn(pl)
-    X, Y, Z = 150, 40, 30
+    X, Y, Z = shape
     rng = np.random.default_rng(42)
     lat = pl.LBM(X, Y, Z, viscosity=0.01, cum_flags=0, storage=getattr(pl, "STORE_" + storage))
     lat.set_map(duct_map(X, Y, Z))
@@ -78,3 +81,51 @@ def test_noalloc_rejects_sizes_beyond_its_maximum(pl):
     assert b"exceed the maximum" in pl.library().lbm_last_error()
     assert fn(out.data_ptr(), 0, 0, out.data_ptr(), None) == 1
     assert fn(out.data_ptr(), 7, 16, out.data_ptr(), None) == 1
+
+
+def test_noalloc_calls_allocate_no_device_memory(pl):
+    """After the set-up call, further calls leave the device's free memory
+    unchanged (cudaMemGetInfo)."""
+    import torch
+    fn = noalloc_fn(pl)
+    X, Y, Z = 96, 40, 30
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, cum_flags=0, storage=pl.STORE_F32, periodic=True)
+    lat.init_equilibrium()
+    lat.step(2, macro=True)
+    out = torch.zeros(6, dtype=torch.float64, device="cuda")
+    view = lat.device_view()
+    assert fn(view.macro, 1, X * Y * Z, out.data_ptr(), view.stream) == 0
+    lat.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert fn(view.macro, 1, X * Y * Z, out.data_ptr(), view.stream) == 0
+    lat.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    lat.close()
+
+
+def test_noalloc_counts_a_nonfinite_density(pl):
+    """A NaN population spreads to a few sites' densities: the regular path
+    reports them (LBM_ERR_NONFINITE) and the allocation-free sums count
+    exactly the non-finite densities of the macro field."""
+    import torch
+    fn = noalloc_fn(pl)
+    X, Y, Z = 32, 16, 12
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, cum_flags=0, storage=pl.STORE_F64, periodic=True)
+    lat.init_equilibrium()
+    f = lat.get_populations()
+    f[0, 5, 6, 7] = np.nan
+    lat.set_populations(f)
+    lat.step(2, macro=True, sums=True)
+    with pytest.raises(pl.LbmError) as e:
+        lat.sums()
+    assert e.value.code == 4
+    bad = int(np.count_nonzero(~np.isfinite(lat.macro()[0])))
+    assert bad >= 1
+    out = torch.zeros(6, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        view = lat.device_view()
+        assert fn(view.macro, 0, X * Y * Z, out.data_ptr(), view.stream) == 0
+        lat.synchronize()
+        assert out.cpu().numpy()[5] == bad, f"call {call}"
+    lat.close()

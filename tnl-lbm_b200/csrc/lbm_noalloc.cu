@@ -18,9 +18,13 @@
 // fixed grid of that many blocks with a grid-stride loop, so the lattice size
 // is bounded only by LBM_NOALLOC_MAX_SITES.  Every block writes all of its
 // partials before the finishing block reads them, so nothing has to be
-// cleared between calls.  All calls share the one array: calls whose kernels
-// overlap on the GPU (different streams, or several host threads) race on it
-// and must be serialised by the caller.
+// cleared between calls.  Each GPU has its own copy of the array, so calls on
+// different devices may overlap; all calls on one device share its copy, and
+// calls whose kernels overlap on that GPU (different streams, or several host
+// threads) race on it and must be serialised by the caller.  The device
+// address is resolved once per device and kept for the life of the process:
+// after cudaDeviceReset the module is reloaded and the array may move, so the
+// entry point must not be used across a device reset.
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -128,16 +132,27 @@ LBM_API int lbm_macro_sums_noalloc(const void* macro, int dtype, int64_t nsites,
 	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
 		return reject(LBM_ERR_CUDA, "lbm_macro_sums_noalloc: no usable current CUDA device");
 	// set-up, once per device with that device current: the device address of
-	// the scratch array
+	// the scratch array, and the three reduction kernels loaded together with
+	// it (with lazy module loading, the CUDA 12 default, a kernel is otherwise
+	// loaded at its first launch, which could fall into a later capture)
 	double* scratch = nullptr;
 	{
 		std::lock_guard<std::mutex> lock(g_setup_mutex);
 		if (!g_scratch_addr[dev]) {
 			void* ptr = nullptr;
-			const cudaError_t e = cudaGetSymbolAddress(&ptr, g_sums_scratch);
+			cudaError_t e = cudaGetSymbolAddress(&ptr, g_sums_scratch);
 			if (e != cudaSuccess || !ptr)
 				return reject(LBM_ERR_CUDA, "lbm_macro_sums_noalloc: cudaGetSymbolAddress of the scratch array failed (error %lld)",
 							  (long long) e);
+			cudaFuncAttributes attr;
+			const void* kernels[3] = {(const void*) macro_partials<double>, (const void*) macro_partials<float>,
+									  (const void*) finish_partials};
+			for (const void* k : kernels) {
+				e = cudaFuncGetAttributes(&attr, k);
+				if (e != cudaSuccess)
+					return reject(LBM_ERR_CUDA, "lbm_macro_sums_noalloc: loading the reduction kernels failed (error %lld)",
+								  (long long) e);
+			}
 			g_scratch_addr[dev] = (double*) ptr;
 		}
 		scratch = g_scratch_addr[dev];
