@@ -66,6 +66,9 @@ def workload_spec(name):
                              "(Gaussian bumps, amplitude 1e-3), L2 velocity mismatch on 8 cross-sections, 4000 steps, "
                              "sqrt(N) checkpoints, FP32 storage, FP64 gradient accumulation",
                     X=256, Y=64, Z=64, kind="adjoint", cum_flags=0)
+    if name == "tgv256":
+        return dict(workload="periodic Taylor-Green vortex 256^3, U0=0.05, Re=1600", X=256, Y=256, Z=256, kind="tgv",
+                    cum_flags=3)
     if name == "tgv64":
         return dict(workload="periodic Taylor-Green vortex 64^3, U0=0.05, Re=1600", X=64, Y=64, Z=64, kind="tgv",
                     cum_flags=3)
@@ -496,6 +499,59 @@ def time_steps(pl, lat, steps, warmup, stream):
     return e0.elapsed_time(e1) / 1e3
 
 
+def duct_fp32_vs_fp64(pl, device, steps=5000, every=500):
+    """The comparison of the duct configuration: the FP32 duct (two-site
+    kernel, as timed) against an FP64 run of the same duct from the same
+    initial state, kinetic energy every `every` steps and the velocity field
+    after `steps` steps."""
+    spec = workload_spec("duct")
+    runs = {}
+    for st, kernel in (("f64", "direct"), ("f32", "pair")):
+        lat, _ = make_lattice(pl, spec, st, device, kernel)
+        ke, mass = [], []
+        t0 = time.perf_counter()
+        for c in range(steps // every):
+            lat.step(every, macro=(c == steps // every - 1), sums=True)
+            s = lat.sums()
+            ke.append(s[4])
+            mass.append(s[0])
+        runs[st] = (np.array(ke), np.array(mass), lat.macro(), time.perf_counter() - t0)
+        lat.close()
+    ke64, m64, mac64, t64 = runs["f64"]
+    ke32, m32, mac32, t32 = runs["f32"]
+    u_max = 0.04
+    ke_rel = np.abs(ke32 / ke64 - 1)
+    return {"workload": spec["workload"] + f", {steps} steps", "steps": steps,
+            "ke_rel_err_max": float(np.max(ke_rel)), "ke_rel_err_final": float(ke_rel[-1]),
+            "max_abs_du_over_umax": float(np.max(np.abs(mac32[1:] - mac64[1:])) / u_max),
+            "max_abs_drho": float(np.max(np.abs(mac32[0] - mac64[0]))),
+            "mass_rel_diff_final": float(abs(m32[-1] / m64[-1] - 1)),
+            "how": f"kinetic energy sum rho |u|^2 every {every} steps, velocity and density after the last step; "
+                   "FP64 storage on the one-site kernel, FP32 on the two-site kernel",
+            "seconds": {"f64": round(t64, 2), "f32": round(t32, 2)}}
+
+
+def tgv512_throughput(pl, device, steps, warmup, kernel16="pair"):
+    """Throughput of the largest single-GPU configuration, the 512^3
+    Taylor-Green vortex, in FP32 and in FP16 shifted storage."""
+    import torch
+    spec = workload_spec("tgv512")
+    sites = spec["X"] * spec["Y"] * spec["Z"]
+    peak, _ = read_peaks()
+    out = {"workload": spec["workload"]}
+    for st, kernel in (("f32", "pair"), ("f16s", kernel16)):
+        lat, _ = make_lattice(pl, spec, st, device, kernel)
+        stream = torch.cuda.ExternalStream(lat.device_view().stream, device=torch.device("cuda", device))
+        secs = time_steps(pl, lat, steps, warmup, stream)
+        lat.close()
+        mlups = sites * steps / secs / 1e6
+        gbs = mlups * 1e6 * 2 * 27 * BYTES_PER_ELEM[st] / 1e9
+        out[st] = {"mlups": round(mlups, 1), "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                   "step_kernel": kernel}
+    out["f16s_speedup_vs_f32"] = round(out["f16s"]["mlups"] / out["f32"]["mlups"], 3)
+    return out
+
+
 def run_adjoint(args):
     """Forward pass with checkpoints plus backward pass of the discrete adjoint;
     value = sites x steps / (forward + backward device time)."""
@@ -585,7 +641,8 @@ def run_ours(args):
     lat, prof = make_lattice(pl, spec, args.storage, local, args.kernel)
     if args.autotune:
         lat.autotune(16)  # block shape and step kernel, 16 timed steps per candidate
-    kernel_name = {pl.KERNEL_DIRECT: "direct", pl.KERNEL_TILE: "tile", pl.KERNEL_SPLIT: "split", pl.KERNEL_PAIR: "pair"}.get(lat.kernel, "direct")
+    kernel_name = {pl.KERNEL_DIRECT: "direct", pl.KERNEL_TILE: "tile", pl.KERNEL_SPLIT: "split", pl.KERNEL_PAIR: "pair"}.get(
+        lat.kernel, "direct")
     stream = torch.cuda.ExternalStream(lat.device_view().stream, device=device)
     if dist is not None:
         dist.barrier()
@@ -663,14 +720,21 @@ def run_ours(args):
     else:
         lat.close()
 
-    # the error each storage format costs: Taylor-Green 128^3, Re 1600, 5000
-    # steps (about 12 convective times, the span of the 512^3 20000-step case),
-    # kinetic energy and dissipation rate against the FP64-storage run
+    # the precision configuration: the Taylor-Green vortex at 256^3, Re 1600,
+    # 20000 steps, kinetic energy and dissipation rate of every storage format
+    # against the FP64-storage run (BF16 with round-to-nearest diverges on
+    # this case and is left out)
     precision = None
     if args.precision and rank == 0:
         from pytnl_lbm import precision as prec
-        precision = prec.study(128, 5000, 100, ("f32", "f16s", "bf16s", "f16sr", "bf16sr"), local)
+        precision = prec.study(256, 20000, 200, ("f32", "f16s", "f16sr", "bf16sr"), local)
         precision.pop("series")
+    # the duct configuration's FP32-against-FP64 comparison and the 512^3
+    # Taylor-Green throughput
+    duct_cmp = tgv512 = None
+    if args.configs and rank == 0 and spec["kind"] == "duct" and not spec.get("ade"):
+        duct_cmp = duct_fp32_vs_fp64(pl, local)
+        tgv512 = tgv512_throughput(pl, local, max(args.steps, 20), args.warmup)
 
     line = None
     if rank == 0:
@@ -703,6 +767,10 @@ def run_ours(args):
             line["storage_variants"] = variants
         if precision is not None:
             line["precision"] = precision
+        if duct_cmp is not None:
+            line["duct_fp32_vs_fp64"] = duct_cmp
+        if tgv512 is not None:
+            line["tgv512"] = tgv512
         if args.cpu_baseline and world == 1 and not spec.get("ade"):
             line["cpu_baseline"] = cpu_baseline(spec, args)
     if dist is not None:
@@ -833,11 +901,13 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="duct", choices=["duct", "duct_ade", "tgv512", "tgv64", "ensemble64", "ensemble_small", "adjoint"])
+    ap.add_argument("--workload", default="duct", choices=["duct", "duct_ade", "tgv512", "tgv256", "tgv64", "ensemble64", "ensemble_small", "adjoint"])
     ap.add_argument("--storage", default="f32", choices=list(BYTES_PER_ELEM))
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-precision", dest="precision", action="store_false")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the duct FP32-vs-FP64 comparison and the 512^3 Taylor-Green throughput")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default block shape and kernel instead of lbm_autotune's choice")
     ap.add_argument("--kernel", default="direct", choices=["direct", "tile", "split", "pair"])

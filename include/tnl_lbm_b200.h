@@ -234,9 +234,20 @@ LBM_API int lbm_checkpoint_save(lbm_handle h, const char* path);
 LBM_API int lbm_checkpoint_load(lbm_handle h, const char* path);
 
 /* Device status word: bit LBM_STATUS_TIMEOUT is set when a bounded wait inside
- * a kernel gave up (the kernel then stops early; the step's result is invalid). */
+ * a kernel gave up (the kernel then stops early; the step's result is invalid).
+ * Waits for the handle's work, returns the word and clears it.  The reference
+ * has no status word (CUDA errors throw, TNL_BACKEND_SAFE_CALL in
+ * lbm_block.hpp:132); this replaces its terminate flag (state.hpp:1486-1491)
+ * for failures inside a step. */
 #define LBM_STATUS_TIMEOUT 1
 LBM_API int lbm_status(lbm_handle h, int* status);
+/* Bound of the tile kernel's (LBM_KERNEL_TILE) per-tile mbarrier waits, in
+ * tries; a negative value restores the default (about seconds).  With 0 the
+ * waits give up at once while the tile's bulk copies are still in flight:
+ * the step stops early, sets LBM_STATUS_TIMEOUT and still waits (with the
+ * default bound) for every copy it issued, so tests can drive the timeout
+ * path without a fault.  No counterpart in the reference. */
+LBM_API int lbm_set_wait_limit(lbm_handle h, int64_t tries);
 
 /* Device view for zero-copy interop (pytnl_lbm): the population base pointer
  * and strides in elements: index(q,x,y,z) = q*sq + (z+1)*sz + (y+1)*sy + x0 + x. */
@@ -264,10 +275,13 @@ LBM_API int lbm_device_view_get(lbm_handle h, lbm_device_view* out);
  * The partial sums live in a file-scope device array of
  * LBM_NOALLOC_SCRATCH_DOUBLES doubles (96 KiB per GPU that loads the library,
  * kept until the process exits).  The call allocates nothing.  Its first
- * call on a device resolves the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  Calls share the array:
- * calls that overlap on the GPU race and must be serialised.  nsites above
- * LBM_NOALLOC_MAX_SITES returns LBM_ERR_SIZE. */
+ * call on a device resolves the array's device address (cudaGetSymbolAddress)
+ * and loads its reduction kernels, so make that first call before any stream
+ * capture; the address is kept for the life of the process, so do not call
+ * it again after a cudaDeviceReset.  The race is per device: calls on
+ * different GPUs may overlap, while calls on one GPU share its array, and
+ * calls that overlap there (other streams, other host threads) race and must
+ * be serialised.  nsites above LBM_NOALLOC_MAX_SITES returns LBM_ERR_SIZE. */
 #define LBM_NOALLOC_MAX_BLOCKS 2048
 #define LBM_NOALLOC_SCRATCH_DOUBLES (6 * LBM_NOALLOC_MAX_BLOCKS)
 #define LBM_NOALLOC_MAX_SITES ((int64_t) 1 << 40)
@@ -346,8 +360,12 @@ LBM_API int lbm_ensemble_autotune(lbm_ensemble e, int ntrials);
  * lbm_adjoint_forward starts from the current populations and iteration,
  * advances the lattice by nsteps (force NULL: the descriptor's uniform
  * force) and returns the objective.  lbm_adjoint_backward returns seed * dJ/dF
- * (host [3][Z][Y][X] doubles, or NULL) and seed * dJ/d(initial populations)
- * (layout and dtype as lbm_get_populations, or NULL).
+ * ([3][Z][Y][X] doubles, or NULL) and seed * dJ/d(initial populations)
+ * (layout and dtype as lbm_get_populations, or NULL).  force, grad_force and
+ * grad_populations may point to host or device memory (unified addressing).
+ * The adjoint populations are FP64 whatever the storage: with LBM_STORE_F32
+ * the primal runs in FP32 and its transpose is evaluated and accumulated in
+ * FP64 at the FP32 primal's values.
  * lbm_adjoint_release frees the checkpoints. */
 LBM_API int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64_t checkpoint_every,
                                 const int64_t* samples, int32_t nsamples, const double* target, double rho_weight,

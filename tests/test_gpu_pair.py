@@ -125,3 +125,4 @@ def test_autotune_may_choose_the_pair_kernel(pl):
     lat.step(4, sums=True)
     assert abs(lat.sums()[0] - 256 * 32 * 16) < 1e-3
     lat.close()
+

@@ -119,7 +119,8 @@ struct StorageUnit
 			*L.blocks_out = grid;
 		if (L.dry_run)
 			return cudaSuccess;
-		kern<<<(unsigned) grid, threads, smem, L.stream>>>(a, L.status, ntiles, tiles_x);
+		kern<<<(unsigned) grid, threads, smem, L.stream>>>(a, L.status, ntiles, tiles_x,
+														   L.wait_limit >= 0 ? L.wait_limit : WAIT_LIMIT);
 		return cudaGetLastError();
 	}
 

@@ -27,7 +27,10 @@
 //
 // Waits on mbarriers are bounded; a timeout sets LBM_STATUS_TIMEOUT in the
 // device status word, stops the tile loop and still drains the copies this
-// CTA has issued before it exits.
+// CTA has issued before it exits.  The tile loop's waits take their bound
+// from the launch (wait_limit tries, WAIT_LIMIT by default), so that a test
+// can make them run out while copies are in flight; the drain always waits
+// with the full bound, so no copy lands after the CTA has exited.
 #pragma once
 
 #include "aa_kernels.cuh"
@@ -72,10 +75,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 	return ok != 0;
 }
 
-// bounded wait on one phase of an mbarrier; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// bounded wait on one phase of an mbarrier (at most `limit` tries); false on
+// timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_LIMIT)
 {
-	for (long long i = 0; i < WAIT_LIMIT; i++)
+	for (long long i = 0; i < limit; i++)
 		if (mbar_try_wait(bar, parity))
 			return true;
 	return false;
@@ -218,7 +222,8 @@ __device__ __forceinline__ void issue_tile(const StepArgs<typename S::T, typenam
 
 template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, int TX, int STAGES>
 __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
-	aa_tile_kernel(const StepArgs<typename S::T, typename S::R> a, int* status, long long ntiles, int tiles_x)
+	aa_tile_kernel(const StepArgs<typename S::T, typename S::R> a, int* status, long long ntiles, int tiles_x,
+				   long long wait_limit)
 {
 	using R = typename S::R;
 	using T = typename S::T;
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 				phase ^= 1u;
 			}
 		}
-		if (!mbar_wait(&full[s], phase)) {
+		if (!mbar_wait(&full[s], phase, wait_limit)) {
 			timed_out = true;
 			break;
 		}
@@ -311,7 +316,7 @@ __global__ void __launch_bounds__(TX, LBM_TILE_MINB)
 		if (warp0 && i + STAGES < my_tiles) {
 			bool ok = true;
 			if (lane == 0)
-				ok = mbar_wait(&empty[s], phase);
+				ok = mbar_wait(&empty[s], phase, wait_limit);
 			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 			if (!ok) {
 				timed_out = true;

@@ -34,7 +34,7 @@ template <typename T, typename R>
 struct AdjArgs
 {
 	T* f;			   // primal populations (the step's input, or the state to observe)
-	R* lam;			   // adjoint populations, same layout as f
+	double* lam;	   // adjoint populations, FP64 whatever the storage, same layout (element strides) as f
 	long long sq;
 	int sy, sz, x0;
 	int X, Y, Z;
@@ -42,7 +42,7 @@ struct AdjArgs
 	const R* in_vx;		 // inlet profiles [Z][Y] (GEO_INFLOW) or null
 	const R* in_vy;
 	const R* in_vz;
-	const R* force;	  // per-site body force [3][Z][Y][X] or null (uniform p.fx..fz)
+	const double* force;  // per-site body force [3][Z][Y][X] or null (uniform p.fx..fz)
 	double* grad;	  // d objective / d force, [3][Z][Y][X], accumulated
 	CollParams<R> p;
 };
@@ -72,9 +72,9 @@ __device__ __forceinline__ CollParams<R> site_params(const AdjArgs<T, R>& a, lon
 {
 	CollParams<R> p = a.p;
 	if (a.force) {
-		p.fx = a.force[site];
-		p.fy = a.force[nsites + site];
-		p.fz = a.force[2 * nsites + site];
+		p.fx = (R) a.force[site];
+		p.fy = (R) a.force[nsites + site];
+		p.fz = (R) a.force[2 * nsites + site];
 		p.hfx = R(0.5) * p.fx;
 		p.hfy = R(0.5) * p.fy;
 		p.hfz = R(0.5) * p.fz;
@@ -95,91 +95,112 @@ __device__ __forceinline__ void add_dfeq_du(R lq, R rho, R vx, R vy, R vz, R& bx
 	bz += s * (g * R(cz(q)) - R(3) * vz);
 }
 
-// transpose of the SRT update with body force at one site: g = J^T l, and the
-// force gradient dF += (d out / d F)^T l
-template <typename R>
-__device__ __forceinline__ void srt_vjp(const Site<R>& s, const CollParams<R>& p, const R* l, R* g, double* dF)
+// primal moments and collision constants of one site, in FP64: the
+// transpose is evaluated in FP64 at the primal's values (the FP32 primal's
+// moments and constants converted exactly), so that the adjoint carries no
+// FP32 rounding whatever the storage
+struct AdjSite
 {
-	const R rho = s.rho, ir = s.rho == R(0) ? R(1) : s.ir;
-	const R vx = s.vx, vy = s.vy, vz = s.vz;
-	const R usq = vx * vx + vy * vy + vz * vz;
-	const R it = p.inv_tau, k = p.srt_force;
-	R A = 0, bx = 0, by = 0, bz = 0, hx = 0, hy = 0, hz = 0;
+	double rho, ir, vx, vy, vz;
+	double fx, fy, fz;		  // the site's body force
+	double inv_tau, srt_force;  // 1/tau, 1 - 1/(2 tau)
+};
+
+template <typename R>
+__device__ __forceinline__ AdjSite adj_site(const Site<R>& s, const CollParams<R>& p)
+{
+	AdjSite m;
+	m.rho = (double) s.rho;
+	m.ir = s.rho == R(0) ? 1.0 : (double) s.ir;
+	m.vx = (double) s.vx;
+	m.vy = (double) s.vy;
+	m.vz = (double) s.vz;
+	m.fx = (double) p.fx;
+	m.fy = (double) p.fy;
+	m.fz = (double) p.fz;
+	m.inv_tau = (double) p.inv_tau;
+	m.srt_force = (double) p.srt_force;
+	return m;
+}
+
+// transpose of the SRT update with body force at one site, in place: l <-
+// J^T l, and the force gradient dF += (d out / d F)^T l
+__device__ __forceinline__ void srt_vjp(const AdjSite& m, double* l, double* dF)
+{
+	const double rho = m.rho, ir = m.ir;
+	const double vx = m.vx, vy = m.vy, vz = m.vz;
+	const double usq = vx * vx + vy * vy + vz * vz;
+	const double it = m.inv_tau, k = m.srt_force;
+	double A = 0, bx = 0, by = 0, bz = 0, hx = 0, hy = 0, hz = 0;
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			const R feq = eq_second<q>(rho, vx, vy, vz, usq);
-			const R S = R(3) * ((R(cx(q)) - vx) * p.fx + (R(cy(q)) - vy) * p.fy + (R(cz(q)) - vz) * p.fz) * ir;
-			const R lq = l[q];
+			const double feq = eq_second<q>(rho, vx, vy, vz, usq);
+			const double S = 3.0 * ((cx(q) - vx) * m.fx + (cy(q) - vy) * m.fy + (cz(q) - vz) * m.fz) * ir;
+			const double lq = l[q];
 			A += lq * feq;
 			// d feq / d u weighted by (it + k S)
 			add_dfeq_du<q>(lq * (it + k * S), rho, vx, vy, vz, bx, by, bz);
 			// k feq dS/du = -3 k feq F / rho ; k feq dS/dF_a = 3 k feq (c_a - u_a) / rho
-			const R lf = lq * feq;
-			hx += lf * (R(cx(q)) - vx);
-			hy += lf * (R(cy(q)) - vy);
-			hz += lf * (R(cz(q)) - vz);
+			const double lf = lq * feq;
+			hx += lf * (cx(q) - vx);
+			hy += lf * (cy(q) - vy);
+			hz += lf * (cz(q) - vz);
 		}
 	);
 	// sum_q l_q feq_q, used by the density derivative and the dS/du term
-	const R sum_lf = A;
+	const double sum_lf = A;
 	A = it * sum_lf * ir;
-	bx -= R(3) * k * sum_lf * p.fx * ir;
-	by -= R(3) * k * sum_lf * p.fy * ir;
-	bz -= R(3) * k * sum_lf * p.fz * ir;
-	const R omit = R(1) - it;
+	bx -= 3.0 * k * sum_lf * m.fx * ir;
+	by -= 3.0 * k * sum_lf * m.fy * ir;
+	bz -= 3.0 * k * sum_lf * m.fz * ir;
+	const double omit = 1.0 - it;
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int j = decltype(Qc)::value;
-			g[j] = omit * l[j] + A + (bx * (R(cx(j)) - vx) + by * (R(cy(j)) - vy) + bz * (R(cz(j)) - vz)) * ir;
+			l[j] = omit * l[j] + A + (bx * (cx(j) - vx) + by * (cy(j) - vy) + bz * (cz(j) - vz)) * ir;
 		}
 	);
 	// d out / d F: through u (du/dF = 1 / (2 rho)) and through S directly
-	const R half_ir = R(0.5) * ir, three_k_ir = R(3) * k * ir;
-	dF[0] += (double) (bx * half_ir + three_k_ir * hx);
-	dF[1] += (double) (by * half_ir + three_k_ir * hy);
-	dF[2] += (double) (bz * half_ir + three_k_ir * hz);
+	const double half_ir = 0.5 * ir, three_k_ir = 3.0 * k * ir;
+	dF[0] += bx * half_ir + three_k_ir * hx;
+	dF[1] += by * half_ir + three_k_ir * hy;
+	dF[2] += bz * half_ir + three_k_ir * hz;
 }
 
-// transpose of out = feq(1, u(f)) (GEO_OUTFLOW_EQ)
-template <typename R>
-__device__ __forceinline__ void outflow_eq_vjp(const Site<R>& s, const R* l, R* g, double* dF)
+// transpose of out = feq(1, u(f)) (GEO_OUTFLOW_EQ), in place
+__device__ __forceinline__ void outflow_eq_vjp(const AdjSite& m, double* l, double* dF)
 {
-	const R ir = s.ir, vx = s.vx, vy = s.vy, vz = s.vz;
-	R bx = 0, by = 0, bz = 0;
+	const double ir = m.ir, vx = m.vx, vy = m.vy, vz = m.vz;
+	double bx = 0, by = 0, bz = 0;
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			add_dfeq_du<q>(l[q], R(1), vx, vy, vz, bx, by, bz);
+			add_dfeq_du<q>(l[q], 1.0, vx, vy, vz, bx, by, bz);
 		}
 	);
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int j = decltype(Qc)::value;
-			g[j] = (bx * (R(cx(j)) - vx) + by * (R(cy(j)) - vy) + bz * (R(cz(j)) - vz)) * ir;
+			l[j] = (bx * (cx(j) - vx) + by * (cy(j) - vy) + bz * (cz(j) - vz)) * ir;
 		}
 	);
-	const R half_ir = R(0.5) * ir;
-	dF[0] += (double) (bx * half_ir);
-	dF[1] += (double) (by * half_ir);
-	dF[2] += (double) (bz * half_ir);
+	const double half_ir = 0.5 * ir;
+	dF[0] += bx * half_ir;
+	dF[1] += by * half_ir;
+	dF[2] += bz * half_ir;
 }
 
-// transpose of the mirror copy of a symmetry plane (see symmetry(), aa_kernels.cuh)
-template <typename R>
-__device__ __forceinline__ void symmetry_vjp(const R* l, R* g, int axis, int side)
+// transpose of the mirror copy of a symmetry plane (see symmetry(),
+// aa_kernels.cuh), in place: the directions whose component along the normal
+// equals `side` hand their adjoint to their mirror image (which is never one
+// of them) and become zero
+__device__ __forceinline__ void symmetry_vjp(double* l, int axis, int side)
 {
-	static_for<27>(
-		[&](auto Qc)
-		{
-			constexpr int q = decltype(Qc)::value;
-			g[q] = l[q];
-		}
-	);
 	static_for<27>(
 		[&](auto Qc)
 		{
@@ -187,22 +208,22 @@ __device__ __forceinline__ void symmetry_vjp(const R* l, R* g, int axis, int sid
 			if constexpr (cx(q) != 0) {
 				constexpr int m = dir(-cx(q), cy(q), cz(q));
 				if (axis == 0 && cx(q) == side) {
-					g[m] += l[q];
-					g[q] = R(0);
+					l[m] += l[q];
+					l[q] = 0.0;
 				}
 			}
 			if constexpr (cy(q) != 0) {
 				constexpr int m = dir(cx(q), -cy(q), cz(q));
 				if (axis == 1 && cy(q) == side) {
-					g[m] += l[q];
-					g[q] = R(0);
+					l[m] += l[q];
+					l[q] = 0.0;
 				}
 			}
 			if constexpr (cz(q) != 0) {
 				constexpr int m = dir(cx(q), cy(q), -cz(q));
 				if (axis == 2 && cz(q) == side) {
-					g[m] += l[q];
-					g[q] = R(0);
+					l[m] += l[q];
+					l[q] = 0.0;
 				}
 			}
 		}
@@ -242,7 +263,10 @@ __global__ void __launch_bounds__(128) adj_primal_kernel(const AdjArgs<typename 
 
 // Adjoint of one A-A step: lam (adjoint of the step's output) is replaced in
 // place by the adjoint of its input, with f the step's primal input; grad
-// accumulates the force gradient of this step.
+// accumulates the force gradient of this step.  The adjoint values of a site
+// are gathered from its write locations, transformed in place in FP64 and
+// scattered to its read locations; the addresses are formed again for the
+// scatter instead of being kept in registers across the transform.
 template <typename S, bool ODD>
 __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S::T, typename S::R> a)
 {
@@ -256,25 +280,29 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 	const uint8_t geo = a.map ? a.map[site] : (uint8_t) GEO_PERIODIC;
 	if (geo == GEO_NOTHING)
 		return;
-	const CollParams<R> p = site_params(a, site, nsites);
 	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-	const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-	R l[27], g[27];
-	static_for<27>(
-		[&](auto Qc)
-		{
-			constexpr int q = decltype(Qc)::value;
-			l[q] = a.lam[aa_write_loc<ODD, q>(a.sq, base, o)];
-		}
-	);
+	double l[27];
+	{
+		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		static_for<27>(
+			[&](auto Qc)
+			{
+				constexpr int q = decltype(Qc)::value;
+				l[q] = a.lam[aa_write_loc<ODD, q>(a.sq, base, o)];
+			}
+		);
+	}
 	double dF[3] = {0, 0, 0};
 	switch (geo) {
 		case GEO_WALL:
-			static_for<27>(
+			// full-way bounce-back swaps opposite directions: its transpose too
+			static_for<13>(
 				[&](auto Qc)
 				{
-					constexpr int q = decltype(Qc)::value;
-					g[q] = l[opp(q)];
+					constexpr int q = 2 * decltype(Qc)::value + 1;
+					const double t = l[q];
+					l[q] = l[opp(q)];
+					l[opp(q)] = t;
 				}
 			);
 			break;
@@ -283,7 +311,7 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 				[&](auto Qc)
 				{
 					constexpr int q = decltype(Qc)::value;
-					g[q] = R(0);
+					l[q] = 0.0;
 				}
 			);
 			break;
@@ -295,26 +323,35 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 		case GEO_SYM_FRONT: {
 			const int axis = geo <= GEO_SYM_BOTTOM ? 2 : (geo <= GEO_SYM_RIGHT ? 0 : 1);
 			const int side = (geo == GEO_SYM_TOP || geo == GEO_SYM_RIGHT || geo == GEO_SYM_FRONT) ? -1 : 1;
-			symmetry_vjp(l, g, axis, side);
+			symmetry_vjp(l, axis, side);
 			break;
 		}
 		default: {	// FLUID, PERIODIC, OUTFLOW_EQ: need the primal moments
-			Site<R> s;
-			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
-			density_velocity(s, p);
+			const CollParams<R> p = site_params(a, site, nsites);
+			AdjSite m;
+			{
+				const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+				Site<R> s;
+				aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+				density_velocity(s, p);
+				m = adj_site(s, p);
+			}
 			if (geo == GEO_OUTFLOW_EQ)
-				outflow_eq_vjp(s, l, g, dF);
+				outflow_eq_vjp(m, l, dF);
 			else
-				srt_vjp(s, p, l, g, dF);
+				srt_vjp(m, l, dF);
 		}
 	}
-	static_for<27>(
-		[&](auto Qc)
-		{
-			constexpr int q = decltype(Qc)::value;
-			a.lam[aa_read_loc<ODD, q>(a.sq, base, o)] = g[q];
-		}
-	);
+	{
+		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		static_for<27>(
+			[&](auto Qc)
+			{
+				constexpr int q = decltype(Qc)::value;
+				a.lam[aa_read_loc<ODD, q>(a.sq, base, o)] = l[q];
+			}
+		);
+	}
 	if (a.grad && a.force && (dF[0] != 0.0 || dF[1] != 0.0 || dF[2] != 0.0)) {
 		a.grad[site] += dF[0];
 		a.grad[nsites + site] += dF[1];
@@ -356,13 +393,13 @@ __global__ void adj_objective_kernel(const AdjArgs<typename S::T, typename S::R>
 	loss[i] = 0.5 * (w_rho * drho * drho + dvx * dvx + dvy * dvy + dvz * dvz);
 	if (!a.lam)
 		return;
-	const R ir = s.ir;
-	const R ex = (R) (seed * dvx), ey = (R) (seed * dvy), ez = (R) (seed * dvz), er = (R) (seed * w_rho * drho);
+	const double ir = (double) s.ir, vx = (double) s.vx, vy = (double) s.vy, vz = (double) s.vz;
+	const double ex = seed * dvx, ey = seed * dvy, ez = seed * dvz, er = seed * w_rho * drho;
 	static_for<27>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
-			const R d = er + (ex * (R(cx(q)) - s.vx) + ey * (R(cy(q)) - s.vy) + ez * (R(cz(q)) - s.vz)) * ir;
+			const double d = er + (ex * (cx(q) - vx) + ey * (cy(q) - vy) + ez * (cz(q) - vz)) * ir;
 			a.lam[aa_read_loc<ODD, q>(a.sq, base, o)] += d;
 		}
 	);

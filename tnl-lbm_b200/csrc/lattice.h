@@ -61,6 +61,7 @@ struct lbm_lattice
 	int kernel = lbm::KERNEL_DIRECT;
 	int sms = 148;
 	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
+	long long wait_limit = -1;	// tile kernel's loop waits (lbm_set_wait_limit); negative: the default
 	long long last_blocks = 0;	// partial-sum slots of the last step launch
 	lbm::CollParamsD p{};
 	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration

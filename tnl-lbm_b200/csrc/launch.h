@@ -73,6 +73,7 @@ struct StepLaunch
 	int kernel;		   // KERNEL_DIRECT, KERNEL_TILE, KERNEL_SPLIT or KERNEL_PAIR
 	dim3 grid, block;  // direct kernel launch shape
 	int* status;	   // device status word (STATUS_* bits)
+	long long wait_limit;  // tries per mbarrier wait in the tile kernel's loop; negative: the default
 	cudaStream_t stream;
 	long long* blocks_out;	// partial-sum slots the launch writes (blocks or warps)
 	bool dry_run;			// only resolve launch facts (attributes, grid), launch nothing

@@ -181,6 +181,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.stream = h->stream;
 	L.kernel = h->kernel;
 	L.status = h->status_dev;
+	L.wait_limit = h->wait_limit;
 	long long blocks = 0;
 	L.blocks_out = &blocks;
 	L.dry_run = dry_run;
@@ -1136,7 +1137,17 @@ int lbm_status(lbm_handle h, int* status)
 	if (!status)
 		return fail(LBM_ERR_INVALID, "null output");
 	LBM_CUDA(cudaMemcpyAsync(status, h->status_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+	LBM_CUDA(cudaMemsetAsync(h->status_dev, 0, sizeof(int), h->stream));
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	return LBM_OK;
+}
+
+int lbm_set_wait_limit(lbm_handle h, int64_t tries)
+{
+	if (int rc = check(h))
+		return rc;
+	h->wait_limit = tries < 0 ? -1 : tries;
+	h->drop_graph();
 	return LBM_OK;
 }
 

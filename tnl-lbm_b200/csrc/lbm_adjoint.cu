@@ -34,11 +34,11 @@ namespace lbm {
 
 struct AdjointState
 {
-	void* force = nullptr;	// R [3][Z][Y][X]
+	double* force = nullptr;	 // [3][Z][Y][X]
 	std::vector<void*> ckpt;
 	void* final_state = nullptr;
 	std::vector<void*> seg;
-	void* lam = nullptr;
+	double* lam = nullptr;	 // FP64, the element strides of the population array
 	double* grad = nullptr;	 // [3][Z][Y][X]
 	long long* samples = nullptr;
 	double* target = nullptr;
@@ -99,7 +99,7 @@ lbm::AdjArgs<typename S::T, typename S::R> make_args(lbm_handle h, void* f, void
 	using R = typename S::R;
 	lbm::AdjArgs<typename S::T, R> a{};
 	a.f = (typename S::T*) f;
-	a.lam = (R*) lam;
+	a.lam = (double*) lam;
 	a.sq = h->g.sq;
 	a.sy = h->g.sy;
 	a.sz = h->g.sz;
@@ -111,7 +111,7 @@ lbm::AdjArgs<typename S::T, typename S::R> make_args(lbm_handle h, void* f, void
 	a.in_vx = (const R*) h->inflow[0];
 	a.in_vy = (const R*) h->inflow[1];
 	a.in_vz = (const R*) h->inflow[2];
-	a.force = (const R*) h->adjoint->force;
+	a.force = h->adjoint->force;
 	a.grad = grad;
 	a.p = lbm::make_coll_params<R>(h->p);
 	return a;
@@ -182,14 +182,20 @@ int forward_typed(lbm_handle h)
 	return LBM_OK;
 }
 
+// bytes of the FP64 adjoint array (the population array's element count)
+size_t lam_bytes(lbm_handle h)
+{
+	return h->pop_bytes / (size_t) h->ops->elem_size * sizeof(double);
+}
+
 template <typename S>
 int backward_typed(lbm_handle h, double seed)
 {
 	auto* st = h->adjoint;
-	const size_t pb = h->pop_bytes;
-	ADJ_CUDA(cudaMemsetAsync(st->lam, 0, pb, h->stream));
+	ADJ_CUDA(cudaMemsetAsync(st->lam, 0, lam_bytes(h), h->stream));
 	ADJ_CUDA(cudaMemsetAsync(st->grad, 0, sizeof(double) * 3 * h->sites(), h->stream));
 	ADJ_CUDA(objective<S>(h, true, seed));
+	const size_t pb = h->pop_bytes;
 	const long long nseg = st->nckpt;
 	for (long long s = nseg - 1; s >= 0; s--) {
 		const long long n0 = s * st->every;
@@ -268,18 +274,18 @@ int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64
 		h->adjoint = nullptr;
 		return rc;
 	};
-	// the control: per-site force in the compute type (the uniform force of the
-	// descriptor when force is NULL)
-	std::vector<unsigned char> fh((size_t) 3 * nsites * cs);
-	for (long long k = 0; k < 3; k++)
-		for (long long i = 0; i < nsites; i++) {
-			const double v = force ? force[k * nsites + i] : (k == 0 ? h->d.fx : (k == 1 ? h->d.fy : h->d.fz));
-			if (cs == 8)
-				((double*) fh.data())[k * nsites + i] = v;
-			else
-				((float*) fh.data())[k * nsites + i] = (float) v;
-		}
-	if ((!st->force && cudaMalloc(&st->force, fh.size()) != cudaSuccess)
+	// the control: per-site force in FP64, from host or device memory (the
+	// uniform force of the descriptor when force is NULL); each step rounds it
+	// to the compute type
+	const size_t force_bytes = sizeof(double) * 3 * (size_t) nsites;
+	std::vector<double> fh;
+	if (!force) {
+		fh.resize((size_t) 3 * nsites);
+		for (long long k = 0; k < 3; k++)
+			for (long long i = 0; i < nsites; i++)
+				fh[(size_t) (k * nsites + i)] = k == 0 ? h->d.fx : (k == 1 ? h->d.fy : h->d.fz);
+	}
+	if ((!st->force && cudaMalloc(&st->force, force_bytes) != cudaSuccess)
 		|| (!st->final_state && cudaMalloc(&st->final_state, h->pop_bytes) != cudaSuccess))
 		return fail_free(afail(LBM_ERR_CUDA, "adjoint buffers: allocation failed"));
 	if (nsamples > st->nsamples_cap) {
@@ -302,7 +308,7 @@ int lbm_adjoint_forward(lbm_handle h, const double* force, int64_t nsteps, int64
 		st->ckpt.push_back(p);
 	}
 	st->nckpt = nckpt;
-	if (cudaMemcpyAsync(st->force, fh.data(), fh.size(), cudaMemcpyHostToDevice, h->stream) != cudaSuccess
+	if (cudaMemcpyAsync(st->force, force ? force : fh.data(), force_bytes, cudaMemcpyDefault, h->stream) != cudaSuccess
 		|| cudaMemcpyAsync(st->samples, samples, sizeof(long long) * nsamples, cudaMemcpyHostToDevice, h->stream) != cudaSuccess
 		|| cudaMemcpyAsync(st->target, target, sizeof(double) * 4 * nsamples, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
 		return fail_free(afail(LBM_ERR_CUDA, "adjoint inputs: copy failed"));
@@ -329,7 +335,7 @@ int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, void* gr
 	if (grad_populations && ((layout != 0 && layout != 1) || (dtype != 0 && dtype != 1)))
 		return afail(LBM_ERR_INVALID, "bad layout or dtype");
 	const size_t pb = h->pop_bytes;
-	if (!st->lam && (cudaMalloc(&st->lam, pb) != cudaSuccess || cudaMalloc(&st->grad, sizeof(double) * 3 * h->sites()) != cudaSuccess))
+	if (!st->lam && (cudaMalloc(&st->lam, lam_bytes(h)) != cudaSuccess || cudaMalloc(&st->grad, sizeof(double) * 3 * h->sites()) != cudaSuccess))
 		return afail(LBM_ERR_CUDA, "adjoint state allocation failed");
 	while ((long long) st->seg.size() < st->every) {
 		void* p = nullptr;
@@ -341,11 +347,11 @@ int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, void* gr
 	if (rc)
 		return rc;
 	if (grad_force)
-		ADJ_CUDA(cudaMemcpyAsync(grad_force, st->grad, sizeof(double) * 3 * h->sites(), cudaMemcpyDeviceToHost, h->stream));
+		ADJ_CUDA(cudaMemcpyAsync(grad_force, st->grad, sizeof(double) * 3 * h->sites(), cudaMemcpyDefault, h->stream));
 	if (grad_populations) {
 		// the adjoint of the initial population array, in the dense layout of
-		// lbm_get_populations (the storage is the compute type, so the
-		// storage's pack kernel converts it unchanged)
+		// lbm_get_populations (an FP64 array with the population array's
+		// element strides, converted by the FP64 storage's pack kernel)
 		const int gh = layout == LBM_LAYOUT_GHOST ? 2 : 0;
 		const size_t count = (size_t) 27 * (h->d.X + gh) * (h->d.Y + gh) * (h->d.Z + gh);
 		const size_t bytes = count * (dtype == 0 ? 8 : 4);
@@ -353,12 +359,12 @@ int lbm_adjoint_backward(lbm_handle h, double seed, double* grad_force, void* gr
 		ADJ_CUDA(cudaMallocAsync(&dev, bytes, h->stream));
 		lbm::Geometry g = h->g;
 		g.f = st->lam;
-		const cudaError_t e = h->ops->pack(g, dev, dtype, layout, h->stream);
+		const cudaError_t e = lbm::storage_ops(lbm::ST_F64).pack(g, dev, dtype, layout, h->stream);
 		if (e != cudaSuccess) {
 			cudaFreeAsync(dev, h->stream);
 			return afail(LBM_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
 		}
-		ADJ_CUDA(cudaMemcpyAsync(grad_populations, dev, bytes, cudaMemcpyDeviceToHost, h->stream));
+		ADJ_CUDA(cudaMemcpyAsync(grad_populations, dev, bytes, cudaMemcpyDefault, h->stream));
 		cudaFreeAsync(dev, h->stream);
 	}
 	ADJ_CUDA(cudaStreamSynchronize(h->stream));

@@ -274,6 +274,111 @@ __device__ __forceinline__ void pair_write(typename S::T* __restrict__ f, long l
 	);
 }
 
+// Addresses of the two-site kernels without 64-bit multiplies: the byte
+// offsets q sq sizeof(T) of the 27 slot rows of a lattice row come from the
+// kernel parameters (constant-bank operands), the rows of the pair's three z
+// planes from three pointers, and the y neighbours from three offsets, so an
+// access is one pointer plus two offsets.  (Formed as f + q * sq + ..., every
+// access took 64-bit integer multiply-adds, which run on the FMA pipe that
+// the 16-bit formats' collision already fills.)
+struct PairSlots
+{
+	int b[27];
+};
+
+inline PairSlots make_pair_slots(long long sq, int elem)
+{
+	PairSlots ps;
+	for (int q = 0; q < 27; q++)
+		ps.b[q] = (int) (q * sq * elem);
+	return ps;
+}
+
+struct PairAt
+{
+	char* P[3];		   // row (y, x of the first site) in planes z - 1, z, z + 1
+	long long oy[3];   // byte offsets of rows y - 1, y, y + 1 from row y
+	int left, right;   // x offsets (elements) of the pair's outer neighbours, as PairX
+};
+
+// neighbours of the pair (x, x + 1) of row (y, z): periodic sites wrap in x
+// and y (wrap) and in z (wrap && zwrap), all others reach the ghost layer
+template <typename T>
+__device__ __forceinline__ PairAt pair_at(const StepArgs<T, float>& a, int x, int y, int z, bool wrap)
+{
+	PairAt at;
+	constexpr long long E = (long long) sizeof(T);
+	const int zm = (wrap && a.zwrap && z == 0) ? a.Z - 1 : z - 1;
+	const int zp = (wrap && a.zwrap && z == a.Z - 1) ? 0 : z + 1;
+	const long long ry = (long long) (y + 1) * a.sy + a.x0 + x;
+	char* f = reinterpret_cast<char*>(a.f);
+	at.P[0] = f + ((long long) (zm + 1) * a.sz + ry) * E;
+	at.P[1] = f + ((long long) (z + 1) * a.sz + ry) * E;
+	at.P[2] = f + ((long long) (zp + 1) * a.sz + ry) * E;
+	at.oy[0] = (long long) ((wrap && y == 0) ? a.Y - 1 : -1) * a.sy * E;
+	at.oy[1] = 0;
+	at.oy[2] = (long long) ((wrap && y == a.Y - 1) ? -(a.Y - 1) : 1) * a.sy * E;
+	at.left = (wrap && x == 0) ? a.X - 1 : -1;
+	at.right = (wrap && x + 1 == a.X - 1) ? -(a.X - 1) : 1;
+	return at;
+}
+
+// pair_read with the addresses of PairAt / PairSlots
+template <typename S, bool ODD>
+__device__ __forceinline__ void pair_read_at(const PairAt& at, const PairSlots& ps, Site<F2>& s)
+{
+	using T = typename S::T;
+	using IO = PairIO<S>;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (!ODD)
+				s.f[q] = IO::template load2<q>(reinterpret_cast<const T*>(at.P[1] + ps.b[q]));
+			else {
+				// direction q of site x comes from slot opp(q) of site x - c_q
+				const T* c = reinterpret_cast<const T*>(at.P[1 - cz(q)] + at.oy[1 - cy(q)] + ps.b[opp(q)]);
+				if constexpr (cx(q) == 0)
+					s.f[q] = IO::template load2<opp(q)>(c);
+				else if constexpr (cx(q) > 0)
+					s.f[q] = F2(S::template load<opp(q)>(c + at.left), S::template load<opp(q)>(c));
+				else
+					s.f[q] = F2(S::template load<opp(q)>(c + 1), S::template load<opp(q)>(c + 1 + at.right));
+			}
+		}
+	);
+}
+
+// pair_write with the addresses of PairAt / PairSlots
+template <typename S, bool ODD>
+__device__ __forceinline__ void pair_write_at(const PairAt& at, const PairSlots& ps, const Site<F2>& s)
+{
+	using T = typename S::T;
+	using IO = PairIO<S>;
+	static_for<27>(
+		[&](auto Qc)
+		{
+			constexpr int q = decltype(Qc)::value;
+			if constexpr (!ODD)
+				IO::template store2<opp(q)>(reinterpret_cast<T*>(at.P[1] + ps.b[opp(q)]), s.f[q]);
+			else {
+				// direction q of site x goes to slot q of site x + c_q
+				T* c = reinterpret_cast<T*>(at.P[1 + cz(q)] + at.oy[1 + cy(q)] + ps.b[q]);
+				if constexpr (cx(q) == 0)
+					IO::template store2<q>(c, s.f[q]);
+				else if constexpr (cx(q) > 0) {
+					S::template store<q>(c + 1, s.f[q].v.x);
+					S::template store<q>(c + 1 + at.right, s.f[q].v.y);
+				}
+				else {
+					S::template store<q>(c + at.left, s.f[q].v.x);
+					S::template store<q>(c, s.f[q].v.y);
+				}
+			}
+		}
+	);
+}
+
 // outputs of an observation step for both sites (step_outputs of the scalar
 // kernel); in = site inside the lattice; the warp's partial sums go to slot
 // `slot` of nslots
@@ -328,42 +433,35 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 // warp calls it (threads past the lattice with x >= X).
 template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT>
 __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
-											const uint8_t* __restrict__ groups, int x, int y, int z, long long slot,
-											long long nslots)
+											const PairSlots& ps, const uint8_t* __restrict__ groups, int x, int y, int z,
+											long long slot, long long nslots)
 {
 	bool act = x < a.X && y < a.Y;
-	long long site = 0, base = 0;
+	long long site = 0;
 	Site<F2> s;
-	Offsets o;
-	PairX px{-1, 1};
+	PairAt at;
 	if (act) {
 		site = ((long long) z * a.Y + y) * a.X + x;
-		base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
 		if constexpr (GENERAL) {
 			// a pair away from every lattice face has the same neighbours
 			// whether it wraps or not: its loads are issued together with the
 			// group flag's (and are discarded if the group is not a pair group)
 			const bool inner = x > 0 && x + 2 < a.X && y > 0 && y < a.Y - 1 && z > 0 && z < a.Z - 1;
 			if (inner) {
-				o = neighbour_offsets(false, false, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-				pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+				at = pair_at(a, x, y, z, false);
+				pair_read_at<S, ODD>(at, ps, s);
 			}
 			const int gx = (a.X + PAIR_GROUP - 1) / PAIR_GROUP;
 			const uint8_t g = groups[((long long) z * a.Y + y) * gx + x / PAIR_GROUP];
 			act = g != PAIR_GROUP_REST;
 			if (act && !inner) {
-				const bool wrap = g == PAIR_GROUP_PERIODIC;
-				o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-				px.left = (wrap && x == 0) ? a.X - 1 : -1;
-				px.right = (wrap && x + 1 == a.X - 1) ? -(a.X - 1) : 1;
-				pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+				at = pair_at(a, x, y, z, g == PAIR_GROUP_PERIODIC);
+				pair_read_at<S, ODD>(at, ps, s);
 			}
 		}
 		else {
-			o = neighbour_offsets(true, a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-			px.left = x == 0 ? a.X - 1 : -1;
-			px.right = x + 1 == a.X - 1 ? -(a.X - 1) : 1;
-			pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
+			at = pair_at(a, x, y, z, true);
+			pair_read_at<S, ODD>(at, ps, s);
 		}
 		if (act)
 			density_velocity(s, p2);
@@ -375,7 +473,7 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 	if (!act)
 		return;
 	collide_cumulant<F2, CUMF>(s, p2);
-	pair_write<S, ODD>(a.f, a.sq, base, o, px, s);
+	pair_write_at<S, ODD>(at, ps, s);
 }
 
 // The per-site update of aa_step_kernel for entry i of a host-built site list
@@ -445,12 +543,12 @@ __device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>
 // (t, y) of the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).
 template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
-															 long long red_slots)
+															 const PairSlots ps, long long red_slots)
 {
 	const int wpb = (blockDim.x * blockDim.y) >> 5;
 	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
 	const long long slot = block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5);
-	pair_update<S, CUMF, ODD, false, OUT>(a, p2, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
+	pair_update<S, CUMF, ODD, false, OUT>(a, p2, ps, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
 										  blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, slot, red_slots);
 }
 
@@ -463,9 +561,9 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 // their DRAM sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
 template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
-	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const uint8_t* __restrict__ groups,
-						const unsigned* __restrict__ work, const unsigned long long* __restrict__ rest, long long nrest,
-						int tiles_x)
+	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const PairSlots ps,
+						const uint8_t* __restrict__ groups, const unsigned* __restrict__ work,
+						const unsigned long long* __restrict__ rest, long long nrest, int tiles_x)
 {
 	const unsigned w = work[blockIdx.x];
 	const long long slot = (long long) blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -476,7 +574,7 @@ __global__ void __launch_bounds__(128, MINB)
 	else {
 		const unsigned row = w / (unsigned) tiles_x;
 		const int x = (int) (w - row * (unsigned) tiles_x) * 256 + 2 * (int) threadIdx.x;
-		pair_update<S, CUMF, ODD, true, OUT>(a, p2, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
+		pair_update<S, CUMF, ODD, true, OUT>(a, p2, ps, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
 											 slot, nslots);
 	}
 }
@@ -532,6 +630,10 @@ cudaError_t pair_step(const StepLaunch& L)
 	a.zwrap = L.distributed_z ? 0 : 1;
 	a.p = make_coll_params<float>(L.p);
 	const CollParams<F2> p2 = make_coll_params<F2>(L.p);
+	// every slot offset of a lattice row fits 32 bits (sq < 2^26 elements)
+	if (27ll * L.g.sq * (long long) sizeof(T) >= (1ll << 31))
+		return cudaErrorNotSupported;
+	const PairSlots ps = make_pair_slots(L.g.sq, (int) sizeof(T));
 	const dim3 block = general ? dim3(128, 1, 1) : L.block;
 	const int pairs = (L.g.X + 1) / 2;
 	const dim3 grid = general ? dim3((unsigned) W.nwork, 1, 1)
@@ -548,15 +650,15 @@ cudaError_t pair_step(const StepLaunch& L)
 		if (general) {                                                                                                    \
 			if (out)                                                                                                      \
 				aa_pair_work_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(        \
-					a, p2, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
+					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 			else                                                                                                          \
 				aa_pair_work_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(       \
-					a, p2, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
+					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 		}                                                                                                                 \
 		else if (out)                                                                                                     \
-			aa_pair_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, red_slots);  \
+			aa_pair_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);  \
 		else                                                                                                              \
-			aa_pair_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, red_slots); \
+			aa_pair_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots); \
 	} while (0)
 #define LBM_PAIR_PARITY(CUMF)           \
 	do {                                \

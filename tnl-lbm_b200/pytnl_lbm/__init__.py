@@ -266,6 +266,11 @@ class LBM:
         _abi.check(self.lib.lbm_status(self.h, ctypes.byref(v)))
         return v.value
 
+    def set_wait_limit(self, tries=-1):
+        """Bound of the tile kernel's per-tile waits in tries (negative: the
+        default); see lbm_set_wait_limit."""
+        _abi.check(self.lib.lbm_set_wait_limit(self.h, int(tries)))
+
     def autotune(self, ntrials=4):
         _abi.check(self.lib.lbm_autotune(self.h, int(ntrials)))
         return self.block()
@@ -306,27 +311,44 @@ class LBM:
         ``force`` [3, Z, Y, X] (None: the uniform force of the lattice) and
         return J = sum_i 1/2 [rho_weight (rho_i - rho*_i)^2 + |u_i - u*_i|^2]
         at the sample sites (flat indices (z*Y + y)*X + x) against
-        ``target`` [n, 4] = (rho*, u*x, u*y, u*z)."""
+        ``target`` [n, 4] = (rho*, u*x, u*y, u*z).  ``force`` may be a numpy
+        array or a float64 torch tensor; a CUDA tensor is read in place on the
+        device (no host round trip)."""
         samples = np.ascontiguousarray(samples, dtype=np.int64)
         target = np.ascontiguousarray(target, dtype=np.float64).reshape(len(samples), 4)
         fp = None
+        keep = None
         if force is not None:
-            force = np.ascontiguousarray(force, dtype=np.float64)
-            if force.shape != (3,) + self.shape:
+            if tuple(force.shape) != (3,) + self.shape:
                 raise ValueError(f"force must have shape {(3,) + self.shape}")
-            fp = _abi.dptr(force)
+            if _is_cuda_tensor(force):
+                keep = force.detach().to(dtype=_torch().float64).contiguous()
+                fp = ctypes.cast(ctypes.c_void_p(keep.data_ptr()), ctypes.POINTER(ctypes.c_double))
+            else:
+                keep = np.ascontiguousarray(force, dtype=np.float64)
+                fp = _abi.dptr(keep)
         loss = ctypes.c_double(0.0)
         _abi.check(self.lib.lbm_adjoint_forward(
             self.h, fp, int(nsteps), int(checkpoint_every), samples.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
             len(samples), _abi.dptr(target), float(rho_weight), ctypes.byref(loss)))
         return loss.value
 
-    def adjoint_backward(self, seed=1.0, populations=False, layout=LAYOUT_GHOST):
+    def adjoint_backward(self, seed=1.0, populations=False, layout=LAYOUT_GHOST, out=None):
         """seed * dJ/dF [3, Z, Y, X] and, with ``populations``, seed * dJ/d(initial
-        populations) in the layout of get_populations."""
-        g = np.empty((3,) + self.shape, np.float64)
+        populations) in the layout of get_populations.  ``out``: a contiguous
+        float64 CUDA tensor [3, Z, Y, X] that receives dJ/dF on the device
+        (returned in place of a numpy array)."""
+        if out is not None:
+            if not (_is_cuda_tensor(out) and out.dtype == _torch().float64 and out.is_contiguous()
+                    and tuple(out.shape) == (3,) + self.shape):
+                raise ValueError(f"out must be a contiguous float64 CUDA tensor of shape {(3,) + self.shape}")
+            g = out
+            gptr = ctypes.cast(ctypes.c_void_p(out.data_ptr()), ctypes.POINTER(ctypes.c_double))
+        else:
+            g = np.empty((3,) + self.shape, np.float64)
+            gptr = _abi.dptr(g)
         gp = np.empty(self._pop_shape(layout), np.float64) if populations else None
-        _abi.check(self.lib.lbm_adjoint_backward(self.h, float(seed), _abi.dptr(g),
+        _abi.check(self.lib.lbm_adjoint_backward(self.h, float(seed), gptr,
                                                  gp.ctypes.data if gp is not None else None, layout, 0))
         return (g, gp) if populations else g
 
@@ -342,6 +364,15 @@ class LBM:
               2: torch.float16 if self.storage in (STORE_F16S, STORE_F16SR) else torch.bfloat16}[v.elem_size]
         flat = _wrap_device(v.populations, v.sz * (self.Z + 2), dt, self.desc.device)
         return flat.as_strided((27, self.Z + 2, self.Y + 2, v.sq), (v.sq, v.sz, v.sy, 1))
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_cuda_tensor(a):
+    return hasattr(a, "is_cuda") and hasattr(a, "data_ptr") and bool(a.is_cuda)
 
 
 def _wrap_device(ptr, n, dtype, device):

@@ -110,6 +110,7 @@ SIGNATURES = {
     "lbm_halo_pack": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "lbm_halo_unpack": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "lbm_halo_copy": (ctypes.c_int, [_H, ctypes.c_int, _H, ctypes.c_int, ctypes.c_int]),
+    "lbm_set_wait_limit": (ctypes.c_int, [_H, ctypes.c_int64]),
     "lbm_ade_enable": (ctypes.c_int, [_H, ctypes.POINTER(lbm_ade_desc)]),
     "lbm_ade_disable": (ctypes.c_int, [_H]),
     "lbm_ade_set_map": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_uint8)]),

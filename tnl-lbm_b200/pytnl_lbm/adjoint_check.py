@@ -10,8 +10,9 @@ against a target flow generated with a different seeded control.
 
 Reports the time of the forward pass (with sqrt(N) checkpoints) and of the
 backward pass, the device memory of the checkpoints, the agreement of the FP64
-gradient with central finite differences on random cells, and of the FP32
-gradient with the FP64 one.
+gradient and of the FP32 one (FP32 primal, FP64 adjoint) with central finite
+differences of the FP64 objective on random cells, and of the two gradients
+with each other.
 
     python -m pytnl_lbm.adjoint_check --steps 4000 --fd-cells 32
 """
@@ -126,14 +127,13 @@ def check(steps=4000, fd_cells=32, h=1e-6, seed=7):
     fluid = np.flatnonzero((m == GEO["FLUID"]).ravel())
     cells = rng.choice(fluid, size=fd_cells, replace=False)
     scale = np.max(np.abs(g[0]))
-    errs = []
+    fds = []
     for c in cells:
         idx = np.unravel_index(int(c), m.shape)
         Fp, Fm = F.copy(), F.copy()
         Fp[(0,) + idx] += h
         Fm[(0,) + idx] -= h
-        fd = (run(lat, Fp, steps, samples, target, steps) - run(lat, Fm, steps, samples, target, steps)) / (2 * h)
-        errs.append(abs(fd - g[(0,) + idx]) / max(abs(fd), 1e-3 * scale))
+        fds.append((run(lat, Fp, steps, samples, target, steps) - run(lat, Fm, steps, samples, target, steps)) / (2 * h))
     sy = (16 + X + 4 + 15) // 16 * 16  # row pitch of the FP64 layout
     pop_bytes = 27 * sy * (Y + 2) * (Z + 2) * 8
     lat.close()
@@ -143,12 +143,18 @@ def check(steps=4000, fd_cells=32, h=1e-6, seed=7):
     g32 = lat32.adjoint_backward()
     t4 = time.perf_counter()
     lat32.close()
+
+    def rel_errs(grad):
+        return [abs(fd - grad[(0,) + np.unravel_index(int(c), m.shape)]) / max(abs(fd), 1e-3 * scale)
+                for c, fd in zip(cells, fds)]
+    errs, errs32 = rel_errs(g), rel_errs(g32)
     return {
         "case": f"channel {X}x{Y}x{Z}, SRT, inlet u_max {U_MAX}, nu {NU}, {steps} steps, {len(samples)} samples on 8 planes",
         "objective": J, "checkpoint_every": every,
         "f64_forward_s": t1 - t0, "f64_backward_s": t2 - t1, "f32_forward_backward_s": t4 - t3,
         "checkpoint_memory_gb_f64": (math.ceil(steps / every) + every + 2) * pop_bytes / 1e9,
         "fd_cells": fd_cells, "fd_step": h, "fd_max_rel_err": float(np.max(errs)), "fd_median_rel_err": float(np.median(errs)),
+        "fd_f32_max_rel_err": float(np.max(errs32)),
         "f32_vs_f64_grad_rel_linf": float(np.max(np.abs(g32[0] - g[0])) / scale),
     }
 

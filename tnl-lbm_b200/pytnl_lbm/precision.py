@@ -27,8 +27,8 @@ import time
 
 import numpy as np
 
-from . import COLL_CUM, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, LBM, STORE_BF16S, STORE_BF16SR, STORE_F16S, \
-    STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64
+from . import COLL_CUM, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, KERNEL_DIRECT, KERNEL_PAIR, LBM, STORE_BF16S, \
+    STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64
 
 STORAGES = {"f64": STORE_F64, "f32": STORE_F32, "f32s": STORE_F32S, "f16s": STORE_F16S, "bf16s": STORE_BF16S,
             "f16sr": STORE_F16SR, "bf16sr": STORE_BF16SR}
@@ -41,15 +41,20 @@ def viscosity(n: int) -> float:
     return U0 * (n / (2 * math.pi)) / RE
 
 
-def tgv_series(n: int, steps: int, every: int, storage: str, device: int = 0) -> dict:
+def tgv_series(n: int, steps: int, every: int, storage: str, device: int = 0, kernel: int | None = None) -> dict:
     """E(t) and eps(t) every `every` steps (an even number: the A-A state is
-    read after even steps, as the reference's probes are)."""
+    read after even steps, as the reference's probes are).  kernel: the step
+    kernel (LBM_KERNEL_*); by default the two-site kernel for the formats
+    with FP32 arithmetic, the one the throughput runs use."""
     if every % 2:
         raise ValueError("every must be even")
     nu = viscosity(n)
     lat = LBM(n, n, n, viscosity=nu, collision=COLL_CUM, cum_flags=CUM_GEIER_2017 | CUM_ANTIALIAS,
               equilibrium=EQ_INV_CUM, storage=STORAGES[storage], periodic=True, device=device)
     try:
+        if kernel is None:
+            kernel = KERNEL_DIRECT if storage == "f64" else KERNEL_PAIR
+        lat.set_kernel(kernel)
         lat.init_taylor_green(U0, 1.0)
         vol = float(n) ** 3
         t, ke, eps = [], [], []
