@@ -608,14 +608,14 @@ def run_adjoint(args):
             "grad_max_abs": float(np.max(np.abs(g[0]))),
             "roofline": {"bound": "hbm", "achieved": None, "peak": read_peaks()[0], "unit": "GB/s", "frac": None,
                          "traffic": None,
-                         "note": "per step: two primal A-A steps (216 B/site each) and one adjoint step "
-                                 "(27 primal reads + 27 adjoint reads + 27 adjoint writes, 324 B/site), "
-                                 "plus a 27-value copy per recomputed state"},
+                         "note": "per step: two primal A-A steps (216 B/site each), one adjoint step "
+                                 "(27 FP32 primal reads + 27 FP64 adjoint reads + 27 FP64 adjoint writes, 540 B/site) "
+                                 "and a 27-value FP32 copy per recomputed state (216 B/site)"},
             "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                     "per_run": "lbm_adjoint_forward + lbm_adjoint_backward through the C-ABI"},
             "clocks": clk.summary(),
         }
-        bytes_per_site_step = 2 * 216 + 324 + 2 * 108
+        bytes_per_site_step = 2 * 216 + 540 + 216
         line["roofline"]["achieved"] = round(bytes_per_site_step * sites * steps / secs / 1e9, 1)
         line["roofline"]["frac"] = round(line["roofline"]["achieved"] / line["roofline"]["peak"], 4)
     if dist is not None:
@@ -780,9 +780,13 @@ def run_ours(args):
         print(json.dumps(line))
 
 
-def cpu_baseline(spec, args):
+def time_reference_cpu(spec, storage, sample_steps, warmup, min_seconds=10.0):
     """The reference's own per-site code (oracle/_ref, OpenMP on all host
-    cores) on a bounded sample of the workload."""
+    cores; the restatement in oracle/ if the reference was not built) on the
+    workload: warm-up steps, then samples of `sample_steps` full-lattice A-A
+    steps (at most ~60 s each) until at least `min_seconds` have been timed.
+    Both the reference arm and the cpu_baseline leg of our arm use it, so
+    that they measure the same thing."""
     sys.path.insert(0, ROOT)
     import oracle
     cores = os.cpu_count() or 1
@@ -795,38 +799,46 @@ def cpu_baseline(spec, args):
     else:
         m = np.full((Z, Y, X), 9, np.uint8)
         nu = 0.05 * (X / (2 * math.pi)) / 1600.0
-        inflow = None
-        fields = None
-    prec = np.float64 if args.storage == "f64" else np.float32
-    if use_ref:
-        impl = oracle.Reference(flags, fast=True)
-        kind = "reference"
-    else:
-        impl = oracle.Port()
-        kind = "port"
+        inflow, fields = None, None
+    prec = np.float64 if storage == "f64" else np.float32
+    impl = oracle.Reference(flags, fast=True) if use_ref else oracle.Port()
     f = impl.allocate(X, Y, Z, prec)
     impl.init_equilibrium(f, X, Y, Z, eq="INV_CUM", fields=fields)
     m16 = m.astype(np.int16)
 
     def run(n, start):
-        t0 = time.perf_counter()
         if use_ref:
             _, el = impl.aa_run(f, m16, coll="CUM", eq="INV_CUM", nu=nu, inflow=inflow, start_iter=start, nsteps=n,
                                 nthreads=cores, return_time=True)
             return el
+        t0 = time.perf_counter()
         impl.aa_run(f, m16, coll="CUM", eq="INV_CUM", cum_flags=flags, nu=nu, inflow=inflow, start_iter=start,
                     nsteps=n, nthreads=cores)
         return time.perf_counter() - t0
 
-    # calibrate on two steps, then time about 10 s of stepping
-    per_step = run(2, 0) / 2
-    steps = int(min(400, max(2, 10.0 / max(per_step, 1e-6))))
+    warm = max(1, min(warmup, 2))
+    per_step = run(warm, 0) / warm
+    steps = int(max(2, min(sample_steps, 60.0 / max(per_step, 1e-6))))
     steps += steps % 2
-    el = run(steps, 2)
-    return {"value": round(X * Y * Z * steps / el / 1e6, 3), "unit": "MLUPS", "cores": cores, "kind": kind,
-            "sample": f"{steps} A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), {el:.1f} s, OpenMP on "
-                      f"{cores} threads, loop order of state.hpp:1388-1397",
-            "cpu": cpu_description()}
+    it, el, reps = warm, 0.0, 0
+    while reps == 0 or el < min_seconds:
+        el += run(steps, it)
+        it += steps
+        reps += 1
+    value = X * Y * Z * steps * reps / el / 1e6
+    cpu = cpu_description()
+    sample = (f"{reps} samples of {steps} A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), {el:.1f} s in "
+              f"all, OpenMP on {cores} threads, loop order of state.hpp:1388-1397, {cpu['isa']} build")
+    return {"value": value, "steps": steps, "reps": reps, "seconds": el, "cores": cores,
+            "kind": "reference" if use_ref else "port", "sample": sample, "cpu": cpu, "prec": prec}
+
+
+def cpu_baseline(spec, args):
+    """The cpu_baseline object of our arm's line (time_reference_cpu with the
+    reference arm's sampling)."""
+    r = time_reference_cpu(spec, args.storage, min(args.steps, 20), args.warmup)
+    return {"value": round(r["value"], 3), "unit": "MLUPS", "cores": r["cores"], "kind": r["kind"],
+            "sample": r["sample"], "cpu": r["cpu"]}
 
 
 def run_reference(args):
@@ -852,45 +864,19 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no time-dependent adjoint of this "
                           "workload (sim_adjoint solves a steady adjoint about a frozen flow)"}))
         return
-    X, Y, Z = spec["X"], spec["Y"], spec["Z"]
-    if spec["kind"] == "duct":
-        m, prof, nu, fields = duct_setup(X, Y, Z)
-        inflow = (prof, None, None)
-    else:
-        m = np.full((Z, Y, X), 9, np.uint8)
-        nu = 0.05 * (X / (2 * math.pi)) / 1600.0
-        inflow, fields = None, None
-    prec = np.float64 if args.storage == "f64" else np.float32
-    impl = oracle.Reference(flags, fast=True)
-    f = impl.allocate(X, Y, Z, prec)
-    impl.init_equilibrium(f, X, Y, Z, eq="INV_CUM", fields=fields)
-    m16 = m.astype(np.int16)
-    warm = max(1, min(args.warmup, 2))
-    _, el_w = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, nsteps=warm, nthreads=cores, return_time=True)
-    per_step = el_w / warm
-    steps = int(max(2, min(args.steps, 60.0 / max(per_step, 1e-6))))
-    steps += steps % 2
-    it, el, reps = warm, 0.0, 0
-    while reps == 0 or el < 10.0:
-        _, e = impl.aa_run(f, m16, coll="CUM", nu=nu, inflow=inflow, start_iter=it, nsteps=steps, nthreads=cores,
-                           return_time=True)
-        el += e
-        it += steps
-        reps += 1
-    value = X * Y * Z * steps * reps / el / 1e6
-    sample = (f"{reps} samples of {steps} timed A-A steps of the full {X}x{Y}x{Z} workload ({prec.__name__}), "
-              f"{el:.1f} s in all, OpenMP on {cores} threads, loop order of state.hpp:1388-1397")
-    cpu = cpu_description()
+    r = time_reference_cpu(spec, args.storage, args.steps, args.warmup)
+    value = r["value"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "MLUPS", "n_gpus": world,
-        "steps": steps, "warmup": args.warmup, "ms_per_step": round(el / (steps * reps) * 1e3, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == np.float64 else "f32",
+        "steps": r["steps"], "warmup": args.warmup, "ms_per_step": round(r["seconds"] / (r["steps"] * r["reps"]) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if r["prec"] == np.float64 else "f32",
         "data": "synthetic (seeded initial state of the named configuration)",
         "config": workload_config(spec, args.storage, world),
-        "implementation": "TNL-LBM per-site headers (oracle/_ref, %s build) + the reference's OpenMP loop" % cpu["isa"],
-        "repetitions": reps,
-        "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": cores, "kind": "reference",
-                         "sample": sample, "cpu": cpu},
+        "implementation": "TNL-LBM per-site headers (oracle/_ref, %s build) + the reference's OpenMP loop" % r["cpu"]["isa"],
+        "repetitions": r["reps"],
+        "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"], "cpu": r["cpu"]},
         "e2e": {"value": round(value, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

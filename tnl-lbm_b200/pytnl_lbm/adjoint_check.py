@@ -148,13 +148,14 @@ def check(steps=4000, fd_cells=32, h=1e-6, seed=7):
         return [abs(fd - grad[(0,) + np.unravel_index(int(c), m.shape)]) / max(abs(fd), 1e-3 * scale)
                 for c, fd in zip(cells, fds)]
     errs, errs32 = rel_errs(g), rel_errs(g32)
+    normwise32 = [abs(fd - g32[(0,) + np.unravel_index(int(c), m.shape)]) / scale for c, fd in zip(cells, fds)]
     return {
         "case": f"channel {X}x{Y}x{Z}, SRT, inlet u_max {U_MAX}, nu {NU}, {steps} steps, {len(samples)} samples on 8 planes",
         "objective": J, "checkpoint_every": every,
         "f64_forward_s": t1 - t0, "f64_backward_s": t2 - t1, "f32_forward_backward_s": t4 - t3,
         "checkpoint_memory_gb_f64": (math.ceil(steps / every) + every + 2) * pop_bytes / 1e9,
         "fd_cells": fd_cells, "fd_step": h, "fd_max_rel_err": float(np.max(errs)), "fd_median_rel_err": float(np.median(errs)),
-        "fd_f32_max_rel_err": float(np.max(errs32)),
+        "fd_f32_max_rel_err": float(np.max(errs32)), "fd_f32_max_normwise_err": float(np.max(normwise32)),
         "f32_vs_f64_grad_rel_linf": float(np.max(np.abs(g32[0] - g[0])) / scale),
     }
 
