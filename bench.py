@@ -87,25 +87,22 @@ def ensemble_setup(count=64, seed=4321, u0=0.05, edges=(32, 48, 64, 96, 128)):
     return sizes, nus
 
 
-def run_ensemble(args):
-    """One persistent launch per step over all members, against the same
-    members run one after the other as single lattices."""
+def measure_ensemble(pl, local, spec, storage, steps, warmup, dist=None, world=1):
+    """The ensemble workload: every launch shape timed over 256 steps, the
+    autotuner's choice timed over `steps` steps, an e2e leg with the
+    per-member sums read every step, and the same members run one after the
+    other as single lattices on the two-site kernel (the single-lattice
+    step's best kernel for these widths)."""
     import torch
-    import pytnl_lbm as pl
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = init_dist(world, local, "nccl")
     device = torch.device("cuda", local)
-    spec = workload_spec(args.workload)
     sizes, nus = ensemble_setup(spec["count"], edges=spec["edges"])
     sites = sum(x * y * z for x, y, z in sizes)
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
-          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[args.storage]
+          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
     ens = pl.Ensemble(sizes, nus, cum_flags=3, storage=st, device=local)
     ens.init_taylor_green(0.05)
-    # every launch shape, timed over 256 steps, then the autotuner's choice
     shapes = {}
-    cands = ((128, 0), (256, 0), (128, 1), (128, 2)) + (((256, 3),) if args.storage != "f64" else ())
+    cands = ((128, 0), (256, 0), (128, 1), (128, 2)) + (((256, 3),) if storage != "f64" else ())
     for tile, gp in cands:
         ens.set_shape(tile, gp)
         ens.step(16)
@@ -118,7 +115,7 @@ def run_ensemble(args):
     shape = ens.autotune(3)
     ens.init_taylor_green(0.05)
     stream = torch.cuda.ExternalStream(ens.stream, device=device)
-    warm = max(args.warmup, 16) + (max(args.warmup, 16) % 2)
+    warm = max(warmup, 16) + (max(warmup, 16) % 2)
     ens.step(warm)
     ens.synchronize()
     if dist is not None:
@@ -127,30 +124,26 @@ def run_ensemble(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ens.step(args.steps)
+        ens.step(steps)
         e1.record(stream)
         e1.synchronize()
     secs = e0.elapsed_time(e1) / 1e3
     secs_max = max_over_ranks(dist, secs, device)
-    value = sites * args.steps * world / secs_max / 1e6
+    value = sites * steps * world / secs_max / 1e6
     ens.step(2, sums=True)
     ke_ens = ens.kinetic_energy()
-    # e2e through the public API: one step with the per-member sums and the
-    # sums read back to the host, every step
-    e2e_steps = max(10, min(args.steps // 4, 200))
+    e2e_steps = max(10, min(steps // 4, 200))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         ens.step(1, sums=True)
         ens.sums()
     e2e_secs = max_over_ranks(dist, time.perf_counter() - t0, device)
     ens.close()
-
-    # the same members as single lattices, one after the other (device time of
-    # each run on its own stream, summed)
     seq_secs = 0.0
     ke_seq = []
     for (X, Y, Z), nu in zip(sizes, nus):
         lat = pl.LBM(X, Y, Z, viscosity=nu, cum_flags=3, storage=st, periodic=True, device=local)
+        lat.set_kernel(pl.KERNEL_PAIR)
         lat.init_taylor_green(0.05)
         lat.step(warm)
         lat.synchronize()
@@ -158,50 +151,66 @@ def run_ensemble(args):
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record(ls)
-        lat.step(args.steps)
+        lat.step(steps)
         a1.record(ls)
         a1.synchronize()
         seq_secs += a0.elapsed_time(a1) / 1e3
         lat.step(2, sums=True)
         ke_seq.append(pl.kinetic_energy(lat))
         lat.close()
-    seq_value = sites * args.steps / seq_secs / 1e6
+    seq_value = sites * steps / seq_secs / 1e6
     ke_diff = float(np.max(np.abs(np.asarray(ke_seq) - ke_ens) / np.abs(np.asarray(ke_seq))))
+    return {"sizes": sizes, "sites": sites, "value": value, "secs": secs, "secs_max": secs_max, "shapes": shapes,
+            "shape": shape, "e2e_value": sites * e2e_steps * world / e2e_secs / 1e6, "e2e_steps": e2e_steps,
+            "seq_value": seq_value, "ke_diff": ke_diff, "clocks": clk.summary()}
 
+
+GRID_POLICIES = ["persistent", "one block per tile", "per-member launches in concurrent graph branches",
+                 "persistent, two sites per thread (packed FP32)"]
+
+
+def run_ensemble(args):
+    """The ensemble workload's line: the autotuned batched step against the
+    same members run one after the other as single lattices."""
+    import torch
+    import pytnl_lbm as pl
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, local, "nccl")
+    spec = workload_spec(args.workload)
+    r = measure_ensemble(pl, local, spec, args.storage, args.steps, args.warmup, dist, world)
+    sizes, sites, shape = r["sizes"], r["sites"], r["shape"]
     bpe = BYTES_PER_ELEM[args.storage]
-    achieved = 2 * 27 * bpe * sites / (secs / args.steps) / 1e9
+    achieved = 2 * 27 * bpe * sites / (r["secs"] / args.steps) / 1e9
     peak, peak_kind = read_peaks()
     line = None
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(secs_max / args.steps * 1e3, 5), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": DTYPE_LABEL[args.storage],
+            "metric": METRIC, "value": round(r["value"], 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(r["secs_max"] / args.steps * 1e3, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE_LABEL[args.storage],
             "data": "synthetic (seeded member sizes, viscosities and Taylor-Green initial states)",
             "config": {"workload": spec["workload"], "members": len(sizes), "sites": sites,
                        "storage": args.storage, "parallelism": f"replicas x{world}",
-                       "launch": {"tile_sites": shape[0],
-                                  "grid": ["persistent", "one block per tile",
-                                           "per-member launches in concurrent graph branches",
-                                           "persistent, two sites per thread (packed FP32)"][shape[1]],
-                                  "autotuned": True},
                        "l2": "populations (%.2f GB) larger than L2; no flush" % (27 * bpe * sites / 1e9)},
+            "launch": {"tile_sites": shape[0], "grid": GRID_POLICIES[shape[1]], "autotuned": True},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_site_update": 2 * 27 * bpe},
-            "e2e": {"value": round(sites * e2e_steps * world / e2e_secs / 1e6, 2), "unit": "MLUPS",
-                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 6 * 8 * len(sizes), "steps": e2e_steps,
+            "e2e": {"value": round(r["e2e_value"], 2), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 6 * 8 * len(sizes), "steps": r["e2e_steps"],
                     "per_step": "lbm_ensemble_step(1, LBM_STEP_SUMS) + lbm_ensemble_get_sums"},
-            "shapes_mlups": shapes,
-            "sequential": {"value": round(seq_value, 2), "unit": "MLUPS", "speedup": round(value / seq_value, 3),
-                           "kinetic_energy_max_rel_diff": ke_diff,
-                           "how": f"the same {len(sizes)} members as single periodic lattices (lbm_create), one after the "
-                                  "other, each replayed from its CUDA graphs; summed device time"},
-            "clocks": clk.summary(),
+            "shapes_mlups": r["shapes"],
+            "sequential": {"value": round(r["seq_value"], 2), "unit": "MLUPS",
+                           "speedup": round(r["value"] / r["seq_value"], 3),
+                           "kinetic_energy_max_rel_diff": r["ke_diff"],
+                           "how": f"the same {len(sizes)} members as single periodic lattices (lbm_create) on the "
+                                  "two-site kernel, one after the other, each replayed from its CUDA graphs; summed "
+                                  "device time"},
+            "clocks": r["clocks"],
         }
     if dist is not None:
         dist.barrier()
@@ -457,14 +466,16 @@ def max_over_ranks(dist, value, device):
     return float(t.item())
 
 
-def make_lattice(pl, spec, storage, device, kernel="direct"):
+def make_lattice(pl, spec, storage, device, kernel="direct", collision="cum"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
-        lat = pl.LBM(X, Y, Z, viscosity=nu, collision=pl.COLL_CUM, cum_flags=spec["cum_flags"],
-                     equilibrium=pl.EQ_INV_CUM, storage=st, device=device)
+        coll = {"cum": pl.COLL_CUM, "srt": pl.COLL_SRT, "bgk": pl.COLL_BGK, "mrt": pl.COLL_MRT}[collision]
+        lat = pl.LBM(X, Y, Z, viscosity=nu, collision=coll, cum_flags=spec["cum_flags"],
+                     equilibrium=pl.EQ_INV_CUM if collision == "cum" else pl.EQ_SECOND_ORDER, storage=st,
+                     device=device)
         lat.set_kernel({"tile": pl.KERNEL_TILE, "split": pl.KERNEL_SPLIT, "pair": pl.KERNEL_PAIR}.get(kernel, pl.KERNEL_DIRECT))
         lat.set_map(m)
         lat.set_inflow(prof, None, None)
@@ -717,6 +728,18 @@ def run_ours(args):
             vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
             variants[f"f32_{other}_kernel"] = {"mlups": sites * args.steps / vsecs / 1e6}
             vl.close()
+        # the other collisions of the COLL slot (one-site kernel, autotuned block)
+        if spec["kind"] == "duct":
+            for coll in ("srt", "bgk", "mrt"):
+                vl, _ = make_lattice(pl, spec, "f32", local, "direct", coll)
+                if args.autotune:
+                    vl.autotune(16)
+                vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
+                vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
+                gbs = 216 * sites / (vsecs / args.steps) / 1e9
+                variants[f"f32_{coll}"] = {"mlups": sites * args.steps / vsecs / 1e6, "achieved_gbs": gbs,
+                                           "frac": gbs / peak}
+                vl.close()
     else:
         lat.close()
 
@@ -731,10 +754,18 @@ def run_ours(args):
         precision.pop("series")
     # the duct configuration's FP32-against-FP64 comparison and the 512^3
     # Taylor-Green throughput
-    duct_cmp = tgv512 = None
+    duct_cmp = tgv512 = ens_block = None
     if args.configs and rank == 0 and spec["kind"] == "duct" and not spec.get("ade"):
         duct_cmp = duct_fp32_vs_fp64(pl, local)
         tgv512 = tgv512_throughput(pl, local, max(args.steps, 20), args.warmup)
+        # the batching configuration: 64 Taylor-Green lattices, autotuned
+        r = measure_ensemble(pl, local, workload_spec("ensemble64"), "f32", 200, args.warmup)
+        ens_block = {"workload": workload_spec("ensemble64")["workload"], "steps": 200,
+                     "mlups": round(r["value"], 1), "launch": GRID_POLICIES[r["shape"][1]],
+                     "tile_sites": r["shape"][0], "shapes_mlups": r["shapes"],
+                     "sequential_mlups": round(r["seq_value"], 1),
+                     "speedup_vs_sequential": round(r["value"] / r["seq_value"], 3),
+                     "kinetic_energy_max_rel_diff": r["ke_diff"]}
 
     line = None
     if rank == 0:
@@ -771,6 +802,8 @@ def run_ours(args):
             line["duct_fp32_vs_fp64"] = duct_cmp
         if tgv512 is not None:
             line["tgv512"] = tgv512
+        if ens_block is not None:
+            line["ensemble64"] = ens_block
         if args.cpu_baseline and world == 1 and not spec.get("ade"):
             line["cpu_baseline"] = cpu_baseline(spec, args)
     if dist is not None:

@@ -141,7 +141,10 @@ __global__ void __launch_bounds__(TPB, MINB)
 
 // One A-A step of every member, two x-adjacent sites per thread (grid policy
 // 3): tiles of 256 sites, 128 threads, the per-pair code of aa_pair_kernel
-// with the member's constants.  Every member's X is even, so a tile's pairs
+// with the member's constants.  The grid walks the tile list with a stride
+// of the grid size, so the blocks resident at one time work on neighbouring
+// tiles and share the rows they touch through L2 (contiguous ranges per
+// block ran 7 % slower on 64 members).  Every member's X is even, so a tile's pairs
 // never straddle two rows.  OUT: per-tile FP64 partial sums as
 // ens_step_kernel's.
 template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
@@ -151,6 +154,9 @@ __global__ void __launch_bounds__(128, MINB)
 {
 	using T = typename S::T;
 	__shared__ EnsMember<T, float> M;
+	// byte offsets of the current member's 27 slot rows (pair_read_at reads
+	// them from shared memory instead of multiplying per access)
+	__shared__ PairSlots ps;
 	constexpr int WORDS = (int) (sizeof(EnsMember<T, float>) / 4);
 	static_assert(sizeof(EnsMember<T, float>) % 4 == 0 && WORDS <= 128, "member entry size");
 	int cur = -1;
@@ -160,25 +166,22 @@ __global__ void __launch_bounds__(128, MINB)
 			__syncthreads();
 			if ((int) threadIdx.x < WORDS)
 				reinterpret_cast<unsigned*>(&M)[threadIdx.x] = reinterpret_cast<const unsigned*>(members + m)[threadIdx.x];
+			if (threadIdx.x < 27)
+				ps.b[threadIdx.x] = (int) (threadIdx.x * members[m].sq * (long long) sizeof(T));
 			__syncthreads();
 			cur = m;
 		}
 		const unsigned i = (unsigned) ((t - M.tile0) * 256) + 2 * threadIdx.x;
 		const bool act = i < (unsigned) M.n;
 		Site<F2> s;
-		Offsets o;
-		PairX px{-1, 1};
-		long long base = 0;
+		PairAt at;
 		if (act) {
 			const unsigned row = fast_div(i, M.dx);
 			const int x = (int) (i - row * (unsigned) M.X);
 			const unsigned z = fast_div(row, M.dy);
 			const int y = (int) (row - z * (unsigned) M.Y);
-			base = (long long) (z + 1) * M.sz + (long long) (y + 1) * M.sy + M.x0 + x;
-			o = neighbour_offsets(true, x, y, (int) z, M.X, M.Y, M.Z, M.sy, M.sz);
-			px.left = x == 0 ? M.X - 1 : -1;
-			px.right = x + 1 == M.X - 1 ? -(M.X - 1) : 1;
-			pair_read<S, ODD>(M.f, M.sq, base, o, px, s);
+			at = pair_at_of(reinterpret_cast<char*>(M.f), sizeof(T), M.sy, M.sz, M.x0, M.X, M.Y, M.Z, x, y, (int) z, true, true);
+			pair_read_at<S, ODD>(at, ps, s);
 			density_velocity(s, M.p2);
 		}
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(128, MINB)
 				}
 			}
 			collide_cumulant<F2, CUMF>(s, M.p2);
-			pair_write<S, ODD>(M.f, M.sq, base, o, px, s);
+			pair_write_at<S, ODD>(at, ps, s);
 		}
 		if constexpr (OUT) {
 #pragma unroll

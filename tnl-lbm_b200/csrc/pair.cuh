@@ -301,26 +301,32 @@ struct PairAt
 	int left, right;   // x offsets (elements) of the pair's outer neighbours, as PairX
 };
 
-// neighbours of the pair (x, x + 1) of row (y, z): periodic sites wrap in x
-// and y (wrap) and in z (wrap && zwrap), all others reach the ghost layer
+// neighbours of the pair (x, x + 1) of row (y, z) of the population array f
+// (element size E bytes, strides in elements): periodic sites wrap in x and
+// y (wrap) and in z (wrap && zwrap), all others reach the ghost layer
+__device__ __forceinline__ PairAt pair_at_of(char* f, long long E, int sy, int sz, int x0, int X, int Y, int Z, int x, int y,
+											 int z, bool wrap, bool zwrap)
+{
+	PairAt at;
+	const int zm = (wrap && zwrap && z == 0) ? Z - 1 : z - 1;
+	const int zp = (wrap && zwrap && z == Z - 1) ? 0 : z + 1;
+	const long long ry = (long long) (y + 1) * sy + x0 + x;
+	at.P[0] = f + ((long long) (zm + 1) * sz + ry) * E;
+	at.P[1] = f + ((long long) (z + 1) * sz + ry) * E;
+	at.P[2] = f + ((long long) (zp + 1) * sz + ry) * E;
+	at.oy[0] = (long long) ((wrap && y == 0) ? Y - 1 : -1) * sy * E;
+	at.oy[1] = 0;
+	at.oy[2] = (long long) ((wrap && y == Y - 1) ? -(Y - 1) : 1) * sy * E;
+	at.left = (wrap && x == 0) ? X - 1 : -1;
+	at.right = (wrap && x + 1 == X - 1) ? -(X - 1) : 1;
+	return at;
+}
+
 template <typename T>
 __device__ __forceinline__ PairAt pair_at(const StepArgs<T, float>& a, int x, int y, int z, bool wrap)
 {
-	PairAt at;
-	constexpr long long E = (long long) sizeof(T);
-	const int zm = (wrap && a.zwrap && z == 0) ? a.Z - 1 : z - 1;
-	const int zp = (wrap && a.zwrap && z == a.Z - 1) ? 0 : z + 1;
-	const long long ry = (long long) (y + 1) * a.sy + a.x0 + x;
-	char* f = reinterpret_cast<char*>(a.f);
-	at.P[0] = f + ((long long) (zm + 1) * a.sz + ry) * E;
-	at.P[1] = f + ((long long) (z + 1) * a.sz + ry) * E;
-	at.P[2] = f + ((long long) (zp + 1) * a.sz + ry) * E;
-	at.oy[0] = (long long) ((wrap && y == 0) ? a.Y - 1 : -1) * a.sy * E;
-	at.oy[1] = 0;
-	at.oy[2] = (long long) ((wrap && y == a.Y - 1) ? -(a.Y - 1) : 1) * a.sy * E;
-	at.left = (wrap && x == 0) ? a.X - 1 : -1;
-	at.right = (wrap && x + 1 == a.X - 1) ? -(a.X - 1) : 1;
-	return at;
+	return pair_at_of(reinterpret_cast<char*>(a.f), (long long) sizeof(T), a.sy, a.sz, a.x0, a.X, a.Y, a.Z, x, y, z, wrap,
+					  a.zwrap != 0);
 }
 
 // pair_read with the addresses of PairAt / PairSlots
