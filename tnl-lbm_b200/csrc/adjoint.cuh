@@ -30,6 +30,11 @@
 
 namespace lbm {
 
+// resident blocks per SM of the adjoint step (register cap 65536 / (128 n))
+#ifndef ADJ_STEP_MINB
+#define ADJ_STEP_MINB 4
+#endif
+
 template <typename T, typename R>
 struct AdjArgs
 {
@@ -93,6 +98,13 @@ __device__ __forceinline__ void add_dfeq_du(R lq, R rho, R vx, R vy, R vz, R& bx
 	bx += s * (g * R(cx(q)) - R(3) * vx);
 	by += s * (g * R(cy(q)) - R(3) * vy);
 	bz += s * (g * R(cz(q)) - R(3) * vz);
+}
+
+// 8-byte asynchronous copy global -> shared (cp.async, cached in L1)
+__device__ __forceinline__ void copy8_async(double* dst, const double* src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned) __cvta_generic_to_shared(dst)), "l"(src)
+				 : "memory");
 }
 
 // primal moments and collision constants of one site, in FP64: the
@@ -266,9 +278,10 @@ __global__ void __launch_bounds__(128) adj_primal_kernel(const AdjArgs<typename 
 // accumulates the force gradient of this step.  The adjoint values of a site
 // are gathered from its write locations, transformed in place in FP64 and
 // scattered to its read locations; the addresses are formed again for the
-// scatter instead of being kept in registers across the transform.
+// scatter instead of being kept in registers across the transform.  Blocks of
+// 128 threads (the shared array has one row per thread).
 template <typename S, bool ODD>
-__global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S::T, typename S::R> a)
+__global__ void __launch_bounds__(128, ADJ_STEP_MINB) adj_step_kernel(const AdjArgs<typename S::T, typename S::R> a)
 {
 	using R = typename S::R;
 	const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,16 +294,34 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 	if (geo == GEO_NOTHING)
 		return;
 	const long long base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-	double l[27];
+	// the site's 27 adjoint values live in shared memory (27 doubles per
+	// thread, an odd stride: no bank conflicts beyond the two wavefronts of a
+	// 64-bit access), not in registers: 54 registers fewer per thread and so
+	// more resident warps for this memory-bound step
+	__shared__ double lsh[128 * 27];
+	double* const l = lsh + threadIdx.x * 27;
+	// the primal populations of the sites whose transpose needs the moments
+	// are loaded before the adjoint values, so that both sets of loads are in
+	// flight together
+	const bool primal = geo != GEO_WALL && geo != GEO_INFLOW && !(geo >= GEO_SYM_TOP && geo <= GEO_SYM_FRONT);
+	Site<R> s;
 	{
 		const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
+		// the adjoint values go straight to shared memory (asynchronous copies,
+		// no registers), and the primal loads are in flight with them
 		static_for<27>(
 			[&](auto Qc)
 			{
 				constexpr int q = decltype(Qc)::value;
-				l[q] = a.lam[aa_write_loc<ODD, q>(a.sq, base, o)];
+				copy8_async(l + q, a.lam + aa_write_loc<ODD, q>(a.sq, base, o));
 			}
 		);
+		asm volatile("cp.async.commit_group;" ::: "memory");
+		if (primal)
+			aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
+		// each thread reads only its own row of lsh: the wait makes this
+		// thread's copies visible to it, no block barrier is needed
+		asm volatile("cp.async.wait_group 0;" ::: "memory");
 	}
 	double dF[3] = {0, 0, 0};
 	switch (geo) {
@@ -328,14 +359,8 @@ __global__ void __launch_bounds__(128) adj_step_kernel(const AdjArgs<typename S:
 		}
 		default: {	// FLUID, PERIODIC, OUTFLOW_EQ: need the primal moments
 			const CollParams<R> p = site_params(a, site, nsites);
-			AdjSite m;
-			{
-				const Offsets o = neighbour_offsets(geo == GEO_PERIODIC, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-				Site<R> s;
-				aa_read<S, ODD>(a.f, a.sq, base, o, s.f);
-				density_velocity(s, p);
-				m = adj_site(s, p);
-			}
+			density_velocity(s, p);
+			const AdjSite m = adj_site(s, p);
 			if (geo == GEO_OUTFLOW_EQ)
 				outflow_eq_vjp(m, l, dF);
 			else
