@@ -60,6 +60,9 @@ typedef struct lbm_lattice* lbm_handle;
 #define LBM_COLL_SRT 1 /* D3Q27_SRT, col_srt.h */
 #define LBM_COLL_BGK 2 /* D3Q27_BGK, col_bgk.h */
 #define LBM_COLL_MRT 3 /* D3Q27_MRT (MRT-LES), col_mrt.h */
+/* ids of user-compiled collisions (lbm_register_collision) */
+#define LBM_COLL_PLUGIN_FIRST 16
+#define LBM_COLL_PLUGIN_LAST 31
 
 /* cumulant variant bits (USE_GEIER_CUM_2017, USE_GEIER_CUM_ANTIALIAS; defs.h:312-315).
  * Valid sets: 0, ANTIALIAS, 2017|ANTIALIAS. */
@@ -455,6 +458,37 @@ LBM_API int64_t lbm_halo_bytes(lbm_handle h);
 LBM_API int lbm_halo_pack(lbm_handle h, int z, int cz, void* dev_buf);
 LBM_API int lbm_halo_unpack(lbm_handle h, int z, int cz, const void* dev_buf);
 LBM_API int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, int cz);
+
+/* ---- Collision plugins (the open COLL slot of LBM_CONFIG) ---------------
+ * The reference composes a user's collision struct into its step kernel at
+ * compile time: LBM_CONFIG<..., COLL, ...> (defs.h:288-310) calls
+ * COLL::collision(KS) on the D3Q27_KernelStruct of each site (defs.h:256-262,
+ * e.g. D3Q27_SRT::collision, d3q27/col_srt.h:7-15).  Here a user compiles a
+ * collision struct into a launcher with LBM_COLLISION_PLUGIN
+ * (tnl-lbm_b200/csrc/plugin.cuh): the launcher runs this library's fused A-A
+ * step (streaming, every boundary type of lbm_set_map, macro and sums
+ * outputs) with the user's collision inlined in it, and registers under an
+ * id in [LBM_COLL_PLUGIN_FIRST, LBM_COLL_PLUGIN_LAST] that lbm_desc.collision
+ * then names.
+ *
+ * A launcher is called with the library's launch record of one step (an
+ * opaque pointer) and the lattice's LBM_STORE_* storage, on the handle's
+ * device; it returns a cudaError_t value (0 = success).  Called with
+ * step == NULL it only answers whether it was built for `storage` (0, or
+ * cudaErrorNotSupported).  abi_version is LBM_PLUGIN_ABI_VERSION as the
+ * plugin saw it when compiled; the launch record's layout is that of the
+ * same header tree, so a plugin is compiled against the headers of the
+ * library it loads into.  Registration is process-wide; a handle keeps the
+ * launcher it was created with, so the plugin's code must stay loaded while
+ * such a handle lives.  launcher == NULL removes the id.  Plugin lattices run
+ * the one-site kernel with A-A streaming (lbm_set_kernel accepts only
+ * LBM_KERNEL_DIRECT, lbm_set_streaming only LBM_STREAMING_AA) and take no
+ * coupled scalar, adjoint or ensemble. */
+#define LBM_PLUGIN_ABI_VERSION 1
+typedef int32_t (*lbm_collision_launcher)(const void* step, int32_t storage);
+LBM_API int lbm_register_collision(int32_t id, lbm_collision_launcher launcher, int32_t abi_version, const char* name);
+/* Name under which `id` was registered (NULL when none). */
+LBM_API const char* lbm_collision_name(int32_t id);
 
 LBM_API const char* lbm_version(void);
 

@@ -157,7 +157,7 @@ def test_autograd_function_keeps_a_cuda_control_on_the_device(pl, port):
     assert ft.grad.is_cuda
     J_host = run(lat, f0, force, samples, target, 14, every=4, w_rho=0.5)
     g_host = lat.adjoint_backward()
-    assert float(J) == J_host
+    assert float(J.detach()) == J_host
     np.testing.assert_array_equal(ft.grad.cpu().numpy(), g_host)
     lat.close()
 

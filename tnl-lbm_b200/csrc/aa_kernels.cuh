@@ -372,8 +372,12 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double* pa
 // periodic (no map read).  GENERAL = true: per-site GEO type from the map with
 // the boundary conditions of D3Q27_BC_All (bc.h:60-422) that are free of
 // cross-site ordering in the A-A pattern.
-template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
-__global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
+// The per-site step of the direct kernel with the collision as a functor
+// collide(Site<R>&): the COLL slot of cudaLBMKernel (kernels.h:59-112), so
+// that the built-in collisions and a user's collision (plugin.cuh) run the
+// same streaming, boundary treatment and outputs.
+template <typename S, bool ODD, bool GENERAL, bool OUT, typename Collide>
+__device__ __forceinline__ void aa_step_site(const StepArgs<typename S::T, typename S::R>& a, Collide&& collide)
 {
 	using R = typename S::R;
 	const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -412,9 +416,16 @@ __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typen
 		step_outputs(a, active, site, s);
 	if (write) {
 		if (coll)
-			collide<R, COLL, CUMF>(s, a.p);
+			collide(s);
 		aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
 	}
+}
+
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int MINB>
+__global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
+{
+	using R = typename S::R;
+	aa_step_site<S, ODD, GENERAL, OUT>(a, [&](Site<R>& s) { collide<R, COLL, CUMF>(s, a.p); });
 }
 
 // Split step for lattices with a map: the host sorts the lattice's tiles of

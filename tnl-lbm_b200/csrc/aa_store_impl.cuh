@@ -247,24 +247,7 @@ struct StorageUnit
 
 	static StepArgs<T, R> step_args(const StepLaunch& L)
 	{
-		StepArgs<T, R> a;
-		a.f = (T*) L.g.f;
-		a.sq = L.g.sq;
-		a.sy = L.g.sy;
-		a.sz = L.g.sz;
-		a.x0 = L.g.x0;
-		a.X = L.g.X;
-		a.Y = L.g.Y;
-		a.Z = L.g.Z;
-		a.map = L.map;
-		a.in_vx = (const R*) L.inflow[0];
-		a.in_vy = (const R*) L.inflow[1];
-		a.in_vz = (const R*) L.inflow[2];
-		a.macro = (R*) L.macro;
-		a.partials = L.partials;
-		a.zwrap = L.distributed_z ? 0 : 1;
-		a.p = make_coll_params<R>(L.p);
-		return a;
+		return make_step_args<S>(L);
 	}
 
 	static cudaError_t step(const StepLaunch& L)

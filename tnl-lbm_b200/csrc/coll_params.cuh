@@ -2,6 +2,7 @@
 // from the double-precision values the host computes once (launch.h).
 #pragma once
 
+#include "aa_kernels.cuh"
 #include "collision.cuh"
 #include "launch.h"
 
@@ -39,6 +40,32 @@ inline CollParams<R> make_coll_params(const CollParamsD& d)
 	p.tau2 = (R) (d.tau * d.tau);
 	p.eq = d.eq;
 	return p;
+}
+
+// kernel arguments of one A-A step of storage S from the host's launch record
+template <typename S>
+inline StepArgs<typename S::T, typename S::R> make_step_args(const StepLaunch& L)
+{
+	using T = typename S::T;
+	using R = typename S::R;
+	StepArgs<T, R> a;
+	a.f = (T*) L.g.f;
+	a.sq = L.g.sq;
+	a.sy = L.g.sy;
+	a.sz = L.g.sz;
+	a.x0 = L.g.x0;
+	a.X = L.g.X;
+	a.Y = L.g.Y;
+	a.Z = L.g.Z;
+	a.map = L.map;
+	a.in_vx = (const R*) L.inflow[0];
+	a.in_vy = (const R*) L.inflow[1];
+	a.in_vz = (const R*) L.inflow[2];
+	a.macro = (R*) L.macro;
+	a.partials = L.partials;
+	a.zwrap = L.distributed_z ? 0 : 1;
+	a.p = make_coll_params<R>(L.p);
+	return a;
 }
 
 }  // namespace lbm

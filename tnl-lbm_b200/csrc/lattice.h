@@ -59,6 +59,7 @@ struct lbm_lattice
 	long long iteration = 0;
 	int bx = 0, by = 0;	 // 0: default
 	int kernel = lbm::KERNEL_DIRECT;
+	lbm_collision_launcher plugin = nullptr;  // a registered collision (desc.collision >= LBM_COLL_PLUGIN_FIRST)
 	int sms = 148;
 	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
 	long long wait_limit = -1;	// tile kernel's loop waits (lbm_set_wait_limit); negative: the default

@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -119,6 +120,20 @@ bool site_type_supported(uint8_t g)
 	}
 }
 
+// collision plugins registered by lbm_register_collision, by id - LBM_COLL_PLUGIN_FIRST
+struct CollisionPlugin
+{
+	lbm_collision_launcher launch = nullptr;
+	std::string name;
+};
+std::mutex g_plugins_mutex;
+CollisionPlugin g_plugins[LBM_COLL_PLUGIN_LAST - LBM_COLL_PLUGIN_FIRST + 1];
+
+bool plugin_id(int id)
+{
+	return id >= LBM_COLL_PLUGIN_FIRST && id <= LBM_COLL_PLUGIN_LAST;
+}
+
 }  // namespace
 
 namespace lbm {
@@ -200,6 +215,17 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 		L.ade = &h->ade->launch;
 		if (!dry_run)
 			h->ade->phi_valid = macro;
+	}
+	if (h->plugin) {  // a registered collision: its own direct kernel
+		const int32_t rc = h->plugin(&L, h->d.storage);
+		if (rc != 0)
+			return fail(LBM_ERR_CUDA, "collision plugin %d step launch failed: %s", h->d.collision,
+						cudaGetErrorString((cudaError_t) rc));
+		if (dry_run)
+			return LBM_OK;
+		h->last_blocks = blocks;
+		h->iteration++;
+		return LBM_OK;
 	}
 	cudaError_t err = cudaErrorNotSupported;
 	// the two-site coupled step (FP32 storage, plain steps of a lattice with a map)
@@ -312,6 +338,30 @@ const char* lbm_last_error(void)
 	return g_error.c_str();
 }
 
+int lbm_register_collision(int32_t id, lbm_collision_launcher launcher, int32_t abi_version, const char* name)
+{
+	if (!plugin_id(id))
+		return fail(LBM_ERR_INVALID, "collision plugin id %d outside %d .. %d", id, LBM_COLL_PLUGIN_FIRST,
+					LBM_COLL_PLUGIN_LAST);
+	if (abi_version != LBM_PLUGIN_ABI_VERSION)
+		return fail(LBM_ERR_UNSUPPORTED, "collision plugin built for plugin ABI %d, the library has %d", abi_version,
+					LBM_PLUGIN_ABI_VERSION);
+	std::lock_guard<std::mutex> lock(g_plugins_mutex);
+	CollisionPlugin& slot = g_plugins[id - LBM_COLL_PLUGIN_FIRST];
+	slot.launch = launcher;
+	slot.name = launcher ? (name ? name : "") : "";
+	return LBM_OK;
+}
+
+const char* lbm_collision_name(int32_t id)
+{
+	if (!plugin_id(id))
+		return nullptr;
+	std::lock_guard<std::mutex> lock(g_plugins_mutex);
+	const CollisionPlugin& slot = g_plugins[id - LBM_COLL_PLUGIN_FIRST];
+	return slot.launch ? slot.name.c_str() : nullptr;
+}
+
 const char* lbm_version(void)
 {
 	return "tnl-lbm-b200 0.1 (sm_100a, D3Q27 A-A)";
@@ -329,7 +379,20 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 		return fail(LBM_ERR_SIZE, "lattice sizes beyond the launch limits");
 	if (d.storage < 0 || d.storage >= lbm::ST_COUNT)
 		return fail(LBM_ERR_INVALID, "unknown storage %d", d.storage);
-	if (d.collision < LBM_COLL_CUM || d.collision > LBM_COLL_MRT)
+	lbm_collision_launcher plugin = nullptr;
+	if (plugin_id(d.collision)) {
+		{
+			std::lock_guard<std::mutex> lock(g_plugins_mutex);
+			plugin = g_plugins[d.collision - LBM_COLL_PLUGIN_FIRST].launch;
+		}
+		if (!plugin)
+			return fail(LBM_ERR_INVALID, "no collision plugin registered under id %d", d.collision);
+		if (plugin(nullptr, d.storage) != 0)
+			return fail(LBM_ERR_UNSUPPORTED, "collision plugin %d was not built for storage %d", d.collision, d.storage);
+		if (d.cum_flags != 0)
+			return fail(LBM_ERR_INVALID, "cumulant flags %d given for a collision plugin", d.cum_flags);
+	}
+	else if (d.collision < LBM_COLL_CUM || d.collision > LBM_COLL_MRT)
 		return fail(LBM_ERR_INVALID, "unknown collision %d", d.collision);
 	if (d.collision == LBM_COLL_CUM && d.cum_flags != 0 && d.cum_flags != LBM_CUM_ANTIALIAS
 		&& d.cum_flags != (LBM_CUM_GEIER_2017 | LBM_CUM_ANTIALIAS))
@@ -347,6 +410,7 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 
 	lbm_lattice* h = new lbm_lattice();
 	h->d = d;
+	h->plugin = plugin;
 	h->ops = &lbm::storage_ops(d.storage);
 	const int es = h->ops->elem_size;
 	h->g = lbm::make_geometry(d.X, d.Y, d.Z, es);
@@ -962,6 +1026,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	// the direct and the two-site kernel take the block shape
 	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->d.collision == LBM_COLL_CUM
 					  && h->streaming == LBM_STREAMING_AA;
+	// a collision plugin runs its own direct kernel: only the block shape is tuned
 	for (auto& c : cands) {
 		if (c[0] > 32 && c[0] / 2 >= h->d.X)
 			continue;  // far wider than the lattice
@@ -994,7 +1059,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	// the tile kernel and, with a map, the split step (the block shape does
 	// not apply to them)
 	for (int k : {(int) lbm::KERNEL_TILE, (int) lbm::KERNEL_SPLIT}) {
-		if (k == lbm::KERNEL_SPLIT && !h->split_tiles)
+		if ((k == lbm::KERNEL_SPLIT && !h->split_tiles) || h->plugin)
 			continue;
 		h->kernel = k;
 		launch_step(h, false, false);
@@ -1083,6 +1148,8 @@ int lbm_set_streaming(lbm_handle h, int streaming)
 		return LBM_OK;
 	if (h->ade)
 		return fail(LBM_ERR_UNSUPPORTED, "the coupled scalar runs on A-A lattices only (lbm_ade_disable first)");
+	if (h->plugin)
+		return fail(LBM_ERR_UNSUPPORTED, "a collision plugin runs with A-A streaming only");
 	if (streaming == LBM_STREAMING_AA) {
 		for (uint8_t g : h->map_host)
 			if (!site_type_supported(g))
@@ -1115,6 +1182,8 @@ int lbm_set_kernel(lbm_handle h, int kernel)
 		return rc;
 	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE && kernel != LBM_KERNEL_SPLIT && kernel != LBM_KERNEL_PAIR)
 		return fail(LBM_ERR_INVALID, "unknown kernel %d", kernel);
+	if (h->plugin && kernel != LBM_KERNEL_DIRECT)
+		return fail(LBM_ERR_UNSUPPORTED, "a collision plugin runs the one-site kernel (LBM_KERNEL_DIRECT) only");
 	h->kernel = kernel;
 	h->drop_graph();
 	return LBM_OK;

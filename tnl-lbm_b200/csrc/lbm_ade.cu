@@ -241,6 +241,8 @@ int lbm_ade_enable(lbm_handle h, const lbm_ade_desc* desc)
 		return efail(LBM_ERR_UNSUPPORTED, "the coupled scalar needs FP64, FP32 or F32S storage (storage %s)", h->ops->name);
 	if (h->streaming != LBM_STREAMING_AA)
 		return efail(LBM_ERR_UNSUPPORTED, "the coupled scalar runs on A-A lattices only");
+	if (h->plugin)
+		return efail(LBM_ERR_UNSUPPORTED, "the coupled scalar runs with the built-in collisions only");
 	if (h->adjoint)
 		return efail(LBM_ERR_UNSUPPORTED, "release the adjoint first (lbm_adjoint_release)");
 	if (desc->collision < 0 || desc->collision > 2)

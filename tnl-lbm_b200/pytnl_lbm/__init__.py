@@ -18,13 +18,14 @@ import numpy as np
 
 from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
-    COLL_BGK, COLL_CUM, COLL_MRT, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
+    COLL_BGK, COLL_CUM, COLL_MRT, COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
     ADE_CLBM, ADE_GEO, ADE_MRT, ADE_SRT, GEO, KERNEL_DIRECT, KERNEL_PAIR, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
     STORE_BF16S, STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64, LbmError, library,
     library_path)
 
 __all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute", "Actions",
-           "Counter", "MAX_COUNTER", "NSE", "macro_from_populations"]
+           "Counter", "MAX_COUNTER", "NSE", "macro_from_populations", "register_collision", "unregister_collision",
+           "collision_name", "plugin_path"]
 
 # D3Q27_MACRO_Default quantity order (include/lbm3d/d3q27/macro.h:61-68)
 macro_names = ("rho", "vx", "vy", "vz")
@@ -500,6 +501,46 @@ class Ensemble:
     def autotune(self, ntrials=4):
         _abi.check(self.lib.lbm_ensemble_autotune(self.h, int(ntrials)))
         return self.shape()
+
+
+# loaded plugin libraries, kept alive while their launchers are registered
+_PLUGINS = {}
+
+
+def plugin_path(name):
+    """Path of a collision plugin built from tnl-lbm_b200/plugins/<name>.cu."""
+    return os.path.join(os.path.dirname(_abi.library_path()), "plugins", name + ".so")
+
+
+def register_collision(id, path, symbol, name=None):
+    """Register the collision plugin launcher `symbol` of the shared library
+    `path` (built with LBM_COLLISION_PLUGIN, tnl-lbm_b200/csrc/plugin.cuh)
+    under `id` in [COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST]; LBM(...,
+    collision=id) then runs it.  Returns id."""
+    lib = library()
+    if not os.path.exists(path):
+        raise LbmError(1, f"collision plugin {path} not found")
+    so = ctypes.CDLL(os.path.abspath(path))
+    fn = getattr(so, symbol)
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    addr = ctypes.cast(fn, ctypes.c_void_p).value
+    label = (name or symbol).encode()
+    _abi.check(lib.lbm_register_collision(int(id), addr, _abi.PLUGIN_ABI_VERSION, label))
+    _PLUGINS[int(id)] = (so, fn)
+    return int(id)
+
+
+def unregister_collision(id):
+    """Remove the plugin registered under `id`; lattices created with it keep
+    their launcher, and the plugin library stays loaded."""
+    _abi.check(library().lbm_register_collision(int(id), None, _abi.PLUGIN_ABI_VERSION, None))
+
+
+def collision_name(id):
+    """Name a plugin was registered under, or None."""
+    n = library().lbm_collision_name(int(id))
+    return None if n is None else n.decode()
 
 
 def kinetic_energy(lbm: LBM, rho0=1.0):

@@ -11,6 +11,8 @@ ERRORS = {1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "non-fini
 
 STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S, STORE_F16SR, STORE_BF16SR = 0, 1, 2, 3, 4, 5, 6
 COLL_CUM, COLL_SRT, COLL_BGK, COLL_MRT = 0, 1, 2, 3
+COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST = 16, 31
+PLUGIN_ABI_VERSION = 1
 CUM_GEIER_2017, CUM_ANTIALIAS = 1, 2
 EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
 LAYOUT_INTERIOR, LAYOUT_GHOST = 0, 1
@@ -134,7 +136,12 @@ SIGNATURES = {
     "lbm_ensemble_set_shape": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int]),
     "lbm_ensemble_get_shape": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "lbm_ensemble_autotune": (ctypes.c_int, [_H, ctypes.c_int]),
+    "lbm_register_collision": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p]),
+    "lbm_collision_name": (ctypes.c_char_p, [ctypes.c_int32]),
 }
+
+# lbm_collision_launcher: int32_t (*)(const void* step, int32_t storage)
+COLLISION_LAUNCHER = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32)
 
 _LIB = None
 
