@@ -466,13 +466,25 @@ def max_over_ranks(dist, value, device):
     return float(t.item())
 
 
+def trt_plugin_id(pl):
+    """Register the example two-relaxation-time collision plugin
+    (tnl-lbm_b200/plugins/example_collisions.cu) in the open COLL slot."""
+    cid = pl.COLL_PLUGIN_FIRST
+    if pl.collision_name(cid) != "TRT":
+        pl.register_collision(cid, pl.plugin_path("example_collisions"), "lbm_example_trt", name="TRT")
+    return cid
+
+
 def make_lattice(pl, spec, storage, device, kernel="direct", collision="cum"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
           "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
-        coll = {"cum": pl.COLL_CUM, "srt": pl.COLL_SRT, "bgk": pl.COLL_BGK, "mrt": pl.COLL_MRT}[collision]
+        if collision == "plugin_trt":
+            coll = trt_plugin_id(pl)
+        else:
+            coll = {"cum": pl.COLL_CUM, "srt": pl.COLL_SRT, "bgk": pl.COLL_BGK, "mrt": pl.COLL_MRT}[collision]
         lat = pl.LBM(X, Y, Z, viscosity=nu, collision=coll, cum_flags=spec["cum_flags"],
                      equilibrium=pl.EQ_INV_CUM if collision == "cum" else pl.EQ_SECOND_ORDER, storage=st,
                      device=device)
@@ -728,9 +740,10 @@ def run_ours(args):
             vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
             variants[f"f32_{other}_kernel"] = {"mlups": sites * args.steps / vsecs / 1e6}
             vl.close()
-        # the other collisions of the COLL slot (one-site kernel, autotuned block)
+        # the other collisions of the COLL slot (one-site kernel, autotuned
+        # block), and a user-compiled collision through the plugin slot
         if spec["kind"] == "duct":
-            for coll in ("srt", "bgk", "mrt"):
+            for coll in ("srt", "bgk", "mrt", "plugin_trt"):
                 vl, _ = make_lattice(pl, spec, "f32", local, "direct", coll)
                 if args.autotune:
                     vl.autotune(16)

@@ -95,3 +95,41 @@ def test_descriptor_checks_for_plugin_ids(pl):
     d.storage, d.cum_flags = pl.STORE_F64, pl.CUM_ANTIALIAS
     assert lib.lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
     assert not h
+
+
+USER_PLUGIN = r"""
+#include "plugin.cuh"
+
+struct Relax
+{
+    template <typename R>
+    __device__ static void collision(lbm::Site<R>& s, const lbm::CollParams<R>& p)
+    {
+        R feq[27];
+        lbm::set_equilibrium(feq, p.eq, s.rho, s.vx, s.vy, s.vz);
+        for (int q = 0; q < 27; q++)
+            s.f[q] += (feq[q] - s.f[q]) * p.inv_tau;
+    }
+};
+
+LBM_COLLISION_PLUGIN(user_relax, Relax, LBM_PLUGIN_STORAGE(LBM_STORE_F64))
+"""
+
+
+def test_build_plugin_compiles_a_user_collision(pl, tmp_path):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("tnl_build", os.path.join(ROOT, "tnl-lbm_b200", "build.py"))
+    build = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(build)
+    if not os.path.exists(build.NVCC):
+        pytest.skip("nvcc unavailable")
+    src = tmp_path / "user_relax.cu"
+    src.write_text(USER_PLUGIN)
+    so = build.build_plugin(str(src), str(tmp_path / "user_relax.so"))
+    lib = ctypes.CDLL(so)
+    lib.user_relax.restype = ctypes.c_int32
+    lib.user_relax.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    assert lib.user_relax(None, pl.STORE_F64) == 0
+    assert lib.user_relax(None, pl.STORE_F32) == NOT_SUPPORTED
+    pl.register_collision(pl.COLL_PLUGIN_FIRST + 5, so, "user_relax", name="relax")
+    assert pl.collision_name(pl.COLL_PLUGIN_FIRST + 5) == "relax"
