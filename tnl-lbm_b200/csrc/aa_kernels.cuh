@@ -305,6 +305,15 @@ __device__ __forceinline__ void warp_reduce_store(const double (&v)[NRED], doubl
 	warp_reduce_store(v, partials, block * wpb + warp, nslots);
 }
 
+// Lets the grid launched after this one as a programmatic dependent (the
+// finish kernel of the sums) be scheduled once every block of this grid has
+// started; the dependent still waits for this grid's completion
+// (griddepcontrol.wait) before it reads anything.
+__device__ __forceinline__ void launch_dependents()
+{
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Outputs of an observation step for one site: the macro field and the
 // per-warp FP64 sums.  Every lane of the warp calls it (lanes past the
 // lattice edge with active = false).  The step kernels call it between the
@@ -425,6 +434,8 @@ template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT, int 
 __global__ void __launch_bounds__(128, MINB) aa_step_kernel(const StepArgs<typename S::T, typename S::R> a)
 {
 	using R = typename S::R;
+	if constexpr (OUT)
+		launch_dependents();
 	aa_step_site<S, ODD, GENERAL, OUT>(a, [&](Site<R>& s) { collide<R, COLL, CUMF>(s, a.p); });
 }
 

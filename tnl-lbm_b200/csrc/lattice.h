@@ -42,9 +42,19 @@ struct lbm_lattice
 	cudaStream_t stream = nullptr;
 	uint8_t* map = nullptr;
 	bool map_set = false;
+	// inlet profiles.  Two device sets: the steps read the current one
+	// (inflow[], a null component reads as zero); lbm_set_inflow uploads into
+	// the other set on upload_stream, so that the copy overlaps the steps
+	// still reading the current set, and makes it current
 	void* inflow[3] = {nullptr, nullptr, nullptr};
-	void* inflow_host = nullptr;  // pinned staging of the converted profiles
-	cudaEvent_t inflow_ev = nullptr;  // recorded after the staging's last copy
+	void* inflow_buf[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+	int inflow_cur = 0;
+	cudaStream_t upload_stream = nullptr;
+	cudaEvent_t inflow_ready = nullptr;						 // an upload has landed (upload_stream)
+	cudaEvent_t inflow_free[2] = {nullptr, nullptr};		 // set b no longer read (recorded on stream)
+	bool inflow_free_valid[2] = {false, false};
+	void* inflow_host = nullptr;							 // pinned staging [2][3][Z Y], compute type
+	cudaEvent_t inflow_staged[2] = {nullptr, nullptr};		 // staging slot b copied out (upload_stream)
 	void* macro = nullptr;
 	bool macro_valid = false;
 	double* partials = nullptr;
@@ -65,12 +75,20 @@ struct lbm_lattice
 	long long wait_limit = -1;	// tile kernel's loop waits (lbm_set_wait_limit); negative: the default
 	long long last_blocks = 0;	// partial-sum slots of the last step launch
 	lbm::CollParamsD p{};
-	// CUDA graph of GRAPH_STEPS plain steps starting at an even iteration
-	cudaGraphExec_t graph = nullptr;
+	// CUDA graphs of GRAPH_STEPS plain steps starting at an even iteration,
+	// for the population buffer and inlet profiles they were captured with
+	// (two: the two inlet sets of alternating lbm_set_inflow calls)
+	struct GraphSlot
+	{
+		cudaGraphExec_t exec = nullptr;
+		const void* f = nullptr;
+		const void* inflow[3] = {nullptr, nullptr, nullptr};
+	};
+	GraphSlot graphs[2];
+	int graph_next = 0;	 // slot the next capture replaces
 	std::vector<uint8_t> map_host;			 // host copy of the accepted map
 	int streaming = LBM_STREAMING_AA;
 	void* f_out = nullptr;		// A-B: the write buffer (swapped with g.f after every step)
-	void* graph_in = nullptr;	// g.f when the graph was captured
 	unsigned* split_tiles = nullptr;  // split step: fluid-only tiles, then the others
 	long long split_n[2] = {0, 0};
 	int split_tiles_x = 0;
@@ -126,10 +144,12 @@ struct lbm_lattice
 	}
 	void drop_graph()
 	{
-		if (graph) {
-			cudaGraphExecDestroy(graph);
-			graph = nullptr;
+		for (GraphSlot& g : graphs) {
+			if (g.exec)
+				cudaGraphExecDestroy(g.exec);
+			g = GraphSlot{};
 		}
+		graph_next = 0;
 	}
 };
 

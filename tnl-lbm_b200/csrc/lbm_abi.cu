@@ -262,9 +262,23 @@ int sync_ab_buffers(lbm_handle h)
 	return LBM_OK;
 }
 
+// the graph slot captured with the current population buffer and inlet
+// profiles, or null
+lbm_lattice::GraphSlot* current_graph(lbm_handle h)
+{
+	for (lbm_lattice::GraphSlot& g : h->graphs)
+		if (g.exec && g.f == h->g.f && g.inflow[0] == h->inflow[0] && g.inflow[1] == h->inflow[1]
+			&& g.inflow[2] == h->inflow[2])
+			return &g;
+	return nullptr;
+}
+
 int build_graph(lbm_handle h)
 {
-	h->drop_graph();
+	lbm_lattice::GraphSlot& slot = h->graphs[h->graph_next];
+	if (slot.exec)
+		cudaGraphExecDestroy(slot.exec);
+	slot = lbm_lattice::GraphSlot{};
 	const long long saved = h->iteration;
 	// resolve per-kernel launch attributes outside of the capture
 	for (int parity = 0; parity < 2; parity++) {
@@ -276,7 +290,6 @@ int build_graph(lbm_handle h)
 		}
 	}
 	h->iteration = 0;  // graph starts at an even step
-	h->graph_in = h->g.f;
 	cudaGraph_t graph = nullptr;
 	LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
 	int rc = LBM_OK;
@@ -291,12 +304,16 @@ int build_graph(lbm_handle h)
 	}
 	if (end != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(end));
-	const cudaError_t inst = cudaGraphInstantiate(&h->graph, graph, 0);
+	const cudaError_t inst = cudaGraphInstantiate(&slot.exec, graph, 0);
 	cudaGraphDestroy(graph);
 	if (inst != cudaSuccess) {
-		h->graph = nullptr;
+		slot.exec = nullptr;
 		return fail(LBM_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(inst));
 	}
+	slot.f = h->g.f;
+	for (int k = 0; k < 3; k++)
+		slot.inflow[k] = h->inflow[k];
+	h->graph_next ^= 1;
 	return LBM_OK;
 }
 
@@ -309,13 +326,14 @@ int run_plain_steps(lbm_handle h, long long n)
 		n--;
 	}
 	if (h->d.use_graphs && n >= lbm_lattice::GRAPH_STEPS) {
-		if (!h->graph || h->graph_in != h->g.f) {
-			int rc = build_graph(h);
-			if (rc)
+		lbm_lattice::GraphSlot* g = current_graph(h);
+		if (!g) {
+			if (int rc = build_graph(h))
 				return rc;
+			g = current_graph(h);
 		}
 		while (n >= lbm_lattice::GRAPH_STEPS) {
-			LBM_CUDA(cudaGraphLaunch(h->graph, h->stream));
+			LBM_CUDA(cudaGraphLaunch(g->exec, h->stream));
 			h->iteration += lbm_lattice::GRAPH_STEPS;
 			n -= lbm_lattice::GRAPH_STEPS;
 		}
@@ -476,13 +494,19 @@ int lbm_destroy(lbm_handle h)
 	cudaFree(h->pair_groups);
 	cudaFree(h->stats);
 	cudaFree(h->map);
-	for (auto* p : h->inflow)
-		cudaFree(p);
+	if (h->upload_stream)
+		cudaStreamSynchronize(h->upload_stream);
+	for (auto& set : h->inflow_buf)
+		for (void* p : set)
+			cudaFree(p);
 	cudaFree(h->macro);
 	if (h->inflow_host)
 		cudaFreeHost(h->inflow_host);
-	if (h->inflow_ev)
-		cudaEventDestroy(h->inflow_ev);
+	for (cudaEvent_t ev : {h->inflow_ready, h->inflow_free[0], h->inflow_free[1], h->inflow_staged[0], h->inflow_staged[1]})
+		if (ev)
+			cudaEventDestroy(ev);
+	if (h->upload_stream)
+		cudaStreamDestroy(h->upload_stream);
 	if (h->halo_ev)
 		cudaEventDestroy(h->halo_ev);
 	cudaFree(h->partials);
@@ -643,36 +667,44 @@ int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const doubl
 	const double* src[3] = {vx, vy, vz};
 	const size_t n = (size_t) h->d.Y * h->d.Z;
 	const int cs = h->ops->compute_size;
-	if (!h->inflow_host)
-		LBM_CUDA(cudaMallocHost(&h->inflow_host, 3 * n * cs));
-	if (!h->inflow_ev)
-		LBM_CUDA(cudaEventCreateWithFlags(&h->inflow_ev, cudaEventDisableTiming));
-	// the staging buffer is reused: wait for the copies of the previous call
-	// (normally long done) instead of synchronising the stream after each call
-	LBM_CUDA(cudaEventSynchronize(h->inflow_ev));
-	bool realloc = false;
+	if (!h->upload_stream) {
+		LBM_CUDA(cudaMallocHost(&h->inflow_host, 2 * 3 * n * cs));
+		LBM_CUDA(cudaStreamCreateWithFlags(&h->upload_stream, cudaStreamNonBlocking));
+		for (cudaEvent_t* ev : {&h->inflow_ready, &h->inflow_free[0], &h->inflow_free[1], &h->inflow_staged[0], &h->inflow_staged[1]})
+			LBM_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+	}
+	// upload into the set that is not current, from staging slot b: the
+	// slot's previous copies (two calls ago) are normally long done, and the
+	// set's last readers are the steps queued before it stopped being current
+	const int b = h->inflow_cur ^ 1;
+	LBM_CUDA(cudaEventSynchronize(h->inflow_staged[b]));
+	if (h->inflow_free_valid[b])
+		LBM_CUDA(cudaStreamWaitEvent(h->upload_stream, h->inflow_free[b], 0));
+	void* next[3] = {nullptr, nullptr, nullptr};
 	for (int k = 0; k < 3; k++) {
-		if (!src[k]) {
-			if (h->inflow[k]) {
-				LBM_CUDA(cudaMemsetAsync(h->inflow[k], 0, n * cs, h->stream));
-			}
-			continue;
-		}
-		if (!h->inflow[k]) {
-			LBM_CUDA(cudaMalloc(&h->inflow[k], n * cs));
-			realloc = true;
-		}
-		unsigned char* stage = (unsigned char*) h->inflow_host + k * n * cs;
+		if (!src[k])
+			continue;  // a null component reads as zero
+		if (!h->inflow_buf[b][k])
+			LBM_CUDA(cudaMalloc(&h->inflow_buf[b][k], n * cs));
+		unsigned char* stage = (unsigned char*) h->inflow_host + (size_t) (3 * b + k) * n * cs;
 		if (cs == 8)
 			std::memcpy(stage, src[k], n * 8);
 		else
 			for (size_t i = 0; i < n; i++)
 				((float*) stage)[i] = (float) src[k][i];
-		LBM_CUDA(cudaMemcpyAsync(h->inflow[k], stage, n * cs, cudaMemcpyHostToDevice, h->stream));
+		LBM_CUDA(cudaMemcpyAsync(h->inflow_buf[b][k], stage, n * cs, cudaMemcpyHostToDevice, h->upload_stream));
+		next[k] = h->inflow_buf[b][k];
 	}
-	LBM_CUDA(cudaEventRecord(h->inflow_ev, h->stream));
-	if (realloc)
-		h->drop_graph();  // kernel arguments changed; new values alone need no new graph
+	LBM_CUDA(cudaEventRecord(h->inflow_staged[b], h->upload_stream));
+	LBM_CUDA(cudaEventRecord(h->inflow_ready, h->upload_stream));
+	// later work on the lattice's stream sees the new profiles; the current
+	// set is free once the work queued so far is done
+	LBM_CUDA(cudaStreamWaitEvent(h->stream, h->inflow_ready, 0));
+	LBM_CUDA(cudaEventRecord(h->inflow_free[h->inflow_cur], h->stream));
+	h->inflow_free_valid[h->inflow_cur] = true;
+	h->inflow_cur = b;
+	for (int k = 0; k < 3; k++)
+		h->inflow[k] = next[k];
 	return LBM_OK;
 }
 

@@ -51,6 +51,9 @@ __global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __
 {
 	__shared__ double sh[FINISH_WARPS][NRED];
 	__shared__ bool last;
+	// launched as a programmatic dependent of the step that wrote the
+	// partials: wait until that grid has completed and its writes are visible
+	asm volatile("griddepcontrol.wait;" ::: "memory");
 	const long long chunk = (nslots + gridDim.x - 1) / gridDim.x;
 	const long long b0 = blockIdx.x * chunk;
 	const long long b1 = b0 + chunk < nslots ? b0 + chunk : nslots;
@@ -98,8 +101,20 @@ long long finish_scratch_doubles()
 
 cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out, cudaStream_t st)
 {
-	finish_kernel<<<FINISH_BLOCKS, FINISH_THREADS, 0, st>>>(partials, nslots, stage, arrived, out);
-	return cudaGetLastError();
+	// programmatic dependent launch: the finish grid is scheduled while the
+	// step's last blocks run (the step kernels trigger it when they start)
+	// instead of after the step has drained, and waits in griddepcontrol.wait
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(FINISH_BLOCKS);
+	cfg.blockDim = dim3(FINISH_THREADS);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = st;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, finish_kernel, partials, nslots, stage, arrived, out);
 }
 
 // rho * |grad u|^2 per site with periodic central differences

@@ -472,8 +472,14 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 		if (act)
 			density_velocity(s, p2);
 	}
-	if constexpr (OUT)
+	if constexpr (OUT) {
+		if (act) {
+			collide_cumulant<F2, CUMF>(s, p2);
+			pair_write_at<S, ODD>(at, ps, s);
+		}
 		pair_outputs(a, act, act, site, s, slot, nslots);
+		return;
+	}
 	else
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
 	if (!act)
@@ -551,6 +557,8 @@ template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
 															 const PairSlots ps, long long red_slots)
 {
+	if constexpr (OUT)
+		launch_dependents();
 	const int wpb = (blockDim.x * blockDim.y) >> 5;
 	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
 	const long long slot = block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5);
@@ -571,6 +579,8 @@ __global__ void __launch_bounds__(128, MINB)
 						const uint8_t* __restrict__ groups, const unsigned* __restrict__ work,
 						const unsigned long long* __restrict__ rest, long long nrest, int tiles_x)
 {
+	if constexpr (OUT)
+		launch_dependents();
 	const unsigned w = work[blockIdx.x];
 	const long long slot = (long long) blockIdx.x * 4 + (threadIdx.x >> 5);
 	const long long nslots = (long long) gridDim.x * 4;

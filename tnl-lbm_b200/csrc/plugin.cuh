@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(128, plugin_minb<typename S::R>())
 	aa_step_plugin_kernel(const StepArgs<typename S::T, typename S::R> a)
 {
 	using R = typename S::R;
+	if constexpr (OUT)
+		launch_dependents();
 	aa_step_site<S, ODD, GENERAL, OUT>(a, [&](Site<R>& s) { C::template collision<R>(s, a.p); });
 }
 
