@@ -120,7 +120,10 @@ LBM_API int lbm_set_map(lbm_handle h, const uint8_t* map);
  * copyMapToHost (include/lbm3d/lbm.h:66). */
 LBM_API int lbm_get_map(lbm_handle h, uint8_t* map);
 
-/* Inlet velocity profiles, host [Z][Y] doubles; NULL means zero.
+/* Inlet velocity profiles, host [Z][Y] doubles; NULL means zero.  The
+ * values are copied before the call returns (the caller may reuse its
+ * buffers); the upload to the device overlaps the steps already enqueued,
+ * and every step enqueued after the call sees the new profiles.
  * Replaces NSE_Data_InflowProfile (include/lbm3d/lbm_data.h:95-133). */
 LBM_API int lbm_set_inflow(lbm_handle h, const double* vx, const double* vy, const double* vz);
 
@@ -160,7 +163,8 @@ LBM_API int lbm_set_iteration(lbm_handle h, int64_t iteration);
 LBM_API int lbm_get_macro(lbm_handle h, double* host);
 
 /* Sums of the last step run with LBM_STEP_SUMS: out[6] = {sum rho, sum rho vx,
- * sum rho vy, sum rho vz, sum rho |u|^2, non-finite count}.  Returns
+ * sum rho vy, sum rho vz, sum rho |u|^2, non-finite count}, accumulated in
+ * FP64 (GEO_NOTHING sites count as rho = 1, u = 0).  Returns
  * LBM_ERR_NONFINITE when the count is non-zero (state.hpp:1469-1492). */
 LBM_API int lbm_get_sums(lbm_handle h, double* out);
 /* The sums of the observation step (LBM_STEP_SUMS) that ended at `iteration`;

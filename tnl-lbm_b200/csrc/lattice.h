@@ -74,6 +74,10 @@ struct lbm_lattice
 	int* status_dev = nullptr;	// STATUS_* bits set by the kernels
 	long long wait_limit = -1;	// tile kernel's loop waits (lbm_set_wait_limit); negative: the default
 	long long last_blocks = 0;	// partial-sum slots of the last step launch
+	long long nothing_sites = 0;  // GEO_NOTHING sites of the map
+	// the last step's partial sums leave out its GEO_NOTHING sites (each adds
+	// rho = 1 and nothing else; the finish kernel adds them to the mass)
+	bool last_nothing_skipped = false;
 	lbm::CollParamsD p{};
 	// CUDA graphs of GRAPH_STEPS plain steps starting at an even iteration,
 	// for the population buffer and inlet profiles they were captured with

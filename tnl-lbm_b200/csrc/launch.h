@@ -88,6 +88,9 @@ struct StepLaunch
 	// observation steps (pair.cuh aa_pair_work_kernel)
 	const uint8_t* pair_groups;	 // PAIR_GROUP_* per group of PAIR_GROUP sites of a row
 	PairWork pair_work, pair_work_out;
+	// set by a step whose partial sums leave out the GEO_NOTHING sites (a
+	// sums-only step of the pair kernel over the plain work list), or null
+	bool* nothing_skipped;
 };
 
 // the coupled D3Q7 advection-diffusion scalar of a lattice (ade.cuh)
@@ -184,8 +187,10 @@ constexpr int NRED_HOST = 6;
 // zero between launches (one per stream that runs finish_sums); out may be
 // device or mapped host memory
 long long finish_scratch_doubles();
+// mass_offset is added to the summed mass (sites left out of the partials
+// that each contribute a known density)
 cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out,
-						cudaStream_t);
+						cudaStream_t, double mass_offset = 0.0);
 // enstrophy-type sum rho * |grad u|^2 with central differences over the macro
 // field (compute type given by compute_size), periodic wrap as sim_4.cu:21-54
 cudaError_t enstrophy_partials(const void* macro, int compute_size, int X, int Y, int Z, double* partials, long long* nblocks,

@@ -199,6 +199,8 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	L.wait_limit = h->wait_limit;
 	long long blocks = 0;
 	L.blocks_out = &blocks;
+	bool nothing_skipped = false;
+	L.nothing_skipped = &nothing_skipped;
 	L.dry_run = dry_run;
 	L.f_out = h->f_out;
 	L.split_tiles = h->split_tiles;
@@ -224,6 +226,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 		if (dry_run)
 			return LBM_OK;
 		h->last_blocks = blocks;
+		h->last_nothing_skipped = false;
 		h->iteration++;
 		return LBM_OK;
 	}
@@ -247,6 +250,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	if (dry_run)
 		return LBM_OK;
 	h->last_blocks = blocks;
+	h->last_nothing_skipped = nothing_skipped;
 	h->iteration++;
 	if (ab)	 // pointer rotation of lbm.hpp:314-322
 		std::swap(h->g.f, h->f_out);
@@ -545,6 +549,9 @@ int lbm_set_map(lbm_handle h, const uint8_t* map)
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
 	h->map_host.assign(map, map + n);
 	h->map_set = true;
+	h->nothing_sites = 0;
+	for (size_t i = 0; i < n; i++)
+		h->nothing_sites += map[i] == lbm::GEO_NOTHING;
 	if (h->ade)
 		h->ade->pair_dirty = true;  // the coupled pair step's lists follow the flow map
 	// tiles of 128 x-sites for the split step: fluid-only ones first
@@ -834,8 +841,9 @@ int finish_observation(lbm_handle h)
 {
 	const int slot = h->sums_last ^ 1;
 	const long long nb = h->last_blocks;
+	const double mass_offset = h->last_nothing_skipped ? (double) h->nothing_sites : 0.0;
 	const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
-										   h->sums_mapped + slot * lbm::NRED_HOST, h->stream);
+										   h->sums_mapped + slot * lbm::NRED_HOST, h->stream, mass_offset);
 	if (e != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
 	LBM_CUDA(cudaEventRecord(h->sums_ev[slot], h->stream));

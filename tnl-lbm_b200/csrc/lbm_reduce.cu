@@ -47,7 +47,7 @@ __device__ __forceinline__ void block_sums(double (&v)[NRED], double (*sh)[NRED]
 
 __global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __restrict__ partials, long long nslots,
 																double* __restrict__ stage, unsigned* __restrict__ arrived,
-																double* __restrict__ out)
+																double* __restrict__ out, double mass_offset)
 {
 	__shared__ double sh[FINISH_WARPS][NRED];
 	__shared__ bool last;
@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(FINISH_THREADS) finish_kernel(const double* __
 			v[k] += __ldcg(stage + k * FINISH_BLOCKS + b);
 	block_sums(v, sh);
 	if (threadIdx.x == 0) {
+		v[0] += mass_offset;
 #pragma unroll
 		for (int k = 0; k < NRED; k++)
 			out[k] = v[k];
@@ -99,7 +100,8 @@ long long finish_scratch_doubles()
 	return (long long) FINISH_BLOCKS * NRED;
 }
 
-cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out, cudaStream_t st)
+cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out, cudaStream_t st,
+						double mass_offset)
 {
 	// programmatic dependent launch: the finish grid is scheduled while the
 	// step's last blocks run (the step kernels trigger it when they start)
@@ -114,7 +116,7 @@ cudaError_t finish_sums(const double* partials, long long nslots, double* stage,
 	attr[0].val.programmaticStreamSerializationAllowed = 1;
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
-	return cudaLaunchKernelEx(&cfg, finish_kernel, partials, nslots, stage, arrived, out);
+	return cudaLaunchKernelEx(&cfg, finish_kernel, partials, nslots, stage, arrived, out, mass_offset);
 }
 
 // rho * |grad u|^2 per site with periodic central differences

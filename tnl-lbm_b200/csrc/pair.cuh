@@ -622,7 +622,10 @@ cudaError_t pair_step(const StepLaunch& L)
 		return cudaErrorNotSupported;
 	if (L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS && L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
 		return cudaErrorInvalidValue;
-	const PairWork& W = out ? L.pair_work_out : L.pair_work;
+	// observation steps with the macro field run the work list that holds the
+	// GEO_NOTHING sites (they output rho = 1, u = 0); a sums-only step runs
+	// the plain list, and the finish kernel adds those sites' rho = 1 each
+	const PairWork& W = L.macro ? L.pair_work_out : L.pair_work;
 	if (general ? (!W.work || !L.pair_groups || W.nwork < 1) : (L.g.X % 2 != 0))
 		return cudaErrorNotSupported;
 	// 8- and 4-byte alignment of every pair's first site
@@ -658,6 +661,8 @@ cudaError_t pair_step(const StepLaunch& L)
 	const long long red_slots = (long long) grid.x * grid.y * grid.z * ((block.x * block.y) / 32);
 	if (L.blocks_out)
 		*L.blocks_out = red_slots;
+	if (L.nothing_skipped)
+		*L.nothing_skipped = general && L.partials && !L.macro;
 	if (L.dry_run)
 		return cudaSuccess;
 	const int tiles_x = (pairs + 127) / 128;
