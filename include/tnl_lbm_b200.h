@@ -198,11 +198,12 @@ LBM_API int lbm_autotune(lbm_handle h, int ntrials);
 #define LBM_KERNEL_SPLIT 3 /* lattices with a map: one launch over the tiles of 128
                               x-sites that hold only GEO_FLUID (no map read, no
                               boundary branch), one over the others */
-#define LBM_KERNEL_PAIR 4  /* two x-adjacent sites per thread, the cumulant collision
-                              of both on the packed FP32 (f32x2) instructions; storages
-                              with FP32 arithmetic and the cumulant only (everything
-                              else runs LBM_KERNEL_DIRECT).  Same update as the direct
-                              kernel up to the rounding of the fused multiply-adds. */
+#define LBM_KERNEL_PAIR 4  /* two x-adjacent sites per thread, the collision of both
+                              on the packed FP32 (f32x2) instructions; storages with
+                              FP32 arithmetic and the built-in collisions (FP64
+                              storage runs LBM_KERNEL_DIRECT).  Same update as the
+                              direct kernel up to the rounding of the fused
+                              multiply-adds. */
 LBM_API int lbm_set_kernel(lbm_handle h, int kernel);
 LBM_API int lbm_get_kernel(lbm_handle h, int* kernel);
 

@@ -1,7 +1,7 @@
 """The two-site step kernel (LBM_KERNEL_PAIR) against the direct kernel.
 
 Both kernels compute the same update; they differ only in how the multiply-adds
-of the cumulant collision are fused (the packed f32x2 instructions take the
+of the collision (the cumulant, SRT, BGK or MRT-LES) are fused (the packed f32x2 instructions take the
 products and sums as written, the scalar kernel lets the compiler contract
 them), so the states agree to FP32 rounding.  After 7 steps:
   FP32 / shifted FP32 storage   |f_pair - f_direct| <= 2e-6
@@ -99,22 +99,63 @@ def test_pair_kernel_long_run_tracks_direct_kernel(pl, port):
     assert abs(out[2][0] - ref[0]) <= 1e-6 * ref[0]
 
 
-def test_pair_kernel_falls_back_for_other_collisions(pl, port):
-    """MRT (and FP64 arithmetic) have no two-site kernel: LBM_KERNEL_PAIR runs
-    the direct kernel, bit for bit."""
+def test_pair_kernel_falls_back_for_fp64(pl, port):
+    """FP64 arithmetic has no two-site kernel: LBM_KERNEL_PAIR runs the direct
+    kernel, bit for bit."""
     X, Y, Z = 40, 9, 7
     rng = np.random.default_rng(11)
     f0 = seeded_state(port, rng, X, Y, Z, eq="EQ")
     res = []
     for kernel in (pl.KERNEL_DIRECT, pl.KERNEL_PAIR):
         lat = pl.LBM(X, Y, Z, viscosity=0.01, collision=pl.COLL_MRT, equilibrium=pl.EQ_SECOND_ORDER,
-                     storage=pl.STORE_F32, periodic=True)
+                     storage=pl.STORE_F64, periodic=True)
         lat.set_kernel(kernel)
-        lat.set_populations(f0.astype(np.float32))
+        lat.set_populations(f0)
         lat.step(5)
         res.append(lat.get_populations())
         lat.close()
     assert np.array_equal(res[0], res[1])
+
+
+def run_collision(pl, kernel, f0, X, Y, Z, storage, coll, eq, kind, steps=7):
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, collision=coll, equilibrium=eq, storage=getattr(pl, "STORE_" + storage),
+                 periodic=(kind == "periodic"), force=(1e-5, 0.0, 2e-6))
+    try:
+        if kind == "duct":
+            lat.set_map(duct_map(X, Y, Z))
+            lat.set_inflow(0.02 * np.ones((Z, Y)), 0.003 * np.ones((Z, Y)), None)
+        elif kind == "random":
+            lat.set_map(random_map(np.random.default_rng(X + Y), X, Y, Z))
+            lat.set_inflow(0.02 * np.ones((Z, Y)), None, None)
+        lat.set_kernel(kernel)
+        lat.set_populations(f0.astype(np.float32))
+        lat.step(steps, macro=True, sums=True)
+        assert lat.status() == 0
+        return lat.get_populations(), lat.macro(), lat.sums()
+    finally:
+        lat.close()
+
+
+@pytest.mark.parametrize("coll", ["SRT", "BGK", "MRT"])
+@pytest.mark.parametrize("storage", ["F32", "F32S", "F16S", "BF16SR"])
+@pytest.mark.parametrize("kind", ["periodic", "duct", "random"])
+@pytest.mark.parametrize("shape", [(128, 16, 8), (37, 9, 7)])
+def test_pair_kernel_other_collisions_match_direct_kernel(pl, port, coll, storage, kind, shape):
+    """SRT (both equilibria), BGK and MRT-LES on the two-site kernel: the same
+    update as the direct kernel to the bounds of the cumulant above."""
+    X, Y, Z = shape
+    rng = np.random.default_rng(X * 13 + Y)
+    f0 = seeded_state(port, rng, X, Y, Z, eq="EQ")
+    tol = STORAGES[storage]
+    eqs = (pl.EQ_SECOND_ORDER, pl.EQ_INV_CUM) if coll == "SRT" else (pl.EQ_SECOND_ORDER,)
+    for eq in eqs:
+        c = getattr(pl, "COLL_" + coll)
+        fd, md, sd = run_collision(pl, pl.KERNEL_DIRECT, f0, X, Y, Z, storage, c, eq, kind)
+        fp, mp, sp = run_collision(pl, pl.KERNEL_PAIR, f0, X, Y, Z, storage, c, eq, kind)
+        assert np.isfinite(fp).all()
+        assert np.max(np.abs(fp.astype(np.float64) - fd)) <= tol, (eq, np.max(np.abs(fp - fd)))
+        assert np.max(np.abs(mp.astype(np.float64) - md)) <= 8 * tol
+        np.testing.assert_allclose(sp, sd, rtol=1e-6, atol=8 * tol * X * Y * Z)
 
 
 def test_autotune_may_choose_the_pair_kernel(pl):

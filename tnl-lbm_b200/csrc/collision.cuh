@@ -421,13 +421,20 @@ __device__ __forceinline__ R force_term(const Site<R>& s, const CollParams<R>& p
 	return R(3) * ((R(cx(Q)) - s.vx) * p.fx + (R(cy(Q)) - s.vy) * p.fy + (R(cz(Q)) - s.vz) * p.fz) * irho;
 }
 
+// 1 / rho for the SRT forcing, 1 where rho = 0 (col_srt.h:19, the ADE case)
+template <typename R>
+__device__ __forceinline__ R inv_rho_or_one(const Site<R>& s)
+{
+	return s.rho == R(0) ? R(1) : s.ir;
+}
+
 // textbook BGK (col_srt.h:14-105)
 template <typename R>
 __device__ __forceinline__ void collide_srt(Site<R>& s, const CollParams<R>& p)
 {
 	R feq[27];
 	set_equilibrium(feq, p.eq, s.rho, s.vx, s.vy, s.vz);
-	const R irho = s.rho == R(0) ? R(1) : s.ir;
+	const R irho = inv_rho_or_one(s);
 #pragma unroll
 	for (int q = 0; q < 27; q++) {
 		R S;

@@ -1064,8 +1064,7 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	int best_kernel = lbm::KERNEL_DIRECT;
 	const int obx = h->bx, oby = h->by;
 	// the direct and the two-site kernel take the block shape
-	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->d.collision == LBM_COLL_CUM
-					  && h->streaming == LBM_STREAMING_AA;
+	const bool pair_ok = lbm::pair_step_of(h->d.storage) && !h->plugin && h->streaming == LBM_STREAMING_AA;
 	// a collision plugin runs its own direct kernel: only the block shape is tuned
 	for (auto& c : cands) {
 		if (c[0] > 32 && c[0] / 2 >= h->d.X)

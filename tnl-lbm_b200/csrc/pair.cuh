@@ -77,6 +77,16 @@ __device__ __forceinline__ F2 fabs(F2 a)
 {
 	return F2(fabsf(a.v.x), fabsf(a.v.y));
 }
+// per lane, correctly rounded as the scalar form
+__device__ __forceinline__ F2 sqrt(F2 a)
+{
+	return F2(sqrtf(a.v.x), sqrtf(a.v.y));
+}
+// 1 / rho of the SRT forcing per lane, 1 where rho = 0 (inv_rho_or_one)
+__device__ __forceinline__ F2 inv_rho_or_one(const Site<F2>& s)
+{
+	return F2(s.rho.v.x == 0.0f ? 1.0f : s.ir.v.x, s.rho.v.y == 0.0f ? 1.0f : s.ir.v.y);
+}
 template <>
 __device__ __forceinline__ F2 rcp<F2>(F2 x)
 {
@@ -437,7 +447,7 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 // rest_update, one thread per site.  OUT: the macro field and the partial sums
 // of the pair, the warp's sums in slot `slot` of nslots.  Every thread of the
 // warp calls it (threads past the lattice with x >= X).
-template <typename S, int CUMF, bool ODD, bool GENERAL, bool OUT>
+template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
 __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
 											const PairSlots& ps, const uint8_t* __restrict__ groups, int x, int y, int z,
 											long long slot, long long nslots)
@@ -472,19 +482,22 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 		if (act)
 			density_velocity(s, p2);
 	}
-	if constexpr (OUT) {
+	if constexpr (OUT && GENERAL) {
+		// the work kernel: populations first, sums after the stores
 		if (act) {
-			collide_cumulant<F2, CUMF>(s, p2);
+			collide<F2, COLL, CUMF>(s, p2);
 			pair_write_at<S, ODD>(at, ps, s);
 		}
 		pair_outputs(a, act, act, site, s, slot, nslots);
 		return;
 	}
+	else if constexpr (OUT)
+		pair_outputs(a, act, act, site, s, slot, nslots);  // no map: before the collision (fewer live registers)
 	else
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
 	if (!act)
 		return;
-	collide_cumulant<F2, CUMF>(s, p2);
+	collide<F2, COLL, CUMF>(s, p2);
 	pair_write_at<S, ODD>(at, ps, s);
 }
 
@@ -492,7 +505,7 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 // rest[i] = row << 32 | x with row = z Y + y (entries i >= n: no site);
 // GEO_NOTHING sites only give their outputs.  OUT: macro field and partial
 // sums, the warp's in slot `slot` of nslots.  Every thread of the warp calls it.
-template <typename S, int CUMF, bool ODD, bool OUT>
+template <typename S, int COLL, int CUMF, bool ODD, bool OUT>
 __device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>& a, const unsigned long long* __restrict__ rest,
 											long long n, long long i, long long slot, long long nslots)
 {
@@ -547,13 +560,13 @@ __device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>
 	if (!rw)
 		return;
 	if (coll)
-		collide_cumulant<float, CUMF>(s, a.p);
+		collide<float, COLL, CUMF>(s, a.p);
 	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
 }
 
 // One A-A step of a lattice without a map, two sites per thread: thread
 // (t, y) of the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).
-template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+template <typename S, int COLL, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
 															 const PairSlots ps, long long red_slots)
 {
@@ -562,7 +575,7 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 	const int wpb = (blockDim.x * blockDim.y) >> 5;
 	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
 	const long long slot = block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5);
-	pair_update<S, CUMF, ODD, false, OUT>(a, p2, ps, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
+	pair_update<S, COLL, CUMF, ODD, false, OUT>(a, p2, ps, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
 										  blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, slot, red_slots);
 }
 
@@ -573,7 +586,7 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 // chunk).  A plane's rest chunks come first and its pair tiles after them, so
 // the rest sites run while the pair tiles around them are in flight and share
 // their DRAM sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
-template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+template <typename S, int COLL, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
 	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const PairSlots ps,
 						const uint8_t* __restrict__ groups, const unsigned* __restrict__ work,
@@ -585,12 +598,12 @@ __global__ void __launch_bounds__(128, MINB)
 	const long long slot = (long long) blockIdx.x * 4 + (threadIdx.x >> 5);
 	const long long nslots = (long long) gridDim.x * 4;
 	if (w & PAIR_WORK_REST) {
-		rest_update<S, CUMF, ODD, OUT>(a, rest, nrest, (long long) (w & ~PAIR_WORK_REST) * 128 + threadIdx.x, slot, nslots);
+		rest_update<S, COLL, CUMF, ODD, OUT>(a, rest, nrest, (long long) (w & ~PAIR_WORK_REST) * 128 + threadIdx.x, slot, nslots);
 	}
 	else {
 		const unsigned row = w / (unsigned) tiles_x;
 		const int x = (int) (w - row * (unsigned) tiles_x) * 256 + 2 * (int) threadIdx.x;
-		pair_update<S, CUMF, ODD, true, OUT>(a, p2, ps, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
+		pair_update<S, COLL, CUMF, ODD, true, OUT>(a, p2, ps, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
 											 slot, nslots);
 	}
 }
@@ -598,7 +611,7 @@ __global__ void __launch_bounds__(128, MINB)
 // Resident 128-thread blocks per SM requested for the pair kernel (register
 // cap 65536 / (128 n)): the largest counts that compile without spills
 // (-Xptxas -v on sm_100a).
-template <typename T, int CUMF, bool ODD>
+template <typename T, int COLL, int CUMF, bool ODD>
 constexpr int pair_minb()
 {
 	// even steps fit 96 registers without spills; odd steps spill 8-32 bytes
@@ -606,6 +619,8 @@ constexpr int pair_minb()
 	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks.  The
 	// even step of the 16-bit formats runs 6 blocks (80 registers, 8-32 bytes
 	// of spills): duct F16S 35.2 against 34.4 GLUPS at 5
+	if (COLL == COLL_SRT || COLL == COLL_BGK)
+		return 4;
 	return sizeof(T) == 2 && !ODD ? 6 : 5;
 }
 // One A-A step through aa_pair_kernel (no map) or aa_pair_work_kernel (a map);
@@ -618,9 +633,10 @@ cudaError_t pair_step(const StepLaunch& L)
 	static_assert(sizeof(typename S::R) == 4, "the pair kernel computes in FP32");
 	const bool general = L.map != nullptr;
 	const bool out = L.macro || L.partials;
-	if (L.coll != COLL_CUM)
+	if (L.coll != COLL_CUM && L.coll != COLL_SRT && L.coll != COLL_BGK && L.coll != COLL_MRT)
 		return cudaErrorNotSupported;
-	if (L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS && L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
+	if (L.coll == COLL_CUM && L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS
+		&& L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
 		return cudaErrorInvalidValue;
 	// observation steps with the macro field run the work list that holds the
 	// GEO_NOTHING sites (they output rho = 1, u = 0); a sums-only step runs
@@ -666,37 +682,50 @@ cudaError_t pair_step(const StepLaunch& L)
 	if (L.dry_run)
 		return cudaSuccess;
 	const int tiles_x = (pairs + 127) / 128;
-#define LBM_PAIR_LAUNCH(CUMF, ODD)                                                                                        \
+#define LBM_PAIR_LAUNCH(COLL, CUMF, ODD)                                                                                        \
 	do {                                                                                                                  \
 		if (general) {                                                                                                    \
 			if (out)                                                                                                      \
-				aa_pair_work_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(        \
+				aa_pair_work_kernel<S, COLL, CUMF, ODD, true, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(        \
 					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 			else                                                                                                          \
-				aa_pair_work_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(       \
+				aa_pair_work_kernel<S, COLL, CUMF, ODD, false, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(       \
 					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
 		}                                                                                                                 \
 		else if (out)                                                                                                     \
-			aa_pair_kernel<S, CUMF, ODD, true, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);  \
+			aa_pair_kernel<S, COLL, CUMF, ODD, true, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);  \
 		else                                                                                                              \
-			aa_pair_kernel<S, CUMF, ODD, false, pair_minb<T, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots); \
+			aa_pair_kernel<S, COLL, CUMF, ODD, false, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots); \
 	} while (0)
-#define LBM_PAIR_PARITY(CUMF)           \
-	do {                                \
-		if (L.odd)                      \
-			LBM_PAIR_LAUNCH(CUMF, true);  \
-		else                            \
-			LBM_PAIR_LAUNCH(CUMF, false); \
+#define LBM_PAIR_PARITY(COLL, CUMF)           \
+	do {                                      \
+		if (L.odd)                            \
+			LBM_PAIR_LAUNCH(COLL, CUMF, true);  \
+		else                                  \
+			LBM_PAIR_LAUNCH(COLL, CUMF, false); \
 	} while (0)
-	switch (L.cum_flags) {
-		case 0:
-			LBM_PAIR_PARITY(0);
+	switch (L.coll) {
+		case COLL_SRT:
+			LBM_PAIR_PARITY(COLL_SRT, 0);
 			break;
-		case CUM_ANTIALIAS:
-			LBM_PAIR_PARITY(CUM_ANTIALIAS);
+		case COLL_BGK:
+			LBM_PAIR_PARITY(COLL_BGK, 0);
+			break;
+		case COLL_MRT:
+			LBM_PAIR_PARITY(COLL_MRT, 0);
 			break;
 		default:
-			LBM_PAIR_PARITY(CUM_2017 | CUM_ANTIALIAS);
+			switch (L.cum_flags) {
+				case 0:
+					LBM_PAIR_PARITY(COLL_CUM, 0);
+					break;
+				case CUM_ANTIALIAS:
+					LBM_PAIR_PARITY(COLL_CUM, CUM_ANTIALIAS);
+					break;
+				default:
+					LBM_PAIR_PARITY(COLL_CUM, CUM_2017 | CUM_ANTIALIAS);
+					break;
+			}
 			break;
 	}
 #undef LBM_PAIR_PARITY
