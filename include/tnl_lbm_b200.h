@@ -486,10 +486,11 @@ LBM_API int lbm_halo_copy(lbm_handle dst, int dst_z, lbm_handle src, int src_z, 
  * library it loads into.  Registration is process-wide; a handle keeps the
  * launcher it was created with, so the plugin's code must stay loaded while
  * such a handle lives.  launcher == NULL removes the id.  Plugin lattices run
- * the one-site kernel with A-A streaming (lbm_set_kernel accepts only
- * LBM_KERNEL_DIRECT, lbm_set_streaming only LBM_STREAMING_AA) and take no
- * coupled scalar, adjoint or ensemble. */
-#define LBM_PLUGIN_ABI_VERSION 1
+ * the one-site kernel, or with LBM_KERNEL_PAIR on storages with FP32
+ * arithmetic the two-site kernel, with A-A streaming (lbm_set_kernel accepts
+ * LBM_KERNEL_DIRECT and LBM_KERNEL_PAIR, lbm_set_streaming only
+ * LBM_STREAMING_AA) and take no coupled scalar, adjoint or ensemble. */
+#define LBM_PLUGIN_ABI_VERSION 2
 typedef int32_t (*lbm_collision_launcher)(const void* step, int32_t storage);
 LBM_API int lbm_register_collision(int32_t id, lbm_collision_launcher launcher, int32_t abi_version, const char* name);
 /* Name under which `id` was registered (NULL when none). */

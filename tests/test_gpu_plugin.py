@@ -9,8 +9,14 @@
   slot q holds the initial populations shifted by 2k c_q (np.roll), exactly.
 * A two-relaxation-time collision, which the built-ins do not have, matches a
   numpy restatement of collide-then-stream on a periodic lattice.
-* Restrictions: plugin lattices run the one-site kernel with A-A streaming
-  and take no coupled scalar or adjoint; graphs and the host loop agree.
+* With LBM_KERNEL_PAIR the plugins run on the two-site kernel (two sites per
+  thread, packed FP32): the SRT plugin equals the built-in SRT's two-site
+  step bit for bit, streaming stays exact, and TRT matches numpy; the sums of
+  a sums-only step (which leaves the GEO_NOTHING sites to the finish kernel)
+  agree with the one-site kernel's.
+* Restrictions: plugin lattices run the one-site or the two-site kernel with
+  A-A streaming and take no coupled scalar or adjoint; graphs and the host
+  loop agree.
 """
 import numpy as np
 import pytest
@@ -173,7 +179,7 @@ def test_graph_replay_equals_host_loop(pl):
 
 def test_plugin_lattice_restrictions(pl):
     lat = make(pl, SRT_ID, pl.STORE_F64, False)
-    for kernel in (pl.KERNEL_TILE, pl.KERNEL_SPLIT, pl.KERNEL_PAIR):
+    for kernel in (pl.KERNEL_TILE, pl.KERNEL_SPLIT):
         with pytest.raises(pl.LbmError) as e:
             lat.set_kernel(kernel)
         assert e.value.code == 2
@@ -186,10 +192,81 @@ def test_plugin_lattice_restrictions(pl):
     with pytest.raises(pl.LbmError) as e:
         lat.adjoint_forward(np.zeros((3, lat.Z, lat.Y, lat.X)), 4, np.zeros(0, np.int64), np.zeros((0, 3)))
     assert e.value.code == 2
+    lat.set_kernel(pl.KERNEL_PAIR)  # accepted; FP64 arithmetic runs the one-site kernel
     lat.autotune(2)
-    assert lat.kernel == pl.KERNEL_DIRECT
+    assert lat.kernel == pl.KERNEL_DIRECT  # FP64: no two-site candidate
     lat.step(4, sums=True)
     assert np.isfinite(lat.sums()).all()
+    lat.close()
+
+
+@pytest.mark.parametrize("storage", ["F32", "F32S", "F16S", "BF16SR"])
+@pytest.mark.parametrize("periodic", [False, True])
+def test_srt_plugin_on_the_two_site_kernel_equals_builtin_srt(pl, storage, periodic):
+    st = getattr(pl, "STORE_" + storage)
+    out = []
+    for coll in (pl.COLL_SRT, SRT_ID):
+        lat = make(pl, coll, st, periodic, force=(1e-5, 0.0, 2e-6))
+        lat.set_kernel(pl.KERNEL_PAIR)
+        lat.step(21)
+        lat.step(1, macro=True, sums=True)
+        m = lat.macro()
+        lat.step(1, sums=True)  # sums only: the GEO_NOTHING sites enter in the finish kernel
+        out.append((lat.get_populations(), m, lat.sums()))
+        lat.close()
+    (f0, m0, s0), (f1, m1, s1) = out
+    np.testing.assert_array_equal(f1, f0)
+    np.testing.assert_array_equal(m1, m0)
+    np.testing.assert_array_equal(s1, s0)
+
+
+def test_plugin_sums_on_the_two_site_kernel_match_the_one_site_kernel(pl):
+    sums = []
+    for kernel in (pl.KERNEL_DIRECT, pl.KERNEL_PAIR):
+        lat = make(pl, TRT_ID, pl.STORE_F32, False, shape=(40, 14, 12))
+        lat.set_kernel(kernel)
+        lat.step(9, sums=True)
+        sums.append(lat.sums())
+        lat.close()
+    # FP32 rounding of the two kernels differs (fused multiply-adds); the mass
+    # also checks the GEO_NOTHING sites added by the finish kernel (about 7 %
+    # of this lattice's sites)
+    np.testing.assert_allclose(sums[1][:5], sums[0][:5], rtol=1e-6, atol=1e-6 * sums[0][0])
+    assert sums[0][5] == sums[1][5] == 0
+
+
+def test_streaming_plugin_on_the_two_site_kernel(pl):
+    X, Y, Z = 14, 10, 8
+    lat = pl.LBM(X, Y, Z, viscosity=0.02, collision=STREAM_ID, storage=pl.STORE_F32, periodic=True)
+    lat.set_kernel(pl.KERNEL_PAIR)
+    f0 = (np.random.default_rng(12).random((27, Z, Y, X)) + 0.5).astype(np.float32)
+    lat.set_populations(f0, layout=pl.LAYOUT_INTERIOR)
+    lat.step(4)
+    f = lat.get_populations(layout=pl.LAYOUT_INTERIOR, dtype=np.float32)
+    for q in range(27):
+        np.testing.assert_array_equal(f[q], np.roll(f0[q], shift=(4 * CZ[q], 4 * CY[q], 4 * CX[q]), axis=(0, 1, 2)))
+    lat.close()
+
+
+def test_trt_plugin_on_the_two_site_kernel_matches_numpy(pl):
+    X, Y, Z = 12, 10, 8
+    nu = 0.01
+    rng = np.random.default_rng(3)
+    lat = pl.LBM(X, Y, Z, viscosity=nu, collision=TRT_ID, equilibrium=pl.EQ_SECOND_ORDER, storage=pl.STORE_F32,
+                 periodic=True)
+    lat.set_kernel(pl.KERNEL_PAIR)
+    rho = 1 + 0.01 * rng.standard_normal((Z, Y, X))
+    u = 0.04 * rng.standard_normal((3, Z, Y, X))
+    lat.init_equilibrium(rho, *u)
+    f0 = lat.get_populations(layout=pl.LAYOUT_INTERIOR)
+    lat.set_populations(f0 * (1 + 0.02 * rng.standard_normal(f0.shape)), layout=pl.LAYOUT_INTERIOR)
+    f0 = lat.get_populations(layout=pl.LAYOUT_INTERIOR)
+    lat.step(4)
+    f = lat.get_populations(layout=pl.LAYOUT_INTERIOR)
+    want = f0
+    for _ in range(4):
+        want = stream(trt_collide(want, nu))
+    assert np.max(np.abs(f - want)) / np.max(np.abs(want)) <= 2e-6
     lat.close()
 
 

@@ -21,6 +21,17 @@ def pl():
         pytnl_lbm.unregister_collision(i)
 
 
+def _abi_version(pl):
+    from pytnl_lbm import _abi
+    return _abi.PLUGIN_ABI_VERSION
+
+
+def test_python_abi_version_matches_the_header():
+    from pytnl_lbm import _abi
+    text = open(os.path.join(ROOT, "include", "tnl_lbm_b200.h")).read()
+    assert int(re.search(r"#define LBM_PLUGIN_ABI_VERSION (\d+)", text).group(1)) == _abi.PLUGIN_ABI_VERSION
+
+
 def example_path(pl):
     path = pl.plugin_path("example_collisions")
     if not os.path.exists(path):
@@ -56,8 +67,9 @@ def test_registration_checks_id_and_abi_version(pl):
         assert e.value.code == 1
     so = ctypes.CDLL(path)
     addr = ctypes.cast(so.lbm_example_trt, ctypes.c_void_p).value
-    assert lib.lbm_register_collision(pl.COLL_PLUGIN_FIRST, addr, 2, b"trt") == 2
-    assert b"plugin ABI 2" in lib.lbm_last_error()
+    bad_version = _abi_version(pl) + 1
+    assert lib.lbm_register_collision(pl.COLL_PLUGIN_FIRST, addr, bad_version, b"trt") == 2
+    assert f"plugin ABI {bad_version}".encode() in lib.lbm_last_error()
     assert pl.collision_name(pl.COLL_PLUGIN_FIRST) is None
     with pytest.raises(AttributeError):
         pl.register_collision(pl.COLL_PLUGIN_FIRST, path, "no_such_launcher")

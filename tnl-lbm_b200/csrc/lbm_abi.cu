@@ -226,7 +226,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 		if (dry_run)
 			return LBM_OK;
 		h->last_blocks = blocks;
-		h->last_nothing_skipped = false;
+		h->last_nothing_skipped = nothing_skipped;
 		h->iteration++;
 		return LBM_OK;
 	}
@@ -1064,8 +1064,9 @@ int lbm_autotune(lbm_handle h, int ntrials)
 	int best_kernel = lbm::KERNEL_DIRECT;
 	const int obx = h->bx, oby = h->by;
 	// the direct and the two-site kernel take the block shape
-	const bool pair_ok = lbm::pair_step_of(h->d.storage) && !h->plugin && h->streaming == LBM_STREAMING_AA;
-	// a collision plugin runs its own direct kernel: only the block shape is tuned
+	const bool pair_ok = lbm::pair_step_of(h->d.storage) && h->streaming == LBM_STREAMING_AA;
+	// a collision plugin runs its own one-site or two-site kernels: the tile
+	// and split kernels are not candidates
 	for (auto& c : cands) {
 		if (c[0] > 32 && c[0] / 2 >= h->d.X)
 			continue;  // far wider than the lattice
@@ -1221,8 +1222,8 @@ int lbm_set_kernel(lbm_handle h, int kernel)
 		return rc;
 	if (kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_TILE && kernel != LBM_KERNEL_SPLIT && kernel != LBM_KERNEL_PAIR)
 		return fail(LBM_ERR_INVALID, "unknown kernel %d", kernel);
-	if (h->plugin && kernel != LBM_KERNEL_DIRECT)
-		return fail(LBM_ERR_UNSUPPORTED, "a collision plugin runs the one-site kernel (LBM_KERNEL_DIRECT) only");
+	if (h->plugin && kernel != LBM_KERNEL_DIRECT && kernel != LBM_KERNEL_PAIR)
+		return fail(LBM_ERR_UNSUPPORTED, "a collision plugin runs the one-site or the two-site kernel (LBM_KERNEL_DIRECT, LBM_KERNEL_PAIR)");
 	h->kernel = kernel;
 	h->drop_graph();
 	return LBM_OK;

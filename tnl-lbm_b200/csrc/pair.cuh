@@ -447,7 +447,7 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 // rest_update, one thread per site.  OUT: the macro field and the partial sums
 // of the pair, the warp's sums in slot `slot` of nslots.  Every thread of the
 // warp calls it (threads past the lattice with x >= X).
-template <typename S, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
+template <typename S, typename C, bool ODD, bool GENERAL, bool OUT>
 __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
 											const PairSlots& ps, const uint8_t* __restrict__ groups, int x, int y, int z,
 											long long slot, long long nslots)
@@ -485,7 +485,7 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 	if constexpr (OUT && GENERAL) {
 		// the work kernel: populations first, sums after the stores
 		if (act) {
-			collide<F2, COLL, CUMF>(s, p2);
+			C::template collision<F2>(s, p2);
 			pair_write_at<S, ODD>(at, ps, s);
 		}
 		pair_outputs(a, act, act, site, s, slot, nslots);
@@ -497,7 +497,7 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 		__syncwarp();  // keeps the collision after the loads (fewer live registers)
 	if (!act)
 		return;
-	collide<F2, COLL, CUMF>(s, p2);
+	C::template collision<F2>(s, p2);
 	pair_write_at<S, ODD>(at, ps, s);
 }
 
@@ -505,7 +505,7 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 // rest[i] = row << 32 | x with row = z Y + y (entries i >= n: no site);
 // GEO_NOTHING sites only give their outputs.  OUT: macro field and partial
 // sums, the warp's in slot `slot` of nslots.  Every thread of the warp calls it.
-template <typename S, int COLL, int CUMF, bool ODD, bool OUT>
+template <typename S, typename C, bool ODD, bool OUT>
 __device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>& a, const unsigned long long* __restrict__ rest,
 											long long n, long long i, long long slot, long long nslots)
 {
@@ -560,13 +560,13 @@ __device__ __forceinline__ void rest_update(const StepArgs<typename S::T, float>
 	if (!rw)
 		return;
 	if (coll)
-		collide<float, COLL, CUMF>(s, a.p);
+		C::template collision<float>(s, a.p);
 	aa_write<S, ODD>(a.f, a.sq, base, o, s.f);
 }
 
 // One A-A step of a lattice without a map, two sites per thread: thread
 // (t, y) of the grid owns sites x = 2t and 2t + 1 of row (y, z = blockIdx.z).
-template <typename S, int COLL, int CUMF, bool ODD, bool OUT, int MINB>
+template <typename S, typename C, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2,
 															 const PairSlots ps, long long red_slots)
 {
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 	const int wpb = (blockDim.x * blockDim.y) >> 5;
 	const long long block = blockIdx.x + (long long) gridDim.x * (blockIdx.y + (long long) gridDim.y * blockIdx.z);
 	const long long slot = block * wpb + ((threadIdx.x + blockDim.x * threadIdx.y) >> 5);
-	pair_update<S, COLL, CUMF, ODD, false, OUT>(a, p2, ps, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
+	pair_update<S, C, ODD, false, OUT>(a, p2, ps, nullptr, 2 * (int) (blockIdx.x * blockDim.x + threadIdx.x),
 										  blockIdx.y * blockDim.y + threadIdx.y, blockIdx.z, slot, red_slots);
 }
 
@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(128, MINB) aa_pair_kernel(const StepArgs<typen
 // chunk).  A plane's rest chunks come first and its pair tiles after them, so
 // the rest sites run while the pair tiles around them are in flight and share
 // their DRAM sectors through L2.  Warp w of block b writes partial-sum slot 4 b + w.
-template <typename S, int COLL, int CUMF, bool ODD, bool OUT, int MINB>
+template <typename S, typename C, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
 	aa_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const PairSlots ps,
 						const uint8_t* __restrict__ groups, const unsigned* __restrict__ work,
@@ -598,12 +598,12 @@ __global__ void __launch_bounds__(128, MINB)
 	const long long slot = (long long) blockIdx.x * 4 + (threadIdx.x >> 5);
 	const long long nslots = (long long) gridDim.x * 4;
 	if (w & PAIR_WORK_REST) {
-		rest_update<S, COLL, CUMF, ODD, OUT>(a, rest, nrest, (long long) (w & ~PAIR_WORK_REST) * 128 + threadIdx.x, slot, nslots);
+		rest_update<S, C, ODD, OUT>(a, rest, nrest, (long long) (w & ~PAIR_WORK_REST) * 128 + threadIdx.x, slot, nslots);
 	}
 	else {
 		const unsigned row = w / (unsigned) tiles_x;
 		const int x = (int) (w - row * (unsigned) tiles_x) * 256 + 2 * (int) threadIdx.x;
-		pair_update<S, COLL, CUMF, ODD, true, OUT>(a, p2, ps, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
+		pair_update<S, C, ODD, true, OUT>(a, p2, ps, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y),
 											 slot, nslots);
 	}
 }
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(128, MINB)
 // Resident 128-thread blocks per SM requested for the pair kernel (register
 // cap 65536 / (128 n)): the largest counts that compile without spills
 // (-Xptxas -v on sm_100a).
-template <typename T, int COLL, int CUMF, bool ODD>
+template <typename T, int COLL, bool ODD>
 constexpr int pair_minb()
 {
 	// even steps fit 96 registers without spills; odd steps spill 8-32 bytes
@@ -623,21 +623,35 @@ constexpr int pair_minb()
 		return 4;
 	return sizeof(T) == 2 && !ODD ? 6 : 5;
 }
-// One A-A step through aa_pair_kernel (no map) or aa_pair_work_kernel (a map);
-// cudaErrorNotSupported for what they do not cover: collisions other than the
-// cumulant, periodic lattices of odd width.
-template <typename S>
-cudaError_t pair_step(const StepLaunch& L)
+// A built-in collision of the COLL slot as a collision type of the two-site
+// kernels (the shape a collision plugin's struct has, plugin.cuh), with its
+// resident blocks per SM
+template <int COLL, int CUMF>
+struct BuiltinCollision
+{
+	template <typename R>
+	__device__ static __forceinline__ void collision(Site<R>& s, const CollParams<R>& p)
+	{
+		collide<R, COLL, CUMF>(s, p);
+	}
+	template <typename T, bool ODD>
+	static constexpr int pair_minb()
+	{
+		return lbm::pair_minb<T, COLL, ODD>();
+	}
+};
+
+// One A-A step of collision type C (BuiltinCollision, or a collision
+// plugin's struct) through aa_pair_kernel (no map) or aa_pair_work_kernel (a
+// map); cudaErrorNotSupported for periodic lattices of odd width and for
+// storage geometries the two-site accesses cannot align to.
+template <typename S, typename C>
+cudaError_t pair_step_with(const StepLaunch& L)
 {
 	using T = typename S::T;
 	static_assert(sizeof(typename S::R) == 4, "the pair kernel computes in FP32");
 	const bool general = L.map != nullptr;
 	const bool out = L.macro || L.partials;
-	if (L.coll != COLL_CUM && L.coll != COLL_SRT && L.coll != COLL_BGK && L.coll != COLL_MRT)
-		return cudaErrorNotSupported;
-	if (L.coll == COLL_CUM && L.cum_flags != 0 && L.cum_flags != CUM_ANTIALIAS
-		&& L.cum_flags != (CUM_2017 | CUM_ANTIALIAS))
-		return cudaErrorInvalidValue;
 	// observation steps with the macro field run the work list that holds the
 	// GEO_NOTHING sites (they output rho = 1, u = 0); a sums-only step runs
 	// the plain list, and the finish kernel adds those sites' rho = 1 each
@@ -682,55 +696,56 @@ cudaError_t pair_step(const StepLaunch& L)
 	if (L.dry_run)
 		return cudaSuccess;
 	const int tiles_x = (pairs + 127) / 128;
-#define LBM_PAIR_LAUNCH(COLL, CUMF, ODD)                                                                                        \
-	do {                                                                                                                  \
-		if (general) {                                                                                                    \
-			if (out)                                                                                                      \
-				aa_pair_work_kernel<S, COLL, CUMF, ODD, true, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(        \
-					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
-			else                                                                                                          \
-				aa_pair_work_kernel<S, COLL, CUMF, ODD, false, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(       \
-					a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);                                             \
-		}                                                                                                                 \
-		else if (out)                                                                                                     \
-			aa_pair_kernel<S, COLL, CUMF, ODD, true, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);  \
-		else                                                                                                              \
-			aa_pair_kernel<S, COLL, CUMF, ODD, false, pair_minb<T, COLL, CUMF, ODD>()><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots); \
-	} while (0)
-#define LBM_PAIR_PARITY(COLL, CUMF)           \
-	do {                                      \
-		if (L.odd)                            \
-			LBM_PAIR_LAUNCH(COLL, CUMF, true);  \
-		else                                  \
-			LBM_PAIR_LAUNCH(COLL, CUMF, false); \
-	} while (0)
+	auto launch = [&](auto odd)
+	{
+		constexpr bool ODD = decltype(odd)::value;
+		constexpr int MINB = C::template pair_minb<T, ODD>();
+		if (general) {
+			if (out)
+				aa_pair_work_kernel<S, C, ODD, true, MINB>
+					<<<grid, block, 0, L.stream>>>(a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);
+			else
+				aa_pair_work_kernel<S, C, ODD, false, MINB>
+					<<<grid, block, 0, L.stream>>>(a, p2, ps, L.pair_groups, W.work, W.rest, W.nrest, tiles_x);
+		}
+		else if (out)
+			aa_pair_kernel<S, C, ODD, true, MINB><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);
+		else
+			aa_pair_kernel<S, C, ODD, false, MINB><<<grid, block, 0, L.stream>>>(a, p2, ps, red_slots);
+	};
+	if (L.odd)
+		launch(std::true_type{});
+	else
+		launch(std::false_type{});
+	return cudaGetLastError();
+}
+
+// One A-A step of the lattice's built-in collision on the two-site kernels;
+// cudaErrorNotSupported where they do not apply (see pair_step_with)
+template <typename S>
+cudaError_t pair_step(const StepLaunch& L)
+{
 	switch (L.coll) {
 		case COLL_SRT:
-			LBM_PAIR_PARITY(COLL_SRT, 0);
-			break;
+			return pair_step_with<S, BuiltinCollision<COLL_SRT, 0>>(L);
 		case COLL_BGK:
-			LBM_PAIR_PARITY(COLL_BGK, 0);
-			break;
+			return pair_step_with<S, BuiltinCollision<COLL_BGK, 0>>(L);
 		case COLL_MRT:
-			LBM_PAIR_PARITY(COLL_MRT, 0);
-			break;
-		default:
+			return pair_step_with<S, BuiltinCollision<COLL_MRT, 0>>(L);
+		case COLL_CUM:
 			switch (L.cum_flags) {
 				case 0:
-					LBM_PAIR_PARITY(COLL_CUM, 0);
-					break;
+					return pair_step_with<S, BuiltinCollision<COLL_CUM, 0>>(L);
 				case CUM_ANTIALIAS:
-					LBM_PAIR_PARITY(COLL_CUM, CUM_ANTIALIAS);
-					break;
+					return pair_step_with<S, BuiltinCollision<COLL_CUM, CUM_ANTIALIAS>>(L);
+				case CUM_2017 | CUM_ANTIALIAS:
+					return pair_step_with<S, BuiltinCollision<COLL_CUM, CUM_2017 | CUM_ANTIALIAS>>(L);
 				default:
-					LBM_PAIR_PARITY(COLL_CUM, CUM_2017 | CUM_ANTIALIAS);
-					break;
+					return cudaErrorInvalidValue;
 			}
-			break;
+		default:
+			return cudaErrorNotSupported;
 	}
-#undef LBM_PAIR_PARITY
-#undef LBM_PAIR_LAUNCH
-	return cudaGetLastError();
 }
 
 }  // namespace lbm

@@ -29,7 +29,13 @@
 // extern "C" launcher that lbm_register_collision takes.  The launcher runs
 // the library's own per-site step (aa_step_site: A-A streaming, every
 // boundary type of the map, macro and sums outputs) with the collision
-// inlined, one thread per site, as the built-in collisions' direct kernel.
+// inlined, one thread per site, as the built-in collisions' direct kernel;
+// with LBM_KERNEL_PAIR on a storage with FP32 arithmetic it runs the
+// two-site kernels (pair.cuh) instead, with R = F2: two x-adjacent sites per
+// thread on the packed FP32 instructions.  A collision written with the
+// arithmetic operators and the library's helpers (set_equilibrium, opp,
+// rcp, sqrt, fabs; no comparisons of R values) compiles for F2 as it does
+// for float and double.
 #pragma once
 
 #include <cstdint>
@@ -41,6 +47,7 @@
 #include "coll_params.cuh"
 #include "d3q27.cuh"
 #include "launch.h"
+#include "pair.cuh"
 
 // storage sets of a plugin: bit LBM_STORE_* per storage it is compiled for
 #define LBM_PLUGIN_STORAGE(st) (1u << (st))
@@ -66,6 +73,23 @@ __global__ void __launch_bounds__(128, plugin_minb<typename S::R>())
 	aa_step_site<S, ODD, GENERAL, OUT>(a, [&](Site<R>& s) { C::template collision<R>(s, a.p); });
 }
 
+// a plugin's collision struct on the two-site kernels: 4 resident blocks per
+// SM (128 registers), the budget of the built-in SRT and BGK
+template <typename C>
+struct PluginPairCollision
+{
+	template <typename R>
+	__device__ static __forceinline__ void collision(Site<R>& s, const CollParams<R>& p)
+	{
+		C::template collision<R>(s, p);
+	}
+	template <typename T, bool ODD>
+	static constexpr int pair_minb()
+	{
+		return 4;
+	}
+};
+
 template <typename S, typename C, bool ODD, bool GENERAL>
 cudaError_t plugin_launch(const StepLaunch& L)
 {
@@ -82,6 +106,14 @@ cudaError_t plugin_launch(const StepLaunch& L)
 template <typename S, typename C>
 cudaError_t plugin_step(const StepLaunch& L)
 {
+	if constexpr (sizeof(typename S::R) == 4)
+		if (L.kernel == KERNEL_PAIR) {
+			const cudaError_t e = pair_step_with<S, PluginPairCollision<C>>(L);
+			if (e != cudaErrorNotSupported)
+				return e;
+		}
+	if (L.nothing_skipped)
+		*L.nothing_skipped = false;
 	if (L.blocks_out)
 		*L.blocks_out = (long long) L.grid.x * L.grid.y * L.grid.z * ((L.block.x * L.block.y) / 32);
 	if (L.dry_run)

@@ -12,7 +12,7 @@ ERRORS = {1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "non-fini
 STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S, STORE_F16SR, STORE_BF16SR = 0, 1, 2, 3, 4, 5, 6
 COLL_CUM, COLL_SRT, COLL_BGK, COLL_MRT = 0, 1, 2, 3
 COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST = 16, 31
-PLUGIN_ABI_VERSION = 1
+PLUGIN_ABI_VERSION = 2
 CUM_GEIER_2017, CUM_ANTIALIAS = 1, 2
 EQ_SECOND_ORDER, EQ_INV_CUM = 0, 1
 LAYOUT_INTERIOR, LAYOUT_GHOST = 0, 1
