@@ -238,7 +238,7 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 				return rc;
 		err = lbm::ade_pair_step_f32(L);
 	}
-	// the two-site kernel where it applies (the cumulant on FP32 arithmetic),
+	// the two-site kernel where it applies (FP32 arithmetic),
 	// else the direct kernel
 	if (!h->ade && !ab && h->kernel == lbm::KERNEL_PAIR)
 		if (const lbm::PairStepFn pair = lbm::pair_step_of(h->d.storage))

@@ -225,7 +225,7 @@ int ens_launch_members(lbm_ensemble e)
 		L.grid = dim3((g.X + bx - 1) / bx, (g.Y + L.block.y - 1) / L.block.y, g.Z);
 		L.stream = e->lanes[m % nl];
 		L.kernel = lbm::KERNEL_DIRECT;
-		// the two-site kernel where it applies (cumulant, FP32 arithmetic, even X)
+		// the two-site kernel where it applies (FP32 arithmetic, even X)
 		cudaError_t err = cudaErrorNotSupported;
 		if (const lbm::PairStepFn pair = lbm::pair_step_of(e->storage))
 			err = pair(L);
