@@ -340,8 +340,8 @@ LBM_API int lbm_ensemble_synchronize(lbm_ensemble e);
  * 2 (every member runs the single-lattice kernel on one of up to 64 streams,
  * the members being independent branches of the captured graph; steps with
  * LBM_STEP_SUMS use the persistent kernel), or 3 (persistent, two x-adjacent
- * sites per thread on packed FP32 arithmetic; tile_sites 256, the cumulant,
- * an FP32-arithmetic storage and members of even width, else
+ * sites per thread on packed FP32 arithmetic; tile_sites 256, an
+ * FP32-arithmetic storage and members of even width, else
  * LBM_ERR_UNSUPPORTED). */
 LBM_API int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy);
 LBM_API int lbm_ensemble_get_shape(lbm_ensemble e, int* tile_sites, int* grid_policy);

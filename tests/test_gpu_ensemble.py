@@ -177,9 +177,29 @@ def test_two_site_policy_matches_single_lattices(pl, storage, flags):
     ens.close()
 
 
+@pytest.mark.parametrize("coll", ["SRT", "BGK", "MRT"])
+def test_two_site_policy_other_collisions_match_single_lattices(pl, coll):
+    """Grid policy 3 with SRT, BGK and MRT-LES against single lattices (the
+    direct kernel), FP32 storage, over an odd start and graph replays."""
+    cid = getattr(pl, "COLL_" + coll)
+    nus = NUS[:len(EVEN_SIZES)]
+    ens = pl.Ensemble(EVEN_SIZES, nus, collision=cid, equilibrium=pl.EQ_SECOND_ORDER, storage=pl.STORE_F32)
+    ens.set_shape(256, 3)
+    ens.init_taylor_green(0.05)
+    ens.step(21)
+    ens.step(20, sums=True)
+    sums = ens.sums()
+    for m, (size, nu) in enumerate(zip(EVEN_SIZES, nus)):
+        f_single, s_single = single_run(pl, size, nu, pl.STORE_F32, cid, 0, pl.EQ_SECOND_ORDER, 41)
+        assert rel_linf(ens.get_populations(m), f_single) <= TOL["F32"], f"member {m}"
+        np.testing.assert_allclose(sums[m, :5], s_single[:5], rtol=1e-6, atol=1e-6 * abs(s_single[0]))
+        assert sums[m, 5] == 0
+    ens.close()
+
+
 def test_two_site_policy_is_refused_where_it_does_not_apply(pl):
     cases = [(SIZES, pl.COLL_CUM, pl.STORE_F32, 256),         # members of odd width
-             (EVEN_SIZES, pl.COLL_MRT, pl.STORE_F32, 256),     # not the cumulant
+             (EVEN_SIZES, pl.COLL_MRT, pl.STORE_F64, 256),     # FP64 arithmetic
              (EVEN_SIZES, pl.COLL_CUM, pl.STORE_F64, 256),     # FP64 arithmetic
              (EVEN_SIZES, pl.COLL_CUM, pl.STORE_F32, 128)]     # tiles of 128 sites
     for sizes, coll, st, tile in cases:

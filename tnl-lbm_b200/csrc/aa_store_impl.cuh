@@ -381,7 +381,7 @@ struct StorageUnit
 	}
 
 	// grid policy 3: the persistent two-site kernel over tiles of 256 sites
-	template <int CUMF, bool ODD, bool OUT>
+	template <int COLL, int CUMF, bool ODD, bool OUT>
 	static cudaError_t ens_pair_launch(const EnsLaunch& L)
 	{
 		if constexpr (sizeof(R) != 4) {
@@ -389,7 +389,7 @@ struct StorageUnit
 			return cudaErrorNotSupported;
 		}
 		else {
-			auto kern = ens_pair_kernel<S, CUMF, ODD, OUT, ENS_PAIR_MINB>;
+			auto kern = ens_pair_kernel<S, COLL, CUMF, ODD, OUT, ENS_PAIR_MINB>;
 			static int per_sm_cache[64] = {0};
 			static int sms_cache[64] = {0};
 			int dev = 0;
@@ -427,11 +427,11 @@ struct StorageUnit
 	{
 		const bool out = L.partials != nullptr;
 		if (L.pair) {
-			if (COLL != COLL_CUM || L.tpb != 256)
+			if (L.tpb != 256)
 				return cudaErrorNotSupported;
 			if (L.odd)
-				return out ? ens_pair_launch<CUMF, true, true>(L) : ens_pair_launch<CUMF, true, false>(L);
-			return out ? ens_pair_launch<CUMF, false, true>(L) : ens_pair_launch<CUMF, false, false>(L);
+				return out ? ens_pair_launch<COLL, CUMF, true, true>(L) : ens_pair_launch<COLL, CUMF, true, false>(L);
+			return out ? ens_pair_launch<COLL, CUMF, false, true>(L) : ens_pair_launch<COLL, CUMF, false, false>(L);
 		}
 		if (L.tpb == 256) {
 			if (L.odd)

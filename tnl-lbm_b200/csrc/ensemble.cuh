@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(TPB, MINB)
 // block ran 7 % slower on 64 members).  Every member's X is even, so a tile's pairs
 // never straddle two rows.  OUT: per-tile FP64 partial sums as
 // ens_step_kernel's.
-template <typename S, int CUMF, bool ODD, bool OUT, int MINB>
+template <typename S, int COLL, int CUMF, bool ODD, bool OUT, int MINB>
 __global__ void __launch_bounds__(128, MINB)
 	ens_pair_kernel(const EnsMember<typename S::T, float>* __restrict__ members, const int* __restrict__ tile_member,
 					long long ntiles, double* __restrict__ partials)
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128, MINB)
 					red[5] += isfinite(rho) ? 0.0 : 1.0;
 				}
 			}
-			collide_cumulant<F2, CUMF>(s, M.p2);
+			collide<F2, COLL, CUMF>(s, M.p2);
 			pair_write_at<S, ODD>(at, ps, s);
 		}
 		if constexpr (OUT) {

@@ -130,11 +130,11 @@ struct lbm_ensemble_t
 
 namespace {
 
-// grid policy 3 (persistent two-site kernel): the cumulant on FP32
-// arithmetic, every member of even width
+// grid policy 3 (persistent two-site kernel): FP32 arithmetic, every member
+// of even width
 bool ens_pair_ok(lbm_ensemble e)
 {
-	if (e->collision != LBM_COLL_CUM || e->ops->compute_size != 4)
+	if (e->ops->compute_size != 4)
 		return false;
 	for (int m = 0; m < e->count; m++)
 		if (e->g[m].X % 2 != 0)
@@ -598,7 +598,7 @@ int lbm_ensemble_set_shape(lbm_ensemble e, int tile_sites, int grid_policy)
 		return efail(LBM_ERR_INVALID, "launch shape: tile_sites 128 or 256, grid_policy 0, 1, 2 or 3");
 	if (grid_policy == 3 && (tile_sites != 256 || !ens_pair_ok(e)))
 		return efail(LBM_ERR_UNSUPPORTED,
-					 "grid policy 3 (two-site kernel) needs tile_sites 256, the cumulant, FP32 arithmetic and members of even width");
+					 "grid policy 3 (two-site kernel) needs tile_sites 256, FP32 arithmetic and members of even width");
 	if (tile_sites != e->tile_sites) {
 		ENS_CUDA(cudaStreamSynchronize(e->stream));
 		e->tile_sites = tile_sites;
