@@ -64,7 +64,14 @@ struct lbm_lattice
 	cudaEvent_t sums_ev[2] = {nullptr, nullptr};  // recorded after each slot's finish kernel
 	long long sums_iter[2] = {-1, -1};			  // iteration at which each slot's step ended
 	int sums_last = 1;							  // slot of the last observation step
-	unsigned* finish_arrived = nullptr;	 // arrival counter of the finish kernel, zero between launches
+	unsigned* finish_arrived = nullptr;	 // [2] arrival counters of the finish kernel per slot, zero between launches
+	// The finish kernel of sums slot s runs on finish_stream (highest
+	// priority) after step_ev[s], the end of its observation step on stream,
+	// so that the lattice's next step does not wait for it; sums_ev[s] then
+	// marks the slot's sums ready.  Each slot has its own partials (partials
+	// holds two slots).
+	cudaStream_t finish_stream = nullptr;
+	cudaEvent_t step_ev[2] = {nullptr, nullptr};
 	bool sums_valid = false;
 	long long iteration = 0;
 	int bx = 0, by = 0;	 // 0: default

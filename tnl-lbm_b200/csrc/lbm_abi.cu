@@ -156,16 +156,28 @@ int check(lbm_handle h)
 	return LBM_OK;
 }
 
+// one slot of partial sums: [NRED][blocks] partials and the finish scratch
+size_t partials_slot_doubles(long long blocks)
+{
+	return (size_t) blocks * lbm::NRED_HOST + lbm::finish_scratch_doubles();
+}
+// slot s of the partial sums
+double* partials_of(lbm_handle h, int s)
+{
+	return h->partials + (size_t) s * partials_slot_doubles(h->partials_cap);
+}
 int ensure_partials(lbm_handle h, long long blocks)
 {
 	if (blocks <= h->partials_cap)
 		return LBM_OK;
-	if (h->partials)
+	if (h->partials) {
+		// a finish kernel may still read the old slots
+		LBM_CUDA(cudaStreamSynchronize(h->finish_stream));
 		cudaFree(h->partials);
+	}
 	h->partials = nullptr;
 	h->partials_cap = 0;
-	// per-block partials [NRED][blocks] followed by the finish-stage scratch
-	LBM_CUDA(cudaMalloc(&h->partials, ((size_t) blocks * lbm::NRED_HOST + lbm::finish_scratch_doubles()) * sizeof(double)));
+	LBM_CUDA(cudaMalloc(&h->partials, 2 * partials_slot_doubles(blocks) * sizeof(double)));
 	h->partials_cap = blocks;
 	return LBM_OK;
 }
@@ -186,7 +198,12 @@ int launch_step(lbm_handle h, bool macro, bool sums, bool dry_run = false)
 	for (int k = 0; k < 3; k++)
 		L.inflow[k] = h->inflow[k];
 	L.macro = macro ? h->macro : nullptr;
-	L.partials = sums ? h->partials : nullptr;
+	// the slot of the sums ring this step fills; the finish kernel that last
+	// read the slot (two observation steps ago) must be done with it
+	const int sums_slot = h->sums_last ^ 1;
+	L.partials = sums ? partials_of(h, sums_slot) : nullptr;
+	if (sums && !dry_run)
+		LBM_CUDA(cudaStreamWaitEvent(h->stream, h->sums_ev[sums_slot], 0));
 	L.p = h->p;
 	L.coll = h->d.collision;
 	L.cum_flags = h->d.cum_flags;
@@ -461,12 +478,20 @@ int lbm_create(const lbm_desc* desc, lbm_handle* out)
 		&& (cudaMalloc(&h->map, (size_t) h->sites() + 64) != cudaSuccess
 			|| cudaMemsetAsync(h->map, 0, (size_t) h->sites() + 64, h->stream) != cudaSuccess))
 		return cleanup(fail(LBM_ERR_CUDA, "map allocation failed"));
+	// the finish stream at the highest priority: its few blocks take the first
+	// SM slots that the next step's blocks free instead of queueing behind
+	// them (at the default priority the end-to-end step was slower)
+	int top = 0;
 	if (cudaHostAlloc(&h->sums_host, 2 * lbm::NRED_HOST * sizeof(double), cudaHostAllocMapped) != cudaSuccess
 		|| cudaEventCreateWithFlags(&h->sums_ev[0], cudaEventDisableTiming) != cudaSuccess
 		|| cudaEventCreateWithFlags(&h->sums_ev[1], cudaEventDisableTiming) != cudaSuccess
 		|| cudaHostGetDevicePointer((void**) &h->sums_mapped, h->sums_host, 0) != cudaSuccess
-		|| cudaMalloc(&h->finish_arrived, sizeof(unsigned)) != cudaSuccess
-		|| cudaMemsetAsync(h->finish_arrived, 0, sizeof(unsigned), h->stream) != cudaSuccess)
+		|| cudaMalloc(&h->finish_arrived, 2 * sizeof(unsigned)) != cudaSuccess
+		|| cudaMemsetAsync(h->finish_arrived, 0, 2 * sizeof(unsigned), h->stream) != cudaSuccess
+		|| cudaDeviceGetStreamPriorityRange(nullptr, &top) != cudaSuccess
+		|| cudaStreamCreateWithPriority(&h->finish_stream, cudaStreamNonBlocking, top) != cudaSuccess
+		|| cudaEventCreateWithFlags(&h->step_ev[0], cudaEventDisableTiming) != cudaSuccess
+		|| cudaEventCreateWithFlags(&h->step_ev[1], cudaEventDisableTiming) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "reduction buffers allocation failed"));
 	if (cudaMalloc(&h->status_dev, sizeof(int)) != cudaSuccess || cudaMemsetAsync(h->status_dev, 0, sizeof(int), h->stream) != cudaSuccess)
 		return cleanup(fail(LBM_ERR_CUDA, "status word allocation failed"));
@@ -513,14 +538,18 @@ int lbm_destroy(lbm_handle h)
 		cudaStreamDestroy(h->upload_stream);
 	if (h->halo_ev)
 		cudaEventDestroy(h->halo_ev);
+	if (h->finish_stream)
+		cudaStreamSynchronize(h->finish_stream);
 	cudaFree(h->partials);
 	cudaFree(h->finish_arrived);
 	cudaFree(h->status_dev);
 	if (h->sums_host)
 		cudaFreeHost(h->sums_host);
-	for (cudaEvent_t ev : h->sums_ev)
+	for (cudaEvent_t ev : {h->sums_ev[0], h->sums_ev[1], h->step_ev[0], h->step_ev[1]})
 		if (ev)
 			cudaEventDestroy(ev);
+	if (h->finish_stream)
+		cudaStreamDestroy(h->finish_stream);
 	if (h->stream)
 		cudaStreamDestroy(h->stream);
 	delete h;
@@ -842,11 +871,15 @@ int finish_observation(lbm_handle h)
 	const int slot = h->sums_last ^ 1;
 	const long long nb = h->last_blocks;
 	const double mass_offset = h->last_nothing_skipped ? (double) h->nothing_sites : 0.0;
-	const cudaError_t e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived,
-										   h->sums_mapped + slot * lbm::NRED_HOST, h->stream, mass_offset);
+	double* part = partials_of(h, slot);
+	// on the finish stream: the lattice's next step does not wait for it
+	LBM_CUDA(cudaEventRecord(h->step_ev[slot], h->stream));
+	LBM_CUDA(cudaStreamWaitEvent(h->finish_stream, h->step_ev[slot], 0));
+	const cudaError_t e = lbm::finish_sums(part, nb, part + nb * lbm::NRED_HOST, h->finish_arrived + slot,
+										   h->sums_mapped + slot * lbm::NRED_HOST, h->finish_stream, mass_offset);
 	if (e != cudaSuccess)
 		return fail(LBM_ERR_CUDA, "sum finish failed: %s", cudaGetErrorString(e));
-	LBM_CUDA(cudaEventRecord(h->sums_ev[slot], h->stream));
+	LBM_CUDA(cudaEventRecord(h->sums_ev[slot], h->finish_stream));
 	h->sums_iter[slot] = h->iteration;
 	h->sums_last = slot;
 	return LBM_OK;
@@ -991,9 +1024,13 @@ int lbm_enstrophy_sum(lbm_handle h, double* out)
 		return rc;
 	double* dres = nullptr;
 	LBM_CUDA(cudaMallocAsync((void**) &dres, lbm::NRED_HOST * sizeof(double), h->stream));
-	cudaError_t e = lbm::enstrophy_partials(h->macro, h->ops->compute_size, h->d.X, h->d.Y, h->d.Z, h->partials, &nb, h->stream);
+	// slot 0 and its counter, once the finish kernels in flight are done
+	for (cudaEvent_t ev : h->sums_ev)
+		LBM_CUDA(cudaStreamWaitEvent(h->stream, ev, 0));
+	double* part = partials_of(h, 0);
+	cudaError_t e = lbm::enstrophy_partials(h->macro, h->ops->compute_size, h->d.X, h->d.Y, h->d.Z, part, &nb, h->stream);
 	if (e == cudaSuccess)
-		e = lbm::finish_sums(h->partials, nb, h->partials + nb * lbm::NRED_HOST, h->finish_arrived, dres, h->stream);
+		e = lbm::finish_sums(part, nb, part + nb * lbm::NRED_HOST, h->finish_arrived, dres, h->stream);
 	double res[lbm::NRED_HOST];
 	if (e == cudaSuccess)
 		e = cudaMemcpyAsync(res, dres, sizeof(res), cudaMemcpyDeviceToHost, h->stream);
@@ -1010,6 +1047,7 @@ int lbm_synchronize(lbm_handle h)
 	if (int rc = check(h))
 		return rc;
 	LBM_CUDA(cudaStreamSynchronize(h->stream));
+	LBM_CUDA(cudaStreamSynchronize(h->finish_stream));
 	return LBM_OK;
 }
 

@@ -103,9 +103,12 @@ long long finish_scratch_doubles()
 cudaError_t finish_sums(const double* partials, long long nslots, double* stage, unsigned* arrived, double* out, cudaStream_t st,
 						double mass_offset)
 {
-	// programmatic dependent launch: the finish grid is scheduled while the
-	// step's last blocks run (the step kernels trigger it when they start)
-	// instead of after the step has drained, and waits in griddepcontrol.wait
+	// programmatic dependent launch: where the finish follows the kernel that
+	// wrote the partials on the same stream, its grid is scheduled while that
+	// kernel's last blocks run (the observation step kernels trigger it when
+	// they start) and waits in griddepcontrol.wait; after a wait on another
+	// stream's event (the sums of lbm_step, on the finish stream) it starts as
+	// an ordinary launch
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3(FINISH_BLOCKS);
 	cfg.blockDim = dim3(FINISH_THREADS);
