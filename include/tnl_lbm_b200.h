@@ -165,7 +165,10 @@ LBM_API int lbm_get_macro(lbm_handle h, double* host);
 /* Sums of the last step run with LBM_STEP_SUMS: out[6] = {sum rho, sum rho vx,
  * sum rho vy, sum rho vz, sum rho |u|^2, non-finite count}, accumulated in
  * FP64 (GEO_NOTHING sites count as rho = 1, u = 0).  Returns
- * LBM_ERR_NONFINITE when the count is non-zero (state.hpp:1469-1492). */
+ * LBM_ERR_NONFINITE when the count is non-zero (state.hpp:1469-1492).  The
+ * last stage of the reduction runs on a stream of the library's own, so the
+ * lattice's next step does not wait for it; lbm_get_sums, lbm_get_sums_of
+ * and lbm_synchronize wait for it. */
 LBM_API int lbm_get_sums(lbm_handle h, double* out);
 /* The sums of the observation step (LBM_STEP_SUMS) that ended at `iteration`;
  * the last two observation steps are kept.  Waits for that step alone, not
@@ -177,7 +180,7 @@ LBM_API int lbm_get_sums_of(lbm_handle h, int64_t iteration, double* out);
  * periodic central differences (sim_4.cu:21-54, :279-298). */
 LBM_API int lbm_enstrophy_sum(lbm_handle h, double* out);
 
-/* Wait for all work of the handle. */
+/* Wait for all work of the handle (its stream and its reduction stream). */
 LBM_API int lbm_synchronize(lbm_handle h);
 
 /* Thread-block shape of the step kernels; (0,0) restores the default. */
