@@ -1,7 +1,7 @@
 """Benchmark of the D3Q27 cumulant A-A hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload duct|tgv512|tgv64] [--storage f32|f64|f32s|f16s|bf16s]
+                    [--workload duct|tgv512|tgv64] [--storage f32|f64|f32s|f16s|bf16s|i16s]
 
 Default workload: rectangular duct 512x128x128, FP32 storage, default cumulant
 (the duct solver's configuration, sim_NSE/sim_2.cu:475), walls (GEO_WALL) one
@@ -36,10 +36,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "tnl-lbm_b200"))
 
 METRIC = "D3Q27 cumulant A-A MLUPS, % HBM roofline; FP16-store vs FP32 at stated error"
-BYTES_PER_ELEM = {"f64": 8, "f32": 4, "f32s": 4, "f16s": 2, "bf16s": 2, "f16sr": 2, "bf16sr": 2}
+BYTES_PER_ELEM = {"f64": 8, "f32": 4, "f32s": 4, "f16s": 2, "bf16s": 2, "f16sr": 2, "bf16sr": 2, "i16s": 2}
 # the type the populations are stored in / the type the update computes in
 DTYPE_LABEL = {"f64": "f64", "f32": "f32", "f32s": "f32", "f16s": "f16-store/f32", "bf16s": "bf16-store/f32",
-               "f16sr": "f16-store/f32", "bf16sr": "bf16-store/f32"}
+               "f16sr": "f16-store/f32", "bf16sr": "bf16-store/f32", "i16s": "i16-store/f32"}
 
 
 def workload_spec(name):
@@ -98,7 +98,7 @@ def measure_ensemble(pl, local, spec, storage, steps, warmup, dist=None, world=1
     sizes, nus = ensemble_setup(spec["count"], edges=spec["edges"])
     sites = sum(x * y * z for x, y, z in sizes)
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
-          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
+          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR, "i16s": pl.STORE_I16S}[storage]
     ens = pl.Ensemble(sizes, nus, cum_flags=3, storage=st, device=local)
     ens.init_taylor_green(0.05)
     shapes = {}
@@ -477,7 +477,7 @@ def trt_plugin_id(pl):
 
 def make_lattice(pl, spec, storage, device, kernel="direct", collision="cum"):
     st = {"f64": pl.STORE_F64, "f32": pl.STORE_F32, "f32s": pl.STORE_F32S, "f16s": pl.STORE_F16S,
-          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR}[storage]
+          "bf16s": pl.STORE_BF16S, "f16sr": pl.STORE_F16SR, "bf16sr": pl.STORE_BF16SR, "i16s": pl.STORE_I16S}[storage]
     X, Y, Z = spec["X"], spec["Y"], spec["Z"]
     if spec["kind"] == "duct":
         m, prof, nu, fields = duct_setup(X, Y, Z)
@@ -556,13 +556,14 @@ def duct_fp32_vs_fp64(pl, device, steps=5000, every=500):
 
 def tgv512_throughput(pl, device, steps, warmup, kernel16="pair"):
     """Throughput of the largest single-GPU configuration, the 512^3
-    Taylor-Green vortex, in FP32 and in FP16 shifted storage."""
+    Taylor-Green vortex, in FP32, in FP16 shifted storage and in 16-bit
+    fixed-point deviations."""
     import torch
     spec = workload_spec("tgv512")
     sites = spec["X"] * spec["Y"] * spec["Z"]
     peak, _ = read_peaks()
     out = {"workload": spec["workload"]}
-    for st, kernel in (("f32", "pair"), ("f16s", kernel16)):
+    for st, kernel in (("f32", "pair"), ("f16s", kernel16), ("i16s", kernel16)):
         lat, _ = make_lattice(pl, spec, st, device, kernel)
         stream = torch.cuda.ExternalStream(lat.device_view().stream, device=torch.device("cuda", device))
         secs = time_steps(pl, lat, steps, warmup, stream)
@@ -572,6 +573,7 @@ def tgv512_throughput(pl, device, steps, warmup, kernel16="pair"):
         out[st] = {"mlups": round(mlups, 1), "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
                    "step_kernel": kernel}
     out["f16s_speedup_vs_f32"] = round(out["f16s"]["mlups"] / out["f32"]["mlups"], 3)
+    out["i16s_speedup_vs_f32"] = round(out["i16s"]["mlups"] / out["f32"]["mlups"], 3)
     return out
 
 
@@ -722,7 +724,7 @@ def run_ours(args):
     variants = {}
     if args.variants and args.storage == "f32" and not spec.get("ade"):
         lat.close()
-        for st in ("f16s", "bf16s", "f16sr", "bf16sr"):
+        for st in ("f16s", "bf16s", "f16sr", "bf16sr", "i16s"):
             vl, _ = make_lattice(pl, spec, st, local, args.kernel)
             if args.autotune:
                 vl.autotune(16)
@@ -763,7 +765,7 @@ def run_ours(args):
     precision = None
     if args.precision and rank == 0:
         from pytnl_lbm import precision as prec
-        precision = prec.study(256, 20000, 200, ("f32", "f16s", "f16sr", "bf16sr"), local)
+        precision = prec.study(256, 20000, 200, ("f32", "f16s", "f16sr", "bf16sr", "i16s"), local)
         precision.pop("series")
     # the duct configuration's FP32-against-FP64 comparison and the 512^3
     # Taylor-Green throughput

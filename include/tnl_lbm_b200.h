@@ -54,6 +54,9 @@ typedef struct lbm_lattice* lbm_handle;
 #define LBM_STORE_BF16S 4 /* bfloat16 f_q - w_q; FP32 arithmetic */
 #define LBM_STORE_F16SR 5  /* as LBM_STORE_F16S, stochastic rounding on store */
 #define LBM_STORE_BF16SR 6 /* as LBM_STORE_BF16S, stochastic rounding on store */
+#define LBM_STORE_I16S 7   /* int16 round((f_q - w_q) / q_q), q_q a power of two with
+                              32767 q_q = 0.42 w_q: fixed point over |f_q - w_q| <= 0.42 w_q
+                              (clamped beyond); FP32 arithmetic */
 
 /* collision slot (COLL of LBM_CONFIG) */
 #define LBM_COLL_CUM 0 /* D3Q27_CUM, include/lbm3d/d3q27/col_cum.h */

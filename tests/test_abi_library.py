@@ -62,7 +62,7 @@ def test_argument_validation_without_gpu():
     for X, Y, Z in ((65535 * 4 + 1, 4, 4), (4, 65536, 4), (4, 4, 65536)):
         d = _abi.lbm_desc(X=X, Y=Y, Z=Z, storage=1, viscosity=0.01)
         assert lib.lbm_create(ctypes.byref(d), ctypes.byref(h)) == 5
-    for field, value in (("storage", 7), ("storage", -1), ("collision", 4), ("equilibrium", 2)):
+    for field, value in (("storage", 8), ("storage", -1), ("collision", 4), ("equilibrium", 2)):
         d = _abi.lbm_desc(X=4, Y=4, Z=4, storage=1, viscosity=0.01)
         setattr(d, field, value)
         assert lib.lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1, (field, value)

@@ -9,6 +9,7 @@ them), so the states agree to FP32 rounding.  After 7 steps:
                                  can move a value by one FP16 step of the
                                  scaled deviation)
   BF16 storage                  <= 4e-4 (one BF16 step)
+  16-bit fixed point            <= 4e-5 (a few quanta of at most 3.8e-6)
   stochastically rounded        4 times the bound of the format: a different
   FP16 / BF16                   value before the store draws an independent
                                 rounding, and the draws of 7 steps add up
@@ -29,7 +30,8 @@ from helpers import duct_map, random_map, seeded_state
 
 pytestmark = pytest.mark.gpu
 
-STORAGES = {"F32": 2e-6, "F32S": 2e-6, "F16S": 4e-5, "F16SR": 1.6e-4, "BF16S": 4e-4, "BF16SR": 1.6e-3}
+STORAGES = {"F32": 2e-6, "F32S": 2e-6, "F16S": 4e-5, "F16SR": 1.6e-4, "BF16S": 4e-4, "BF16SR": 1.6e-3,
+            "I16S": 4e-5}
 
 
 @pytest.fixture(scope="module")

@@ -241,8 +241,50 @@ def test_storage_roundtrip(pl, port, storage, tol):
         assert got.shape == lat._pop_shape(layout)
 
 
+def i16s_quantise(f):
+    """Numpy restatement of the 16-bit fixed-point deviation format (StoreI16S,
+    d3q27.cuh): FP32 populations [27, ...] stored as i = rint((f - w) / q),
+    clamped to +-32767, with q = 2^-18 / 4^nnz(q); read back as the FP32
+    rounding of w + i q.  The store's (f - w) / q is one fused multiply-add:
+    exact in FP64, rounded once to FP32 before the rounding to an integer.
+    A NaN stays NaN."""
+    cx = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])
+    cy = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1])
+    cz = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1])
+    nnz = np.abs(cx) + np.abs(cy) + np.abs(cz)
+    w = np.where(nnz == 0, 8 / 27, np.where(nnz == 1, 2 / 27, np.where(nnz == 2, 1 / 54, 1 / 216))).astype(np.float32)
+    q = 2.0 ** (-18 - 2 * nnz)
+    shape = (27,) + (1,) * (f.ndim - 1)
+    w64, q = w.astype(np.float64).reshape(shape), q.reshape(shape)
+    d = ((f.astype(np.float32).astype(np.float64) - w64) / q).astype(np.float32)
+    i = np.clip(np.rint(d), -32767, 32767).astype(np.float64)
+    return (w64 + i * q).astype(np.float32)
+
+
+def test_i16s_storage_is_the_stated_quantisation(pl, port):
+    rng = np.random.default_rng(19)
+    X, Y, Z = 33, 9, 7
+    f0 = seeded_state(port, rng, X, Y, Z).astype(np.float32)
+    f0[5, 3, 4, 6] = 0.5  # beyond the range: clamped
+    f0[2, 2, 2, 2] = np.nan  # kept as NaN
+    lat = pl.LBM(X, Y, Z, viscosity=0.01, storage=pl.STORE_I16S, periodic=True)
+    lat.set_populations(f0)
+    back = lat.get_populations(dtype=np.float32)
+    np.testing.assert_array_equal(back, i16s_quantise(f0))
+    # resolution inside the range |f - w| < 0.42 w: half a quantum, at most
+    # 2^-19 (the rest population); the seeded state's fastest sites lie beyond
+    # it and are clamped
+    w = (i16s_quantise(np.zeros_like(f0)) * 0 + 1).astype(np.float64)
+    nnz = np.array([0] + [1] * 6 + [2] * 12 + [3] * 8).reshape((27,) + (1,) * (f0.ndim - 1))
+    w = w * np.where(nnz == 0, 8 / 27, np.where(nnz == 1, 2 / 27, np.where(nnz == 2, 1 / 54, 1 / 216)))
+    inside = np.abs(f0 - w) < 0.41 * w
+    assert inside.mean() > 0.99 and np.isnan(back[2, 2, 2, 2])
+    assert np.abs(back.astype(np.float64) - f0)[inside].max() <= 2.0 ** -19
+    lat.close()
+
+
 @pytest.mark.parametrize("storage,tol", [("F32S", 1e-5), ("F16S", 2e-3), ("BF16S", 2e-2), ("F16SR", 2e-3),
-                                         ("BF16SR", 2e-2)])
+                                         ("BF16SR", 2e-2), ("I16S", 2e-3)])
 def test_shifted_storage_follows_fp64(pl, storage, tol):
     """Shifted low-precision storage with FP32 arithmetic against an FP64 run
     of the same Taylor-Green vortex (kinetic energy after 200 steps)."""
@@ -295,19 +337,20 @@ def test_autotune_restores_state(pl, port):
     assert np.array_equal(lat.get_populations(), before)
 
 
-def test_nonfinite_density_is_reported(pl):
-    lat = pl.LBM(16, 8, 8, viscosity=0.01, storage=pl.STORE_F64, periodic=True)
+@pytest.mark.parametrize("storage", ["F64", "F16S", "I16S"])
+def test_nonfinite_density_is_reported(pl, storage):
+    lat = pl.LBM(16, 8, 8, viscosity=0.01, storage=getattr(pl, "STORE_" + storage), periodic=True)
     lat.init_equilibrium()
     f = lat.get_populations()
     f[0, 4, 4, 4] = np.nan
-    lat.set_populations(f)
+    lat.set_populations(f if storage == "F64" else f.astype(np.float32))
     lat.step(2, sums=True)
     with pytest.raises(pl.LbmError) as e:
         lat.sums()
     assert e.value.code == 4
 
 
-@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S", "F16SR", "BF16SR"])
+@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S", "F16SR", "BF16SR", "I16S"])
 @pytest.mark.parametrize("shape", [(128, 16, 8), (200, 9, 7), (40, 33, 5), (37, 9, 7), (5, 4, 3), (300, 10, 8)])
 def test_tile_kernel_matches_direct_kernel(pl, port, storage, shape):
     """The step kernels are the same update: equal results, bit for bit,

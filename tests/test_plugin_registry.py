@@ -48,12 +48,12 @@ def test_plugin_library_exports_only_its_launchers(pl):
 
 def test_launcher_answers_storage_queries_without_a_device(pl):
     so = ctypes.CDLL(example_path(pl))
-    built = {"lbm_example_srt": range(7), "lbm_example_streaming": (0, 1), "lbm_example_trt": (0, 1)}
+    built = {"lbm_example_srt": range(8), "lbm_example_streaming": (0, 1), "lbm_example_trt": (0, 1)}
     for name in LAUNCHERS:
         fn = getattr(so, name)
         fn.restype = ctypes.c_int32
         fn.argtypes = [ctypes.c_void_p, ctypes.c_int32]
-        for storage in range(-1, 8):
+        for storage in range(-1, 9):
             want = 0 if storage in built[name] else NOT_SUPPORTED
             assert fn(None, storage) == want, (name, storage)
 

@@ -87,6 +87,14 @@ __host__ __device__ constexpr float half_scale(int q)
 	return nnz(q) == 0 ? 4.0f : nnz(q) == 1 ? 16.0f : nnz(q) == 2 ? 64.0f : 256.0f;
 }
 
+// quantum of the 16-bit fixed-point deviation format (StoreI16S): the
+// power of two that spreads the deviations |f_q - w_q| <= 0.42 w_q over the
+// signed 16-bit range (32767 q = 0.42 w_q for every weight class)
+__host__ __device__ constexpr float fixed_quantum(int q)
+{
+	return nnz(q) == 0 ? 0x1p-18f : nnz(q) == 1 ? 0x1p-20f : nnz(q) == 2 ? 0x1p-22f : 0x1p-24f;
+}
+
 // GEO site types of D3Q27_BC_All (include/lbm3d/d3q27/bc.h:17-43); the map
 // stores these values as uint8
 enum Geo : uint8_t
@@ -135,6 +143,7 @@ constexpr unsigned PAIR_WORK_REST = 0x80000000u;
 //   F16S  half    (f_q - w_q) * half_scale(q)
 //   BF16S bf16    f_q - w_q
 //   F16SR, BF16SR as F16S and BF16S, rounded stochastically on store
+//   I16S  int16   round((f_q - w_q) / fixed_quantum(q)), clamped to +-32767
 // Every format is read into the compute type R and written back from it.
 // ---------------------------------------------------------------------------
 struct StoreF64
@@ -292,6 +301,59 @@ struct StoreBF16SR : StoreBF16S
 		const float x = stochastic_round_bits<16>(v - (float) weight(Q));
 		const unsigned short h = (unsigned short) (__float_as_uint(x) >> 16);
 		__stcs(reinterpret_cast<unsigned short*>(p), h);
+	}
+};
+
+// 16-bit fixed-point deviations: the integer i = round((f - w) / q) with the
+// power-of-two quantum q = fixed_quantum(Q), kept as the unsigned 16-bit
+// pattern of i + 32768.  Over its range |f - w| <= 0.42 w every value carries
+// the same absolute resolution q / 2 = 6.5e-6 w, where FP16 keeps 11
+// significant bits of the deviation itself (a relative 2.4e-4): about 5x finer
+// at the deviations of u = 0.05 flows (0.15 w), coarser only below 0.03 w.
+// Deviations beyond the range are clamped (densities outside 1 +- 0.3 at low
+// Mach number); a NaN is kept as the one pattern the clamp never produces
+// (0, i = -32768) and read back as NaN, so the non-finite count of the sums
+// still sees it.  The conversions are exact integer-float bit patterns: an
+// integer below 2^16 ORed into the mantissa of 2^23 is the float 2^23 + u, and
+// a float in [2^23, 2^24) has the integer part of its value in the low
+// mantissa bits, so the round to nearest of the store is one addition.
+struct StoreI16S
+{
+	using T = short;
+	using R = float;
+	static constexpr float BIAS = 8421376.0f;	// 2^23 + 2^15
+	static constexpr float ROUND = 12615680.0f;	// 1.5 * 2^23 + 2^15
+	// f from the stored pattern u = i + 2^15 (0: NaN)
+	template <int Q>
+	__device__ static __forceinline__ R from_raw(unsigned u)
+	{
+		const float i = __uint_as_float(0x4B000000u | u) - BIAS;  // exact
+		const float f = __fmaf_rn(i, fixed_quantum(Q), (float) weight(Q));
+		return u ? f : __uint_as_float(0x7FFFFFFFu);
+	}
+	// the stored pattern of f: (f - w) / q as one fused multiply-add (1 / q
+	// and w / q exact), clamped, rounded to nearest by the magic addition
+	template <int Q>
+	__device__ static __forceinline__ unsigned to_raw(R v)
+	{
+		const float d = __fmaf_rn(v, 1.0f / fixed_quantum(Q), -(float) weight(Q) / fixed_quantum(Q));
+		const unsigned u = __float_as_uint(fminf(fmaxf(d, -32767.0f), 32767.0f) + ROUND) & 0xFFFFu;
+		return d == d ? u : 0u;
+	}
+	template <int Q>
+	__device__ static __forceinline__ R load(const T* p)
+	{
+		return from_raw<Q>(__ldcs(reinterpret_cast<const unsigned short*>(p)));
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store(T* p, R v)
+	{
+		__stcs(reinterpret_cast<unsigned short*>(p), (unsigned short) to_raw<Q>(v));
+	}
+	template <int Q>
+	__device__ static __forceinline__ R load_smem(const T* p)
+	{
+		return from_raw<Q>(*reinterpret_cast<const unsigned short*>(p));
 	}
 };
 

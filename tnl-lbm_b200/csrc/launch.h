@@ -18,7 +18,8 @@ enum Storage : int
 	ST_BF16S = 4,
 	ST_F16SR = 5,
 	ST_BF16SR = 6,
-	ST_COUNT = 7
+	ST_I16S = 7,
+	ST_COUNT = 8
 };
 
 // collision-slot constants in double; each unit casts them to its compute type
@@ -133,6 +134,7 @@ cudaError_t pair_step_f16s(const StepLaunch&);
 cudaError_t pair_step_f16sr(const StepLaunch&);
 cudaError_t pair_step_bf16s(const StepLaunch&);
 cudaError_t pair_step_bf16sr(const StepLaunch&);
+cudaError_t pair_step_i16s(const StepLaunch&);
 // upper bound of the tile kernel's grid (blocks per SM x SMs)
 constexpr int TILE_MAX_BLOCKS_PER_SM = 8;
 

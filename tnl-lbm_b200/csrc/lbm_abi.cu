@@ -31,6 +31,7 @@ const StorageOps& storage_ops_f16s();
 const StorageOps& storage_ops_bf16s();
 const StorageOps& storage_ops_f16sr();
 const StorageOps& storage_ops_bf16sr();
+const StorageOps& storage_ops_i16s();
 
 const StorageOps& storage_ops(int storage)
 {
@@ -47,6 +48,8 @@ const StorageOps& storage_ops(int storage)
 			return storage_ops_f16sr();
 		case ST_BF16SR:
 			return storage_ops_bf16sr();
+		case ST_I16S:
+			return storage_ops_i16s();
 		default:
 			return storage_ops_bf16s();
 	}
@@ -68,6 +71,8 @@ PairStepFn pair_step_of(int storage)
 			return pair_step_bf16s;
 		case ST_BF16SR:
 			return pair_step_bf16sr;
+		case ST_I16S:
+			return pair_step_i16s;
 		default:
 			return nullptr;
 	}

@@ -220,6 +220,32 @@ struct PairIO<StoreBF16SR> : PairIO<StoreBF16S>
 	}
 };
 
+template <>
+struct PairIO<StoreI16S>
+{
+	// both sites' patterns from one 32-bit word: each 16-bit half into the
+	// mantissa of 2^23 (byte permutes), the bias off as one packed addition
+	template <int Q>
+	__device__ static __forceinline__ F2 load2(const short* p)
+	{
+		const unsigned w = __ldcs(reinterpret_cast<const unsigned*>(p));
+		const F2 x(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)), __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
+		const F2 f = fma2(x - F2(StoreI16S::BIAS), F2(fixed_quantum(Q)), F2(weight(Q)));
+		const float nan = __uint_as_float(0x7FFFFFFFu);
+		return F2((w & 0xFFFFu) ? f.v.x : nan, (w >> 16) ? f.v.y : nan);  // pattern 0: NaN
+	}
+	template <int Q>
+	__device__ static __forceinline__ void store2(short* p, F2 v)
+	{
+		const F2 d = fma2(v, F2(1.0f / fixed_quantum(Q)), F2(-(float) weight(Q) / fixed_quantum(Q)));
+		const F2 c(fminf(fmaxf(d.v.x, -32767.0f), 32767.0f), fminf(fmaxf(d.v.y, -32767.0f), 32767.0f));
+		const F2 t = c + F2(StoreI16S::ROUND);
+		const unsigned lo = d.v.x == d.v.x ? __float_as_uint(t.v.x) & 0xFFFFu : 0u;  // NaN: pattern 0
+		const unsigned hi = d.v.y == d.v.y ? __float_as_uint(t.v.y) << 16 : 0u;
+		__stcs(reinterpret_cast<unsigned*>(p), lo | hi);
+	}
+};
+
 // x offsets of a pair: the left neighbour of site x and the right neighbour
 // of site x + 1 (the other two are the pair's own sites); periodic sites wrap
 struct PairX

@@ -51,7 +51,7 @@
 
 // storage sets of a plugin: bit LBM_STORE_* per storage it is compiled for
 #define LBM_PLUGIN_STORAGE(st) (1u << (st))
-#define LBM_PLUGIN_ALL_STORAGES 0x7fu
+#define LBM_PLUGIN_ALL_STORAGES 0xffu
 
 namespace lbm {
 
@@ -127,7 +127,7 @@ cudaError_t plugin_step(const StepLaunch& L)
 template <typename C, unsigned STORAGES>
 int32_t plugin_dispatch(const void* step, int32_t storage)
 {
-	if (storage < LBM_STORE_F64 || storage > LBM_STORE_BF16SR || !((STORAGES >> storage) & 1u))
+	if (storage < LBM_STORE_F64 || storage > LBM_STORE_I16S || !((STORAGES >> storage) & 1u))
 		return (int32_t) cudaErrorNotSupported;
 	if (!step)
 		return 0;
@@ -161,6 +161,10 @@ int32_t plugin_dispatch(const void* step, int32_t storage)
 		case LBM_STORE_BF16SR:
 			if constexpr ((STORAGES & LBM_PLUGIN_STORAGE(LBM_STORE_BF16SR)) != 0)
 				e = plugin_step<StoreBF16SR, C>(L);
+			break;
+		case LBM_STORE_I16S:
+			if constexpr ((STORAGES & LBM_PLUGIN_STORAGE(LBM_STORE_I16S)) != 0)
+				e = plugin_step<StoreI16S, C>(L);
 			break;
 		default:
 			break;

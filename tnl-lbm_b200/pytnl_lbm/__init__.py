@@ -20,7 +20,7 @@ from . import _abi
 from ._abi import (  # noqa: F401  (re-exported constants)
     COLL_BGK, COLL_CUM, COLL_MRT, COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST, COLL_SRT, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, EQ_SECOND_ORDER,
     ADE_CLBM, ADE_GEO, ADE_MRT, ADE_SRT, GEO, KERNEL_DIRECT, KERNEL_PAIR, KERNEL_SPLIT, KERNEL_TILE, STREAMING_AA, STREAMING_AB, LAYOUT_GHOST, LAYOUT_INTERIOR, STATUS_TIMEOUT, STEP_MACRO, STEP_SUMS,
-    STORE_BF16S, STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64, LbmError, library,
+    STORE_BF16S, STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64, STORE_I16S, LbmError, library,
     library_path)
 
 __all__ = ["LBM", "Ensemble", "LbmError", "library", "library_path", "GEO", "macro_names", "kinetic_energy", "State", "execute", "Actions",

@@ -9,7 +9,7 @@ PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LBM_OK = 0
 ERRORS = {1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "non-finite density", 5: "size limit"}
 
-STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S, STORE_F16SR, STORE_BF16SR = 0, 1, 2, 3, 4, 5, 6
+STORE_F64, STORE_F32, STORE_F32S, STORE_F16S, STORE_BF16S, STORE_F16SR, STORE_BF16SR, STORE_I16S = 0, 1, 2, 3, 4, 5, 6, 7
 COLL_CUM, COLL_SRT, COLL_BGK, COLL_MRT = 0, 1, 2, 3
 COLL_PLUGIN_FIRST, COLL_PLUGIN_LAST = 16, 31
 PLUGIN_ABI_VERSION = 2

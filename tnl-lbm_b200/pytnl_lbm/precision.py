@@ -28,10 +28,10 @@ import time
 import numpy as np
 
 from . import COLL_CUM, CUM_ANTIALIAS, CUM_GEIER_2017, EQ_INV_CUM, KERNEL_DIRECT, KERNEL_PAIR, LBM, STORE_BF16S, \
-    STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64
+    STORE_BF16SR, STORE_F16S, STORE_F16SR, STORE_F32, STORE_F32S, STORE_F64, STORE_I16S
 
 STORAGES = {"f64": STORE_F64, "f32": STORE_F32, "f32s": STORE_F32S, "f16s": STORE_F16S, "bf16s": STORE_BF16S,
-            "f16sr": STORE_F16SR, "bf16sr": STORE_BF16SR}
+            "f16sr": STORE_F16SR, "bf16sr": STORE_BF16SR, "i16s": STORE_I16S}
 
 U0 = 0.05
 RE = 1600.0
