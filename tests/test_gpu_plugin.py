@@ -77,7 +77,7 @@ def make(pl, collision, storage, periodic, shape=(20, 12, 10), use_graphs=True, 
     return lat
 
 
-@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S", "F16SR", "BF16SR"])
+@pytest.mark.parametrize("storage", ["F64", "F32", "F32S", "F16S", "BF16S", "F16SR", "BF16SR", "I16S"])
 @pytest.mark.parametrize("periodic", [False, True])
 def test_srt_plugin_equals_builtin_srt(pl, storage, periodic):
     st = getattr(pl, "STORE_" + storage)
@@ -200,7 +200,7 @@ def test_plugin_lattice_restrictions(pl):
     lat.close()
 
 
-@pytest.mark.parametrize("storage", ["F32", "F32S", "F16S", "BF16SR"])
+@pytest.mark.parametrize("storage", ["F32", "F32S", "F16S", "BF16SR", "I16S"])
 @pytest.mark.parametrize("periodic", [False, True])
 def test_srt_plugin_on_the_two_site_kernel_equals_builtin_srt(pl, storage, periodic):
     st = getattr(pl, "STORE_" + storage)
