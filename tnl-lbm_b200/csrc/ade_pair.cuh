@@ -17,50 +17,51 @@
 
 namespace lbm {
 
-// A-A read / write of the seven scalar populations of sites (x, x + 1)
+// A-A read / write of the seven scalar populations of sites (x, x + 1), with
+// the addresses of PairAt / PairSlots (pair.cuh) over the scalar's slot rows
 template <bool ODD>
-__device__ __forceinline__ void ade_pair_read(const float* __restrict__ g, long long sq, long long based, const Offsets& od, PairX px,
-											  F2 (&v)[7])
+__device__ __forceinline__ void ade_pair_read_at(const PairAt& at, const PairSlots& ps, F2 (&v)[7])
 {
 	static_for<7>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
 			if constexpr (!ODD)
-				v[q] = F2(*reinterpret_cast<const float2*>(g + q * sq + based));
+				v[q] = F2(*reinterpret_cast<const float2*>(at.P[1] + ps.b[q]));
 			else {
-				const float* c = g + opp(q) * sq + based + od.y[1 - cy(q)] + od.z[1 - cz(q)];
+				// direction q of site x comes from slot opp(q) of site x - c_q
+				const float* c = reinterpret_cast<const float*>(at.P[1 - cz(q)] + at.oy[1 - cy(q)] + ps.b[opp(q)]);
 				if constexpr (cx(q) == 0)
 					v[q] = F2(*reinterpret_cast<const float2*>(c));
 				else if constexpr (cx(q) > 0)
-					v[q] = F2(c[px.left], c[0]);
+					v[q] = F2(c[at.left], c[0]);
 				else
-					v[q] = F2(c[1], c[1 + px.right]);
+					v[q] = F2(c[1], c[1 + at.right]);
 			}
 		}
 	);
 }
 
 template <bool ODD>
-__device__ __forceinline__ void ade_pair_write(float* __restrict__ g, long long sq, long long based, const Offsets& od, PairX px,
-											   const F2 (&v)[7])
+__device__ __forceinline__ void ade_pair_write_at(const PairAt& at, const PairSlots& ps, const F2 (&v)[7])
 {
 	static_for<7>(
 		[&](auto Qc)
 		{
 			constexpr int q = decltype(Qc)::value;
 			if constexpr (!ODD)
-				*reinterpret_cast<float2*>(g + opp(q) * sq + based) = v[q].v;
+				*reinterpret_cast<float2*>(at.P[1] + ps.b[opp(q)]) = v[q].v;
 			else {
-				float* c = g + q * sq + based + od.y[1 + cy(q)] + od.z[1 + cz(q)];
+				// direction q of site x goes to slot q of site x + c_q
+				float* c = reinterpret_cast<float*>(at.P[1 + cz(q)] + at.oy[1 + cy(q)] + ps.b[q]);
 				if constexpr (cx(q) == 0)
 					*reinterpret_cast<float2*>(c) = v[q].v;
 				else if constexpr (cx(q) > 0) {
 					c[1] = v[q].v.x;
-					c[1 + px.right] = v[q].v.y;
+					c[1 + at.right] = v[q].v.y;
 				}
 				else {
-					c[px.left] = v[q].v.x;
+					c[at.left] = v[q].v.x;
 					c[0] = v[q].v.y;
 				}
 			}
@@ -69,17 +70,19 @@ __device__ __forceinline__ void ade_pair_write(float* __restrict__ g, long long 
 }
 
 // The coupled update of the pair (x, x + 1) of row (y, z) if its group is a
-// pair group (groups[] of the coupled step); every thread of the warp calls it.
+// pair group (groups[] of the coupled step); every thread of the warp calls
+// it.  Flow and scalar addresses are plane pointers plus 32-bit slot offsets
+// (ps: the flow's 27 slot rows, psd: the scalar's 7), as in pair_update.
 template <typename S, int CUMF, bool ODD>
 __device__ __forceinline__ void ade_pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
-												const AdeArgs<float>& d, const uint8_t* __restrict__ groups, int x, int y, int z)
+												const PairSlots& ps, const PairSlots& psd, const AdeArgs<float>& d,
+												const uint8_t* __restrict__ groups, int x, int y, int z)
 {
 	bool act = x < a.X && y < a.Y;
 	Site<F2> s;
 	F2 g[7];
-	Offsets o, od;
-	PairX px{-1, 1};
-	long long base = 0, based = 0, site = 0;
+	PairAt at, atd;
+	long long site = 0;
 	if (act) {
 		const long long row = (long long) z * a.Y + y;
 		const int gx = (a.X + PAIR_GROUP - 1) / PAIR_GROUP;
@@ -88,14 +91,12 @@ __device__ __forceinline__ void ade_pair_update(const StepArgs<typename S::T, fl
 		if (act) {
 			const bool wrap = gf == PAIR_GROUP_PERIODIC;
 			site = row * a.X + x;
-			base = (long long) (z + 1) * a.sz + (long long) (y + 1) * a.sy + a.x0 + x;
-			based = (long long) (z + 1) * d.sz + (long long) (y + 1) * d.sy + a.x0 + x;
-			o = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, a.sy, a.sz);
-			od = neighbour_offsets(wrap, wrap && a.zwrap, x, y, z, a.X, a.Y, a.Z, d.sy, d.sz);
-			px.left = (wrap && x == 0) ? a.X - 1 : -1;
-			px.right = (wrap && x + 1 == a.X - 1) ? -(a.X - 1) : 1;
-			pair_read<S, ODD>(a.f, a.sq, base, o, px, s);
-			ade_pair_read<ODD>(d.g, d.sq, based, od, px, g);
+			at = pair_at(a, x, y, z, wrap);
+			// the scalar's rows are the flow's, x0 alike
+			atd = pair_at_of(reinterpret_cast<char*>(d.g), (long long) sizeof(float), d.sy, d.sz, a.x0, a.X, a.Y, a.Z, x, y,
+							 z, wrap, a.zwrap != 0);
+			pair_read_at<S, ODD>(at, ps, s);
+			ade_pair_read_at<ODD>(atd, psd, g);
 			density_velocity(s, p2);
 		}
 	}
@@ -103,20 +104,21 @@ __device__ __forceinline__ void ade_pair_update(const StepArgs<typename S::T, fl
 	if (!act)
 		return;
 	collide_cumulant<F2, CUMF>(s, p2);
-	pair_write<S, ODD>(a.f, a.sq, base, o, px, s);
+	pair_write_at<S, ODD>(at, ps, s);
 	// the scalar, advected with the pair's flow velocity (unchanged by the collision)
 	const F2 phi = ade_phi(g);
 	const F2 D = d.dcoef ? F2(d.dcoef[site], d.dcoef[site + 1]) : F2(d.D);
 	ade_collide(g, phi, s.vx, s.vy, s.vz, D, d.coll);
-	ade_pair_write<ODD>(d.g, d.sq, based, od, px, g);
+	ade_pair_write_at<ODD>(atd, psd, g);
 }
 
 // One plain coupled step over the work list (items as aa_pair_work_kernel's).
 template <typename S, int CUMF, bool ODD, int MINB>
 __global__ void __launch_bounds__(128, MINB)
-	ade_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const AdeArgs<float> d,
-						 const uint8_t* __restrict__ groups, const unsigned* __restrict__ work,
-						 const unsigned long long* __restrict__ rest, long long nrest, int tiles_x)
+	ade_pair_work_kernel(const StepArgs<typename S::T, float> a, const CollParams<F2> p2, const PairSlots ps,
+						 const PairSlots psd, const AdeArgs<float> d, const uint8_t* __restrict__ groups,
+						 const unsigned* __restrict__ work, const unsigned long long* __restrict__ rest, long long nrest,
+						 int tiles_x)
 {
 	const unsigned w = work[blockIdx.x];
 	if (w & PAIR_WORK_REST) {
@@ -136,13 +138,19 @@ __global__ void __launch_bounds__(128, MINB)
 	else {
 		const unsigned row = w / (unsigned) tiles_x;
 		const int x = (int) (w - row * (unsigned) tiles_x) * 256 + 2 * (int) threadIdx.x;
-		ade_pair_update<S, CUMF, ODD>(a, p2, d, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y));
+		ade_pair_update<S, CUMF, ODD>(a, p2, ps, psd, d, groups, x, (int) (row % (unsigned) a.Y), (int) (row / (unsigned) a.Y));
 	}
 }
 
-// resident blocks per SM: the coupled pair holds 34 packed values
-#ifndef ADE_PAIR_MINB
-#define ADE_PAIR_MINB 4
+// resident blocks per SM: the coupled pair holds 34 packed values.  The even
+// step at 5 (96 registers, 32-36 bytes of spills) ran the duct with a scalar
+// at 20.05 GLUPS against 19.05 at 4; the odd step spills 200+ bytes at 5 and
+// stays at 4 (128 registers, no spills)
+#ifndef ADE_PAIR_MINB_EVEN
+#define ADE_PAIR_MINB_EVEN 5
+#endif
+#ifndef ADE_PAIR_MINB_ODD
+#define ADE_PAIR_MINB_ODD 4
 #endif
 
 // One plain coupled step through ade_pair_work_kernel; cudaErrorNotSupported
@@ -190,6 +198,12 @@ cudaError_t ade_pair_step(const StepLaunch& L)
 	d.inflow_phi = (float) A->inflow_phi;
 	d.phi = nullptr;
 	d.coll = A->coll;
+	// every slot offset of a lattice row fits 32 bits (the scalar's rows are
+	// as long as the flow's)
+	if (27ll * L.g.sq * (long long) sizeof(T) >= (1ll << 31) || 27ll * A->sq * (long long) sizeof(float) >= (1ll << 31))
+		return cudaErrorNotSupported;
+	const PairSlots ps = make_pair_slots(L.g.sq, (int) sizeof(T));
+	const PairSlots psd = make_pair_slots(A->sq, (int) sizeof(float));
 	const PairWork& W = A->pair_work;
 	const dim3 grid((unsigned) W.nwork), block(128);
 	if (L.blocks_out)
@@ -200,11 +214,11 @@ cudaError_t ade_pair_step(const StepLaunch& L)
 #define LBM_ADE_PAIR(CUMF)                                                                                             \
 	do {                                                                                                               \
 		if (L.odd)                                                                                                     \
-			ade_pair_work_kernel<S, CUMF, true, ADE_PAIR_MINB>                                                         \
-				<<<grid, block, 0, L.stream>>>(a, p2, d, A->pair_groups, W.work, W.rest, W.nrest, tiles_x);            \
+			ade_pair_work_kernel<S, CUMF, true, ADE_PAIR_MINB_ODD>                                                         \
+				<<<grid, block, 0, L.stream>>>(a, p2, ps, psd, d, A->pair_groups, W.work, W.rest, W.nrest, tiles_x);            \
 		else                                                                                                           \
-			ade_pair_work_kernel<S, CUMF, false, ADE_PAIR_MINB>                                                        \
-				<<<grid, block, 0, L.stream>>>(a, p2, d, A->pair_groups, W.work, W.rest, W.nrest, tiles_x);            \
+			ade_pair_work_kernel<S, CUMF, false, ADE_PAIR_MINB_EVEN>                                                        \
+				<<<grid, block, 0, L.stream>>>(a, p2, ps, psd, d, A->pair_groups, W.work, W.rest, W.nrest, tiles_x);            \
 	} while (0)
 	switch (L.cum_flags) {
 		case 0:
