@@ -24,16 +24,31 @@ namespace lbm {
 // resident warps keep more HBM requests in flight.  The observation variant
 // (OUT) needs no more registers than the plain step: its outputs are written
 // before the collision.  The FP64 kernels need twice the registers per value.
+//
+// FP64 arithmetic: 4 blocks (128 registers, up to 24 bytes of spills) for
+// MRT and the default and anti-aliased cumulant, 3 (168 registers, up to 68
+// bytes) for SRT, BGK and the Geier-2017 cumulant, which spill 140-500 bytes
+// at 4.  Against 2 blocks (the full 256 registers, of which these kernels use
+// 110-150), duct: cumulant 14.5 -> 15.3, SRT 11.7 -> 13.6, BGK 13.1 -> 14.5,
+// MRT 14.3 -> 15.2 GLUPS; 256^3 Taylor-Green vortex (Geier 2017) 10.7 -> 12.9.
 template <typename R, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
 constexpr int direct_minb()
 {
 	if (sizeof(R) == 8)
-		return 2;
+		return COLL == COLL_SRT || COLL == COLL_BGK || (COLL == COLL_CUM && (CUMF & CUM_2017)) ? 3 : 4;
 	if (!ODD && GENERAL)
 		return 6;  // the even general step keeps no neighbour offsets: 80 registers
 	if (COLL == COLL_CUM || COLL == COLL_MRT)
 		return 5;
 	return 4;  // SRT and BGK spill at 5
+}
+
+// resident blocks of the coupled flow + scalar step: as the direct step's,
+// and 2 with FP64 arithmetic (the scalar's seven values on top of the flow's)
+template <typename R, int COLL, int CUMF, bool ODD, bool GENERAL, bool OUT>
+constexpr int ade_minb()
+{
+	return sizeof(R) == 8 ? 2 : direct_minb<R, COLL, CUMF, ODD, GENERAL, OUT>();
 }
 
 // resident blocks of the A-B step; its observation variant spills at 5
@@ -183,10 +198,10 @@ struct StorageUnit
 		if (L.dry_run)
 			return cudaSuccess;
 		if (L.macro || L.partials || d.phi)
-			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, true, direct_minb<R, COLL, CUMF, ODD, GENERAL, true>()>
+			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, true, ade_minb<R, COLL, CUMF, ODD, GENERAL, true>()>
 				<<<L.grid, L.block, 0, L.stream>>>(a, d);
 		else
-			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, false, direct_minb<R, COLL, CUMF, ODD, GENERAL, false>()>
+			ade_step_kernel<S, COLL, CUMF, ODD, GENERAL, false, ade_minb<R, COLL, CUMF, ODD, GENERAL, false>()>
 				<<<L.grid, L.block, 0, L.stream>>>(a, d);
 		return cudaGetLastError();
 	}
