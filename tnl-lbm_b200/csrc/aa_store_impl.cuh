@@ -51,12 +51,14 @@ constexpr int ade_minb()
 	return sizeof(R) == 8 ? 2 : direct_minb<R, COLL, CUMF, ODD, GENERAL, OUT>();
 }
 
-// resident blocks of the A-B step; its observation variant spills at 5
+// resident blocks of the A-B step; its observation variant spills at 5.  In
+// FP64, 3 blocks (168 registers, 56-144 bytes of spills; the step uses about
+// 200 at 2): duct cumulant 11.8 -> 13.8, SRT 11.6 -> 13.7 GLUPS
 template <typename R, int COLL, int CUMF, bool OUT>
 constexpr int ab_minb()
 {
 	if (sizeof(R) == 8)
-		return 2;
+		return 3;
 	if (OUT)
 		return 4;
 	return direct_minb<R, COLL, CUMF, true, true, false>();
