@@ -734,6 +734,15 @@ def run_ours(args):
                             "speedup_vs_f32": secs / vsecs,
                             "achieved_gbs": 2 * 27 * 2 * sites / (vsecs / args.steps) / 1e9}
             vl.close()
+        # FP64 storage (the reference's default arithmetic), one-site kernel
+        vl, _ = make_lattice(pl, spec, "f64", local, "direct")
+        if args.autotune:
+            vl.autotune(16)
+        vs = torch.cuda.ExternalStream(vl.device_view().stream, device=device)
+        vsecs = time_steps(pl, vl, args.steps, args.warmup, vs)
+        gbs = 2 * 27 * 8 * sites / (vsecs / args.steps) / 1e9
+        variants["f64"] = {"mlups": sites * args.steps / vsecs / 1e6, "achieved_gbs": gbs, "frac": gbs / peak}
+        vl.close()
         for other in ("direct", "pair", "tile", "split"):
             if other == args.kernel or (other == "split" and spec["kind"] != "duct"):
                 continue
