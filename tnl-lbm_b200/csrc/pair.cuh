@@ -473,6 +473,18 @@ __device__ __forceinline__ void pair_outputs(const StepArgs<T, float>& a, bool i
 // rest_update, one thread per site.  OUT: the macro field and the partial sums
 // of the pair, the warp's sums in slot `slot` of nslots.  Every thread of the
 // warp calls it (threads past the lattice with x >= X).
+template <int COLL, int CUMF>
+struct BuiltinCollision;
+// true for the built-in collisions, false for a collision plugin's struct
+template <typename C>
+struct is_builtin_collision : std::false_type
+{
+};
+template <int COLL, int CUMF>
+struct is_builtin_collision<BuiltinCollision<COLL, CUMF>> : std::true_type
+{
+};
+
 template <typename S, typename C, bool ODD, bool GENERAL, bool OUT>
 __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>& a, const CollParams<F2>& p2,
 											const PairSlots& ps, const uint8_t* __restrict__ groups, int x, int y, int z,
@@ -519,8 +531,14 @@ __device__ __forceinline__ void pair_update(const StepArgs<typename S::T, float>
 	}
 	else if constexpr (OUT)
 		pair_outputs(a, act, act, site, s, slot, nslots);  // no map: before the collision (fewer live registers)
-	else
-		__syncwarp();  // keeps the collision after the loads (fewer live registers)
+	else if constexpr (!GENERAL || sizeof(typename S::T) == 2 || !is_builtin_collision<C>::value)
+		// keeps the collision after the loads (fewer live registers).  The work
+		// kernel of 32-bit storage with a built-in collision runs without it:
+		// its odd step then compiles without spills (80 bytes with it) and the
+		// duct's FP32 step is 1.6 % faster (cumulant and MRT).  The 16-bit
+		// formats are 1.2 % faster with it, and a collision plugin (4 blocks per
+		// SM) 15 %
+		__syncwarp();
 	if (!act)
 		return;
 	C::template collision<F2>(s, p2);
@@ -640,8 +658,9 @@ __global__ void __launch_bounds__(128, MINB)
 template <typename T, int COLL, bool ODD>
 constexpr int pair_minb()
 {
-	// even steps fit 96 registers without spills; odd steps spill 8-32 bytes
-	// at 96 and still run faster than at 4 blocks (116-128 registers): duct
+	// even steps fit 96 registers without spills; odd steps spill up to 32
+	// bytes at 96 in some variants and still run faster than at 4 blocks
+	// (116-128 registers): duct
 	// 25.2 GLUPS, Taylor-Green 512^3 27.5 against 27.2 at equal clocks.  The
 	// even step of the 16-bit formats runs 6 blocks (80 registers, 8-32 bytes
 	// of spills): duct F16S 35.2 against 34.4 GLUPS at 5
